@@ -1,0 +1,194 @@
+/*
+ * avbd.h - C-ABI of the B200 (sm_100a) augmented vertex block descent step.
+ *
+ * Drop-in boundary for SkyePhyX's `Solver` (src/physics/solver.hpp:22-94):
+ * the same bodies, box colliders, joints, springs, Neo-Hookean tetrahedra and
+ * StVK triangles, built through the same calls and stepped by `avbd_step`,
+ * which replaces `Solver::Step()` (src/physics/solver.cpp:199-627).  All step
+ * work runs in CUDA kernels; the host only stages scenes and reads results.
+ *
+ * Conventions: plain pointers and sizes, float32, quaternions as (w, x, y, z),
+ * vectors as 3 consecutive floats; body / force / energy ids are creation
+ * indices returned by the add_* calls.  Negative returns are AVBD_ERR_* codes;
+ * step calls return an AVBD_STATUS_* value.  One world is not thread-safe;
+ * distinct worlds are independent.
+ */
+#ifndef AVBD_H
+#define AVBD_H
+
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+/* ---- status and error codes ---- */
+#define AVBD_STATUS_OK        0  /* step ran */
+#define AVBD_STATUS_EXPLODED  1  /* a velocity component left [-500, 500] m/s (solver.cpp:182-196); the
+                                    world is frozen like Solver::emergencyStop and later steps are no-ops */
+#define AVBD_STATUS_NAN       2  /* a pose became NaN; frozen like EXPLODED */
+#define AVBD_STATUS_CAPACITY  3  /* a device table was too small for this step; the step was not applied */
+#define AVBD_STATUS_TIMEOUT   4  /* a bounded device wait gave up; the step was not applied */
+
+#define AVBD_ERR_INVALID  (-1)   /* bad argument (unknown id, null pointer, bad size) */
+#define AVBD_ERR_CUDA     (-2)   /* a CUDA runtime call failed */
+#define AVBD_ERR_NOMEM    (-3)   /* device or host allocation failed */
+#define AVBD_ERR_STATE    (-4)   /* call not valid in the current state */
+#define AVBD_ERR_NODEVICE (-5)   /* no CUDA device: there is no CPU fallback */
+
+/* ModelType (geometry.hpp:17-22); every body collides as a box (collision.hpp:28-31). */
+#define AVBD_MODEL_CUBE    0
+#define AVBD_MODEL_SPHERE  1
+#define AVBD_MODEL_PYRAMID 2
+
+/* EigenProjectionMode (math.hpp:99-104). */
+#define AVBD_PROJECT_CLAMP    0
+#define AVBD_PROJECT_ABSOLUTE 1
+#define AVBD_PROJECT_ADAPTIVE 2
+
+/* Public solver parameters, same names and defaults as solver.hpp:69-84. */
+typedef struct AvbdParams {
+    int32_t num_iterations;         /* numIterations = 10 */
+    float   step_value;             /* stepValue (dt) = 1/60 s */
+    float   alpha;                  /* 0.95 */
+    float   beta;                   /* 100000 */
+    float   gamma;                  /* 0.99 */
+    float   on_penetration_penalty; /* 0 */
+    int32_t post_stabilization;     /* 1 */
+    int32_t projection_mode;        /* AVBD_PROJECT_ABSOLUTE */
+    float   trust_region_rho;       /* 0 */
+} AvbdParams;
+
+/* Per-phase device times of the last step in ms, named after SolverTimings
+ * (solver.hpp:10-19) plus the colouring phase this build adds. */
+typedef struct AvbdTimings {
+    float broad_phase_ms;
+    float warmstart_ms;       /* narrowphase + manifold warm-start + incidence build */
+    float colouring_ms;
+    float prediction_ms;
+    float primal_dual_ms;
+    float velocity_update_ms;
+    float post_stab_ms;
+    float total_substep_ms;
+} AvbdTimings;
+
+typedef struct AvbdWorld AvbdWorld;
+typedef struct AvbdBatch AvbdBatch;
+
+void avbd_default_params(AvbdParams* out);
+const char* avbd_status_string(int32_t code);
+
+/* ---------------------------------------------------------------------------
+ * Single scene (the plain path).  Replaces one Solver instance.
+ * ------------------------------------------------------------------------- */
+
+/* Solver::Solver / Solver::Start (solver.cpp:18-33). device = CUDA ordinal. */
+int32_t avbd_world_create(const AvbdParams* params, int32_t device, AvbdWorld** out);
+/* Solver::~Solver / Clear (solver.cpp:23-47). */
+int32_t avbd_world_destroy(AvbdWorld* w);
+int32_t avbd_world_clear(AvbdWorld* w);
+int32_t avbd_set_params(AvbdWorld* w, const AvbdParams* params);
+int32_t avbd_get_params(const AvbdWorld* w, AvbdParams* out);
+
+/* Solver::AddBody (solver.cpp:50-101). Returns the body id. */
+int32_t avbd_add_body(AvbdWorld* w, int32_t model_type, float density, float friction, const float pos[3],
+                      const float scale[3], const float vel[3], const float quat_wxyz[4], const float omega[3],
+                      int32_t is_static);
+/* Solver::AddParticle (solver.cpp:119-131): a 0.1 m cube with zero inertia. */
+int32_t avbd_add_particle(AvbdWorld* w, float mass, float friction, const float pos[3], const float vel[3],
+                          int32_t is_static);
+/* Mesh::isStatic set after creation, as levels.h:472-473 pins cloth corners. */
+int32_t avbd_set_body_static(AvbdWorld* w, int32_t body, int32_t is_static);
+/* Spring (force.hpp:95, spring.cpp:13-37). body_a = -1 anchors r_a in world
+ * space; rest_length < 0 takes the initial distance; fracture applies to its
+ * single row (levels.h:282 sets constraintPoints[0].fracture). Returns force id. */
+int32_t avbd_add_spring(AvbdWorld* w, int32_t body_a, const float r_a[3], int32_t body_b, const float r_b[3],
+                        float stiffness, float rest_length, int32_t is_rope, float fracture);
+/* Joint (force.hpp:119-122, joint.cpp:24-66): 3 positional + 3 angular rows;
+ * stiffness/fracture per row (INFINITY = hard / unbreakable). Returns force id. */
+int32_t avbd_add_joint(AvbdWorld* w, int32_t body_a, const float r_a[3], int32_t body_b, const float r_b[3],
+                       const float stiffness[6], const float fracture[6]);
+/* NeoHookeanFEM (energy.hpp:50-52, neohookeanfem.cpp:5-37). Returns energy id. */
+int32_t avbd_add_neohookean_tet(AvbdWorld* w, const int32_t v[4], float youngs_modulus, float poisson_ratio);
+/* STVKFEM triangle membrane (energy.hpp:90-92, stvkfem.cpp:5-35). Returns energy id. */
+int32_t avbd_add_stvk_tri(AvbdWorld* w, const int32_t v[3], float youngs_modulus, float poisson_ratio);
+/* GeometryHelpers::makeTetVolume (geometry.cpp:30-94): nx*ny*nz particles,
+ * 5 Neo-Hookean tets per hex. Returns the id of the first particle. */
+int32_t avbd_make_tet_volume(AvbdWorld* w, float ox, float oy, float oz, int32_t nx, int32_t ny, int32_t nz,
+                             float cell_size, float youngs_modulus, float poisson_ratio, float particle_mass,
+                             float friction, int32_t pin_min_x);
+
+/* Solver::Step() (solver.cpp:199-627) with the world's params. */
+int32_t avbd_step(AvbdWorld* w);
+/* Sets stepValue/numIterations, then steps. */
+int32_t avbd_step_dt(AvbdWorld* w, float dt, int32_t iterations);
+
+int32_t avbd_num_bodies(const AvbdWorld* w);
+int32_t avbd_num_dynamic_bodies(const AvbdWorld* w);
+/* Solver::emergencyStop (solver.hpp:84). */
+int32_t avbd_emergency_stop(const AvbdWorld* w);
+
+/* Body state by id into caller-owned HOST buffers (any may be NULL):
+ * pos n*3, quat n*4 (w,x,y,z), vel n*3, omega n*3; n = avbd_num_bodies(). */
+int32_t avbd_get_state(AvbdWorld* w, float* pos, float* quat_wxyz, float* vel, float* omega);
+/* Overwrites body state (e.g. to restore a snapshot); NULL leaves a field as is. */
+int32_t avbd_set_state(AvbdWorld* w, const float* pos, const float* quat_wxyz, const float* vel,
+                       const float* omega);
+
+/* Live contact manifolds after the last step (parity introspection).
+ * Returns the count; fills up to max entries: pairs (A,B) body ids, counts,
+ * ids (8 per manifold, unused = 0xFFFFFFFF) and data (8 x 16 floats per
+ * manifold: penetration, normal xyz, rA xyz, rB xyz, penalty x3, lambda x3). */
+int32_t avbd_get_contacts(AvbdWorld* w, int32_t max, int32_t* pairs, int32_t* counts, uint32_t* ids,
+                          float* data);
+/* Colour of each body in the last step (-1 = static); returns the colour count. */
+int32_t avbd_get_colours(AvbdWorld* w, int32_t* colours);
+int32_t avbd_get_timings(const AvbdWorld* w, AvbdTimings* out);
+
+/* CollisionSpace::CollisionBoxBox (collision.cpp:271-447) on two bodies as
+ * they stand, on the device. Fills ids[8], data[8*13] (penetration, normal,
+ * rA, rB, position); returns the contact count. Kernel-level parity check. */
+int32_t avbd_collide(AvbdWorld* w, int32_t body_a, int32_t body_b, uint32_t* ids, float* data);
+
+/* ---------------------------------------------------------------------------
+ * Batched: many independent scenes advanced by one persistent kernel per step
+ * (no reference counterpart; each scene behaves as its own Solver).
+ * ------------------------------------------------------------------------- */
+int32_t avbd_batch_create(const AvbdParams* params, int32_t device, AvbdBatch** out);
+int32_t avbd_batch_destroy(AvbdBatch* b);
+/* Copies the scene staged in `w` (built with the calls above, never stepped)
+ * into the batch. Returns the scene id. Scenes added after the first step are
+ * admitted at the next step. */
+int32_t avbd_batch_add_scene(AvbdBatch* b, const AvbdWorld* w);
+/* Retires a scene and frees its slots for later admissions. */
+int32_t avbd_batch_remove_scene(AvbdBatch* b, int32_t scene);
+/* Advances every live scene by `steps` steps (one persistent kernel launch per
+ * step, replayed from a CUDA graph). Returns AVBD_STATUS_OK or an error. */
+int32_t avbd_batch_step(AvbdBatch* b, int32_t steps);
+int32_t avbd_batch_num_scenes(const AvbdBatch* b);
+int32_t avbd_batch_scene_status(AvbdBatch* b, int32_t scene);
+int32_t avbd_batch_scene_bodies(const AvbdBatch* b, int32_t scene);
+/* Dynamic bodies summed over live scenes (body-iterations per step =
+ * this x num_iterations). */
+int64_t avbd_batch_dynamic_bodies(const AvbdBatch* b);
+/* Poses of one scene into host buffers (pos n*3, quat n*4). */
+int32_t avbd_batch_get_state(AvbdBatch* b, int32_t scene, float* pos, float* quat_wxyz, float* vel,
+                             float* omega);
+/* Poses of all live scenes packed in scene order into one host buffer each. */
+int32_t avbd_batch_get_all_poses(AvbdBatch* b, float* pos, float* quat_wxyz, int64_t max_bodies);
+/* Device bytes a scene staged in `w` needs inside a batch (admission control). */
+int64_t avbd_scene_footprint_bytes(const AvbdWorld* w);
+/* Per-scene counters after the last step: status, colours, candidate pairs,
+ * contact points, incidence entries, steps taken (6 values). */
+int32_t avbd_batch_scene_info(AvbdBatch* b, int32_t scene, int32_t out[6]);
+/* Launch shape of the persistent kernel: threads per CTA and CTAs per SM
+ * (0 = autotuned choice). */
+int32_t avbd_batch_set_launch(AvbdBatch* b, int32_t threads_per_cta, int32_t ctas_per_sm);
+int32_t avbd_batch_get_launch(const AvbdBatch* b, int32_t* threads_per_cta, int32_t* ctas_per_sm);
+/* Device time of the last avbd_batch_step call in ms. */
+float avbd_batch_last_ms(const AvbdBatch* b);
+
+#ifdef __cplusplus
+}
+#endif
+#endif /* AVBD_H */

@@ -1,0 +1,1230 @@
+// C-ABI of the AVBD library (include/avbd.h): device pools, the single-scene
+// launch sequence, the batched persistent kernel, and readback.
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <cmath>
+#include <cstdio>
+#include <cstring>
+#include <memory>
+#include <new>
+#include <vector>
+
+#include "../../include/avbd.h"
+#include "avbd_host.h"
+#include "avbd_step.cuh"
+
+using namespace avbd;
+
+// ===========================================================================
+// Kernels of the single-scene path (grid-wide over the items of scene 0)
+// ===========================================================================
+namespace {
+
+constexpr int kThreads = 128;
+
+__global__ void k_bp_count(World W) {
+    const SceneDesc sc = W.scenes[0];
+    for (int b = sc.body0 + blockIdx.x * blockDim.x + threadIdx.x; b < sc.body0 + sc.nbody;
+         b += gridDim.x * blockDim.x)
+        W.cand_cnt[b] = broadphase_body(W, sc, b, nullptr, 0);
+}
+
+__global__ void k_scan_cand(World W) {
+    const SceneDesc sc = W.scenes[0];
+    const int total = block_exclusive_scan(W.cand_cnt + sc.body0, W.cand_off + sc.body0, sc.nbody);
+    if (threadIdx.x == 0) W.sstate[0].need_cand = total;
+}
+
+__global__ void k_bp_write(World W, int cur) {
+    const SceneDesc sc = W.scenes[0];
+    for (int b = sc.body0 + blockIdx.x * blockDim.x + threadIdx.x; b < sc.body0 + sc.nbody;
+         b += gridDim.x * blockDim.x)
+        broadphase_body(W, sc, b, W.cpair[cur] + sc.cand0 + W.cand_off[b], W.cand_cnt[b]);
+    if (blockIdx.x == 0 && threadIdx.x == 0) { W.sstate[0].kused[cur] = 0; W.sstate[0].need_k = 0; }
+}
+
+__global__ void k_narrow(World W, int cur, int ncand, int old_count) {
+    const SceneDesc sc = W.scenes[0];
+    for (int c = sc.cand0 + blockIdx.x * blockDim.x + threadIdx.x; c < sc.cand0 + ncand;
+         c += gridDim.x * blockDim.x)
+        narrowphase_slot(W, sc, W.sstate, c, cur, old_count);
+}
+
+__global__ void k_force_init(World W) {
+    const SceneDesc sc = W.scenes[0];
+    for (int f = sc.force0 + blockIdx.x * blockDim.x + threadIdx.x; f < sc.force0 + sc.nforce;
+         f += gridDim.x * blockDim.x)
+        force_init(W, f);
+}
+
+__global__ void k_incidence_colour(World W, int cur) {
+    const SceneDesc sc = W.scenes[0];
+    SceneState* st = W.sstate;
+    if (!build_incidence(W, sc, st, cur)) {
+        if (threadIdx.x == 0) st->status = kStatusCapacity;
+        return;
+    }
+    colour_scene(W, sc, st, 0, cur);
+}
+
+__global__ void k_predict(World W) {
+    const SceneDesc sc = W.scenes[0];
+    for (int b = sc.body0 + blockIdx.x * blockDim.x + threadIdx.x; b < sc.body0 + sc.nbody;
+         b += gridDim.x * blockDim.x)
+        predict_body(W, b);
+}
+
+__global__ void k_primal(World W, int cur, int first, int count, float alpha, int write_stick) {
+    const SceneDesc sc = W.scenes[0];
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
+        const int b = W.col_list[sc.body0 + first + i];
+        if (!(W.flags[b] & kBodyRemoved)) primal_body(W, cur, b, alpha, write_stick != 0);
+    }
+}
+
+__global__ void k_dual(World W, int cur, int ncand, float alpha) {
+    const SceneDesc sc = W.scenes[0];
+    const int n = sc.nforce + ncand;
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        if (i < sc.nforce) {
+            if (dual_force(W, sc.force0 + i, alpha)) atomicOr(&W.sstate[0].flags, 8);
+        } else {
+            dual_manifold(W, cur, sc.cand0 + i - sc.nforce, alpha);
+        }
+    }
+}
+
+__global__ void k_fracture_reset(World W, int cur, int ncand) {
+    if (!(W.sstate[0].flags & 8)) return;
+    const SceneDesc sc = W.scenes[0];
+    for (int c = sc.cand0 + blockIdx.x * blockDim.x + threadIdx.x; c < sc.cand0 + ncand; c += gridDim.x * blockDim.x)
+        fracture_reset_slot(W, cur, c);
+}
+
+__global__ void k_fracture_clear(World W) {
+    if (!(W.sstate[0].flags & 8)) return;
+    const SceneDesc sc = W.scenes[0];
+    for (int b = sc.body0 + blockIdx.x * blockDim.x + threadIdx.x; b < sc.body0 + sc.nbody;
+         b += gridDim.x * blockDim.x)
+        W.reset_flag[b] = 0;
+}
+
+__global__ void k_flags_clear(World W, int mask) {
+    if (threadIdx.x == 0) W.sstate[0].flags &= ~mask;
+}
+
+__global__ void k_step_done(World W) {
+    if (threadIdx.x == 0) W.sstate[0].step += 1;
+}
+
+__global__ void k_velocity(World W) {
+    const SceneDesc sc = W.scenes[0];
+    int acc = 0;
+    for (int b = sc.body0 + blockIdx.x * blockDim.x + threadIdx.x; b < sc.body0 + sc.nbody;
+         b += gridDim.x * blockDim.x)
+        acc |= velocity_body(W, b);
+    if (acc) atomicOr(&W.sstate[0].flags, acc);
+}
+
+__global__ void k_remove_oob(World W) {
+    const SceneDesc sc = W.scenes[0];
+    for (int b = sc.body0 + blockIdx.x * blockDim.x + threadIdx.x; b < sc.body0 + sc.nbody;
+         b += gridDim.x * blockDim.x) {
+        const int fl = W.flags[b];
+        if ((fl & (kBodyStatic | kBodyRemoved)) != 0) continue;
+        const float4 p = W.pos[b];
+        if (p.x < kBoundMin || p.x > kBoundMax || p.y < kBoundMin || p.y > kBoundMax || p.z < kBoundMin ||
+            p.z > kBoundMax) {
+            W.flags[b] = fl | kBodyRemoved;
+            for (int e = W.sinc_off[b]; e < W.sinc_off[b + 1]; ++e) {
+                const uint32_t ent = W.sinc[e];
+                const uint32_t k = ent_kind(ent), idx = ent_index(ent);
+                if (k == kEntForce) atomicOr(&W.ftype[idx], kForceRemoved);
+                else if (k == kEntTet) W.tparam[idx].w = 1.f;
+                else if (k == kEntTri) W.rparam[idx].w = 1.f;
+            }
+        }
+    }
+}
+
+__global__ void k_collide(World W, int a, int b, uint32_t* ids, float* data, int* n) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    Collision col;
+    collide_box_box(v3(W.pos[a]), q4(W.rot[a]), v3(W.scale[a]), v3(W.pos[b]), q4(W.rot[b]), v3(W.scale[b]), col);
+    *n = col.n;
+    for (int k = 0; k < col.n; ++k) {
+        const Contact& c = col.c[k];
+        ids[k] = c.id;
+        float* d = data + 13 * k;
+        d[0] = c.penetration;
+        d[1] = c.normal.x; d[2] = c.normal.y; d[3] = c.normal.z;
+        d[4] = c.rA.x; d[5] = c.rA.y; d[6] = c.rA.z;
+        d[7] = c.rB.x; d[8] = c.rB.y; d[9] = c.rB.z;
+        d[10] = c.position.x; d[11] = c.position.y; d[12] = c.position.z;
+    }
+}
+
+// ===========================================================================
+// Batched path: one persistent kernel per step; each CTA pulls scenes from a
+// size-ordered queue and runs a scene's whole step.
+// ===========================================================================
+__global__ void __launch_bounds__(256) k_batch_step(World W, const int* order, int nlive, int* queue) {
+    __shared__ int s_q;
+    for (;;) {
+        if (threadIdx.x == 0) s_q = atomicAdd(queue, 1);
+        __syncthreads();
+        const int q = s_q;
+        __syncthreads();
+        if (q >= nlive) break;
+        scene_step(W, order[q]);
+        __syncthreads();
+    }
+}
+
+int blocks_for(int n, int threads = kThreads) {
+    int b = (n + threads - 1) / threads;
+    return std::max(1, std::min(b, 148 * 32));
+}
+
+}  // namespace
+
+// ===========================================================================
+// Device pools
+// ===========================================================================
+namespace {
+
+struct Pools {
+    World W{};
+    int device = 0;
+    // capacities
+    int nb = 0, nf = 0, nt = 0, nr = 0, ns = 0;
+    int ncand = 0, nk = 0, ninc = 0, nsinc = 0, nsp = 0;
+    std::vector<void*> owned;
+    SceneDesc* d_scenes = nullptr;
+    SceneState* d_sstate = nullptr;
+
+    ~Pools() { release(); }
+    void release() {
+        for (void* p : owned) cudaFree(p);
+        owned.clear();
+        W = World{};
+    }
+    template <typename T>
+    cudaError_t alloc(T*& p, size_t n) {
+        void* q = nullptr;
+        cudaError_t e = cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T));
+        if (e != cudaSuccess) return e;
+        cudaMemset(q, 0, std::max<size_t>(n, 1) * sizeof(T));
+        owned.push_back(q);
+        p = static_cast<T*>(q);
+        return cudaSuccess;
+    }
+    template <typename T>
+    cudaError_t alloc_c(const T*& p, size_t n) {
+        T* q = nullptr;
+        cudaError_t e = alloc(q, n);
+        p = q;
+        return e;
+    }
+    void forget(void* p) {
+        auto it = std::find(owned.begin(), owned.end(), p);
+        if (it != owned.end()) { cudaFree(p); owned.erase(it); }
+    }
+
+    cudaError_t allocate_all() {
+        cudaError_t e = cudaSuccess;
+#define A(expr) if ((e = (expr)) != cudaSuccess) return e
+        A(alloc(d_scenes, ns));
+        A(alloc(d_sstate, ns));
+        W.scenes = d_scenes;
+        W.sstate = d_sstate;
+        W.nscenes = ns;
+        A(alloc(W.pos, nb)); A(alloc(W.rot, nb)); A(alloc(W.scale, nb)); A(alloc(W.lpos, nb));
+        A(alloc(W.lrot, nb)); A(alloc(W.ipos, nb)); A(alloc(W.irot, nb)); A(alloc(W.vel, nb));
+        A(alloc(W.omega, nb)); A(alloc(W.pvel, nb)); A(alloc(W.dlin, nb)); A(alloc(W.dang, nb));
+        A(alloc(W.massI, nb)); A(alloc(W.Mw0, nb)); A(alloc(W.Mw1, nb));
+        A(alloc(W.flags, nb)); A(alloc(W.friction, nb)); A(alloc(W.colour, nb)); A(alloc(W.local, nb));
+        A(alloc(W.reset_flag, nb));
+        A(alloc_c(W.sinc_off, nb + 1)); A(alloc_c(W.sinc_nf, nb)); A(alloc_c(W.sinc, nsinc));
+        A(alloc_c(W.spartner_off, nb + 1)); A(alloc_c(W.spartner, 2 * (size_t)nsp));
+        A(alloc(W.inc_off, nb)); A(alloc(W.inc_cnt, nb)); A(alloc(W.cntB, nb)); A(alloc(W.bcur, nb));
+        A(alloc(W.cand_cnt, nb)); A(alloc(W.cand_off, nb));
+        A(alloc(W.col_list, nb)); A(alloc(W.col_start, (size_t)ns * (kMaxColours + 1)));
+        A(alloc(W.ftype, nf)); A(alloc(W.fbody, nf)); A(alloc(W.frA, nf)); A(alloc(W.frB, nf));
+        A(alloc(W.fq, nf)); A(alloc(W.fparam, nf)); A(alloc(W.fC0p, nf)); A(alloc(W.fC0a, nf));
+        A(alloc(W.fk, 6 * (size_t)nf)); A(alloc(W.ffrac, 6 * (size_t)nf)); A(alloc(W.ffmin, 6 * (size_t)nf));
+        A(alloc(W.ffmax, 6 * (size_t)nf)); A(alloc(W.fpen, 6 * (size_t)nf)); A(alloc(W.flam, 6 * (size_t)nf));
+        A(alloc(W.tidx, nt)); A(alloc(W.tDmInv, 9 * (size_t)nt)); A(alloc(W.tgradN, 12 * (size_t)nt));
+        A(alloc(W.tparam, nt));
+        A(alloc(W.ridx, nr)); A(alloc(W.rDmInv, nr)); A(alloc(W.rgradN, 6 * (size_t)nr)); A(alloc(W.rparam, nr));
+        A(alloc(W.inc, ninc));
+        for (int t = 0; t < 2; ++t) A(alloc_tables(t, ncand, nk));
+#undef A
+        return e;
+    }
+
+    cudaError_t alloc_tables(int t, int nc, int k) {
+        cudaError_t e = cudaSuccess;
+#define A(expr) if ((e = (expr)) != cudaSuccess) return e
+        A(alloc(W.cpair[t], nc)); A(alloc(W.cn[t], nc)); A(alloc(W.cfric[t], nc)); A(alloc(W.kbase[t], nc));
+        A(alloc(W.cbirth[t], nc));
+        A(alloc(W.kid[t], k)); A(alloc(W.krA[t], k)); A(alloc(W.krB[t], k)); A(alloc(W.kn[t], k));
+        A(alloc(W.kt1[t], k)); A(alloc(W.kt2[t], k)); A(alloc(W.krAw[t], k)); A(alloc(W.krBw[t], k));
+        A(alloc(W.kpen[t], k)); A(alloc(W.klam[t], k));
+#undef A
+        return e;
+    }
+
+    template <typename T>
+    cudaError_t grow(T*& p, size_t old_n, size_t new_n, size_t keep) {
+        T* q = nullptr;
+        cudaError_t e = alloc(q, new_n);
+        if (e != cudaSuccess) return e;
+        if (keep) cudaMemcpy(q, p, std::min(keep, old_n) * sizeof(T), cudaMemcpyDeviceToDevice);
+        forget(p);
+        p = q;
+        return cudaSuccess;
+    }
+
+    // Grows the candidate tables of both buffers to nc slots (keeping the
+    // first keep0/keep1 slots) and the contact pools to k slots.
+    cudaError_t grow_tables(int nc, int k, int keep_c0, int keep_c1, int keep_k0, int keep_k1) {
+        cudaError_t e = cudaSuccess;
+        for (int t = 0; t < 2; ++t) {
+            const int kc = t ? keep_c1 : keep_c0, kk = t ? keep_k1 : keep_k0;
+            if (nc > ncand) {
+                if ((e = grow(W.cpair[t], ncand, nc, kc)) != cudaSuccess) return e;
+                if ((e = grow(W.cn[t], ncand, nc, kc)) != cudaSuccess) return e;
+                if ((e = grow(W.cfric[t], ncand, nc, kc)) != cudaSuccess) return e;
+                if ((e = grow(W.kbase[t], ncand, nc, kc)) != cudaSuccess) return e;
+                if ((e = grow(W.cbirth[t], ncand, nc, kc)) != cudaSuccess) return e;
+            }
+            if (k > nk) {
+                if ((e = grow(W.kid[t], nk, k, kk)) != cudaSuccess) return e;
+                if ((e = grow(W.krA[t], nk, k, kk)) != cudaSuccess) return e;
+                if ((e = grow(W.krB[t], nk, k, kk)) != cudaSuccess) return e;
+                if ((e = grow(W.kn[t], nk, k, kk)) != cudaSuccess) return e;
+                if ((e = grow(W.kt1[t], nk, k, kk)) != cudaSuccess) return e;
+                if ((e = grow(W.kt2[t], nk, k, kk)) != cudaSuccess) return e;
+                if ((e = grow(W.krAw[t], nk, k, kk)) != cudaSuccess) return e;
+                if ((e = grow(W.krBw[t], nk, k, kk)) != cudaSuccess) return e;
+                if ((e = grow(W.kpen[t], nk, k, kk)) != cudaSuccess) return e;
+                if ((e = grow(W.klam[t], nk, k, kk)) != cudaSuccess) return e;
+            }
+        }
+        ncand = std::max(ncand, nc);
+        nk = std::max(nk, k);
+        return e;
+    }
+};
+
+// Capacity policy of one scene.
+void scene_caps(const HostScene& h, int& candcap, int& kcap) {
+    const int n = h.nbody();
+    candcap = 8 * n + 64;
+    kcap = 16 * n + 128;
+}
+
+template <typename T>
+void put(T* dst, const std::vector<T>& src, size_t at = 0) {
+    if (!src.empty()) cudaMemcpy(dst + at, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice);
+}
+
+// Packs scenes into freshly allocated pools (state of each scene as staged).
+cudaError_t pack_scenes(Pools& P, const std::vector<const HostScene*>& sc, const std::vector<int>& candcaps,
+                        const std::vector<int>& kcaps, std::vector<SceneDesc>& descs) {
+    P.release();
+    P.ns = (int)sc.size();
+    P.nb = P.nf = P.nt = P.nr = P.ncand = P.nk = P.ninc = 0;
+    descs.resize(sc.size());
+    std::vector<int> soff, snf, poff;
+    std::vector<uint32_t> sent;
+    std::vector<int2> partners;
+    for (size_t i = 0; i < sc.size(); ++i) {
+        const HostScene& h = *sc[i];
+        SceneDesc& d = descs[i];
+        d.body0 = P.nb; d.nbody = h.nbody();
+        d.force0 = P.nf; d.nforce = h.nforce();
+        d.tet0 = P.nt; d.ntet = h.ntet();
+        d.tri0 = P.nr; d.ntri = h.ntri();
+        d.cand0 = P.ncand; d.candcap = candcaps[i];
+        d.k0 = P.nk; d.kcap = kcaps[i];
+        d.ndynamic = h.ndynamic();
+        d.pad = 0;
+        const size_t before = sent.size();
+        h.build_static_incidence(soff, snf, sent, poff, partners, d.body0, d.force0, d.tet0, d.tri0);
+        // static offsets were computed relative to this scene's start of sent
+        for (int b = 0; b < d.nbody; ++b) {
+            soff[d.body0 + b] += 0;   // already global (sent grows monotonically)
+        }
+        d.inc0 = P.ninc;
+        d.inccap = (int)(sent.size() - before) + 2 * d.candcap;
+        P.nb += d.nbody; P.nf += d.nforce; P.nt += d.ntet; P.nr += d.ntri;
+        P.ncand += d.candcap; P.nk += d.kcap; P.ninc += d.inccap;
+    }
+    soff.push_back((int)sent.size());
+    poff.push_back((int)partners.size());
+    P.nsinc = (int)sent.size();
+    P.nsp = (int)partners.size();
+    cudaError_t e = P.allocate_all();
+    if (e != cudaSuccess) return e;
+    World& W = P.W;
+    std::vector<int> local;
+    for (size_t i = 0; i < sc.size(); ++i) {
+        const HostScene& h = *sc[i];
+        const SceneDesc& d = descs[i];
+        put(W.pos, h.pos, d.body0); put(W.rot, h.rot, d.body0); put(W.scale, h.scale, d.body0);
+        put(W.vel, h.vel, d.body0); put(W.omega, h.omega, d.body0); put(W.massI, h.massI, d.body0);
+        put(W.flags, h.flags, d.body0); put(W.friction, h.friction, d.body0);
+        put(W.lpos, h.pos, d.body0); put(W.lrot, h.rot, d.body0);
+        put(W.ipos, h.pos, d.body0); put(W.irot, h.rot, d.body0);
+        local.resize(d.nbody);
+        for (int b = 0; b < d.nbody; ++b) local[b] = b;
+        put(W.local, local, d.body0);
+        // forces: body ids become global
+        std::vector<int2> fb = h.fbody;
+        for (auto& ab : fb) { if (ab.x >= 0) ab.x += d.body0; ab.y += d.body0; }
+        put(W.ftype, h.ftype, d.force0); put(W.fbody, fb, d.force0); put(W.frA, h.frA, d.force0);
+        put(W.frB, h.frB, d.force0); put(W.fq, h.fq, d.force0); put(W.fparam, h.fparam, d.force0);
+        put(W.fk, h.fk, 6 * (size_t)d.force0); put(W.ffrac, h.ffrac, 6 * (size_t)d.force0);
+        put(W.ffmin, h.ffmin, 6 * (size_t)d.force0); put(W.ffmax, h.ffmax, 6 * (size_t)d.force0);
+        std::vector<int4> ti = h.tidx;
+        for (auto& t : ti) { t.x += d.body0; t.y += d.body0; t.z += d.body0; t.w += d.body0; }
+        put(W.tidx, ti, d.tet0); put(W.tDmInv, h.tDmInv, 9 * (size_t)d.tet0);
+        put(W.tgradN, h.tgradN, 12 * (size_t)d.tet0); put(W.tparam, h.tparam, d.tet0);
+        std::vector<int4> ri = h.ridx;
+        for (auto& t : ri) { t.x += d.body0; t.y += d.body0; t.z += d.body0; }
+        put(W.ridx, ri, d.tri0); put(W.rDmInv, h.rDmInv, d.tri0);
+        put(W.rgradN, h.rgradN, 6 * (size_t)d.tri0); put(W.rparam, h.rparam, d.tri0);
+    }
+    cudaMemcpy(const_cast<int*>(W.sinc_off), soff.data(), soff.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if (!snf.empty())
+        cudaMemcpy(const_cast<int*>(W.sinc_nf), snf.data(), snf.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if (!sent.empty())
+        cudaMemcpy(const_cast<uint32_t*>(W.sinc), sent.data(), sent.size() * sizeof(uint32_t), cudaMemcpyHostToDevice);
+    cudaMemcpy(const_cast<int*>(W.spartner_off), poff.data(), poff.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if (!partners.empty())
+        cudaMemcpy(const_cast<int*>(W.spartner), partners.data(), partners.size() * sizeof(int2),
+                   cudaMemcpyHostToDevice);
+    cudaMemcpy(P.d_scenes, descs.data(), descs.size() * sizeof(SceneDesc), cudaMemcpyHostToDevice);
+    std::vector<SceneState> st(sc.size());
+    std::memset(st.data(), 0, st.size() * sizeof(SceneState));
+    cudaMemcpy(P.d_sstate, st.data(), st.size() * sizeof(SceneState), cudaMemcpyHostToDevice);
+    return cudaGetLastError();
+}
+
+Params to_params(const AvbdParams& p) {
+    Params q;
+    q.num_iterations = p.num_iterations;
+    q.dt = p.step_value;
+    q.alpha = p.alpha;
+    q.beta = p.beta;
+    q.gamma = p.gamma;
+    q.on_penetration_penalty = p.on_penetration_penalty;
+    q.post_stabilization = p.post_stabilization;
+    q.projection_mode = p.projection_mode;
+    q.trust_region_rho = p.trust_region_rho;
+    return q;
+}
+
+bool valid_params(const AvbdParams* p) {
+    return p && p->num_iterations >= 0 && p->step_value > 0.f && p->projection_mode >= 0 && p->projection_mode <= 2;
+}
+
+int device_ready(int device) {
+    int n = 0;
+    if (cudaGetDeviceCount(&n) != cudaSuccess || n == 0) return AVBD_ERR_NODEVICE;
+    if (device < 0 || device >= n) return AVBD_ERR_INVALID;
+    return cudaSetDevice(device) == cudaSuccess ? 0 : AVBD_ERR_CUDA;
+}
+
+}  // namespace
+
+// ===========================================================================
+// Single-scene world
+// ===========================================================================
+struct AvbdWorld {
+    AvbdParams params{};
+    int device = 0;
+    HostScene h;
+    bool uploaded = false;
+    bool stopped = false;
+    Pools P;
+    std::vector<SceneDesc> descs;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t ev[8] = {};
+    AvbdTimings timings{};
+    int ncolours = 0;
+    std::vector<int> col_start;
+    SceneState st{};   // host mirror of the scene counters after the last step
+};
+
+namespace {
+
+int sync_state(AvbdWorld* w) {
+    if (cudaMemcpyAsync(&w->st, w->P.d_sstate, sizeof(SceneState), cudaMemcpyDeviceToHost, w->stream) != cudaSuccess)
+        return AVBD_ERR_CUDA;
+    if (cudaStreamSynchronize(w->stream) != cudaSuccess) return AVBD_ERR_CUDA;
+    return 0;
+}
+
+int upload(AvbdWorld* w) {
+    int r = device_ready(w->device);
+    if (r) return r;
+    if (!w->stream) {
+        if (cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking) != cudaSuccess) return AVBD_ERR_CUDA;
+        for (auto& e : w->ev) cudaEventCreate(&e);
+    }
+    int cc, kc;
+    scene_caps(w->h, cc, kc);
+    std::vector<const HostScene*> sc{&w->h};
+    if (pack_scenes(w->P, sc, {cc}, {kc}, w->descs) != cudaSuccess) return AVBD_ERR_NOMEM;
+    w->P.W.P = to_params(w->params);
+    w->uploaded = true;
+    return 0;
+}
+
+// Grows tables of scene 0 so the candidate slots / contacts / incidence fit.
+int ensure_caps(AvbdWorld* w, int need_cand, int need_k) {
+    SceneDesc& d = w->descs[0];
+    bool changed = false;
+    int nc = d.candcap, nk = d.kcap;
+    if (need_cand > nc) { nc = std::max(need_cand + need_cand / 2, 2 * nc); changed = true; }
+    if (need_k > nk) { nk = std::max(need_k + need_k / 2, 2 * nk); changed = true; }
+    if (!changed) return 0;
+    cudaStreamSynchronize(w->stream);
+    SceneState st;
+    cudaMemcpy(&st, w->P.d_sstate, sizeof(SceneState), cudaMemcpyDeviceToHost);
+    if (w->P.grow_tables(nc, nk, st.ncand[0], st.ncand[1], st.kused[0], st.kused[1]) != cudaSuccess)
+        return AVBD_ERR_NOMEM;
+    const int ns = w->P.nsinc;
+    const int inccap = ns + 2 * nc;
+    if (inccap > w->P.ninc) {
+        if (w->P.grow(w->P.W.inc, (size_t)w->P.ninc, (size_t)inccap, 0) != cudaSuccess) return AVBD_ERR_NOMEM;
+        w->P.ninc = inccap;
+    }
+    d.candcap = nc;
+    d.kcap = nk;
+    d.inccap = inccap;
+    cudaMemcpy(w->P.d_scenes, &d, sizeof(SceneDesc), cudaMemcpyHostToDevice);
+    return 0;
+}
+
+float ev_ms(cudaEvent_t a, cudaEvent_t b) {
+    float ms = 0.f;
+    cudaEventElapsedTime(&ms, a, b);
+    return ms;
+}
+
+int world_step(AvbdWorld* w) {
+    if (w->stopped) return AVBD_STATUS_EXPLODED;
+    if (!w->uploaded) {
+        int r = upload(w);
+        if (r) return r;
+    }
+    if (cudaSetDevice(w->device) != cudaSuccess) return AVBD_ERR_CUDA;
+    Pools& P = w->P;
+    P.W.P = to_params(w->params);
+    const SceneDesc& d = w->descs[0];
+    cudaStream_t s = w->stream;
+    int r = sync_state(w);
+    if (r) return r;
+    const int old = w->st.cur, cur = old ^ 1;
+    const int old_count = w->st.ncand[old];
+    cudaEventRecord(w->ev[0], s);
+    // ---- broadphase ----
+    k_bp_count<<<blocks_for(d.nbody), kThreads, 0, s>>>(P.W);
+    k_scan_cand<<<1, 1024, 0, s>>>(P.W);
+    if ((r = sync_state(w))) return r;
+    const int ncand = w->st.need_cand;
+    if ((r = ensure_caps(w, ncand, 0))) return r;
+    k_bp_write<<<blocks_for(d.nbody), kThreads, 0, s>>>(P.W, cur);
+    cudaEventRecord(w->ev[1], s);
+    // ---- narrowphase + manifold warm start (re-run after growing the contact pool) ----
+    for (int attempt = 0; attempt < 4; ++attempt) {
+        k_narrow<<<blocks_for(ncand), kThreads, 0, s>>>(P.W, cur, ncand, old_count);
+        if ((r = sync_state(w))) return r;
+        if (!w->st.need_k) break;
+        if ((r = ensure_caps(w, 0, w->st.kused[cur]))) return r;
+        SceneState fix = w->st;
+        fix.kused[cur] = 0;
+        fix.need_k = 0;
+        cudaMemcpy(P.d_sstate, &fix, sizeof(SceneState), cudaMemcpyHostToDevice);
+    }
+    if (w->st.need_k) return AVBD_STATUS_CAPACITY;
+    {
+        SceneState upd = w->st;
+        upd.ncand[cur] = ncand;
+        upd.cur = cur;
+        upd.status = kStatusOk;
+        upd.flags = 0;
+        cudaMemcpyAsync(P.d_sstate, &upd, sizeof(SceneState), cudaMemcpyHostToDevice, s);
+    }
+    if (d.nforce) k_force_init<<<blocks_for(d.nforce), kThreads, 0, s>>>(P.W);
+    // ---- incidence + colouring (one CTA) ----
+    k_incidence_colour<<<1, 1024, 0, s>>>(P.W, cur);
+    cudaEventRecord(w->ev[2], s);
+    if ((r = sync_state(w))) return r;
+    if (w->st.status != kStatusOk) return w->st.status == kStatusTimeout ? AVBD_STATUS_TIMEOUT : AVBD_STATUS_CAPACITY;
+    const int ncol = w->st.ncolours;
+    w->ncolours = ncol;
+    w->col_start.resize(ncol + 1);
+    cudaMemcpyAsync(w->col_start.data(), P.W.col_start, (ncol + 1) * sizeof(int), cudaMemcpyDeviceToHost, s);
+    cudaStreamSynchronize(s);
+    cudaEventRecord(w->ev[3], s);
+    // ---- prediction ----
+    k_predict<<<blocks_for(d.nbody), kThreads, 0, s>>>(P.W);
+    cudaEventRecord(w->ev[4], s);
+    // ---- iterations ----
+    const float alpha = w->params.alpha;
+    const bool has_fracture = d.nforce > 0;
+    for (int it = 0; it < w->params.num_iterations; ++it) {
+        for (int c = 0; c < ncol; ++c) {
+            const int n = w->col_start[c + 1] - w->col_start[c];
+            if (n > 0) k_primal<<<blocks_for(n), kThreads, 0, s>>>(P.W, cur, w->col_start[c], n, alpha, 0);
+        }
+        if (d.nforce + ncand > 0) k_dual<<<blocks_for(d.nforce + ncand), kThreads, 0, s>>>(P.W, cur, ncand, alpha);
+        if (has_fracture) {
+            k_fracture_reset<<<blocks_for(ncand), kThreads, 0, s>>>(P.W, cur, ncand);
+            k_fracture_clear<<<blocks_for(d.nbody), kThreads, 0, s>>>(P.W);
+            k_flags_clear<<<1, 32, 0, s>>>(P.W, 8);
+        }
+    }
+    cudaEventRecord(w->ev[5], s);
+    // ---- velocities ----
+    k_velocity<<<blocks_for(d.nbody), kThreads, 0, s>>>(P.W);
+    if ((r = sync_state(w))) return r;
+    cudaEventRecord(w->ev[6], s);
+    int status = AVBD_STATUS_OK;
+    if (w->st.flags & 1) status = AVBD_STATUS_EXPLODED;
+    else if (w->st.flags & 2) status = AVBD_STATUS_NAN;
+    if (status != AVBD_STATUS_OK) {
+        w->stopped = true;
+        cudaStreamSynchronize(s);
+        return status;
+    }
+    if (w->st.flags & 4) k_remove_oob<<<blocks_for(d.nbody), kThreads, 0, s>>>(P.W);
+    k_step_done<<<1, 32, 0, s>>>(P.W);
+    // ---- post-stabilisation ----
+    if (w->params.post_stabilization) {
+        for (int c = 0; c < ncol; ++c) {
+            const int n = w->col_start[c + 1] - w->col_start[c];
+            if (n > 0) k_primal<<<blocks_for(n), kThreads, 0, s>>>(P.W, cur, w->col_start[c], n, 0.f, 1);
+        }
+    }
+    cudaEventRecord(w->ev[7], s);
+    if (cudaStreamSynchronize(s) != cudaSuccess) return AVBD_ERR_CUDA;
+    if (cudaGetLastError() != cudaSuccess) return AVBD_ERR_CUDA;
+    AvbdTimings& t = w->timings;
+    t.broad_phase_ms = ev_ms(w->ev[0], w->ev[1]);
+    t.warmstart_ms = ev_ms(w->ev[1], w->ev[2]);
+    t.colouring_ms = 0.f;
+    t.prediction_ms = ev_ms(w->ev[3], w->ev[4]);
+    t.primal_dual_ms = ev_ms(w->ev[4], w->ev[5]);
+    t.velocity_update_ms = ev_ms(w->ev[5], w->ev[6]);
+    t.post_stab_ms = ev_ms(w->ev[6], w->ev[7]);
+    t.total_substep_ms = ev_ms(w->ev[0], w->ev[7]);
+    return AVBD_STATUS_OK;
+}
+
+}  // namespace
+
+// ===========================================================================
+// Batch
+// ===========================================================================
+struct AvbdBatch {
+    AvbdParams params{};
+    int device = 0;
+    std::vector<HostScene> scenes;   // staged copies, by scene id
+    std::vector<int> live;           // 1 = live
+    bool packed = false;
+    Pools P;
+    std::vector<SceneDesc> descs;
+    int* d_order = nullptr;
+    int* d_queue = nullptr;
+    int nlive = 0;
+    cudaStream_t stream = nullptr;
+    cudaEvent_t e0 = nullptr, e1 = nullptr;
+    cudaGraphExec_t graph = nullptr;
+    int threads = 0, ctas_per_sm = 0;   // 0 = automatic
+    int grid = 0;
+    float last_ms = 0.f;
+    std::vector<SceneState> st;
+};
+
+namespace {
+
+void batch_drop_graph(AvbdBatch* b) {
+    if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
+}
+
+int batch_pack(AvbdBatch* b) {
+    int r = device_ready(b->device);
+    if (r) return r;
+    if (!b->stream) {
+        if (cudaStreamCreateWithFlags(&b->stream, cudaStreamNonBlocking) != cudaSuccess) return AVBD_ERR_CUDA;
+        cudaEventCreate(&b->e0);
+        cudaEventCreate(&b->e1);
+    }
+    batch_drop_graph(b);
+    std::vector<const HostScene*> sc;
+    std::vector<int> cc, kc;
+    for (auto& h : b->scenes) {
+        int c, k;
+        scene_caps(h, c, k);
+        sc.push_back(&h);
+        cc.push_back(c);
+        kc.push_back(k);
+    }
+    if (pack_scenes(b->P, sc, cc, kc, b->descs) != cudaSuccess) return AVBD_ERR_NOMEM;
+    b->P.W.P = to_params(b->params);
+    // work queue: live scenes, largest first
+    std::vector<int> order;
+    for (size_t i = 0; i < b->scenes.size(); ++i) if (b->live[i]) order.push_back((int)i);
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        const HostScene& a = b->scenes[x];
+        const HostScene& c = b->scenes[y];
+        return (a.nbody() + a.ntet()) > (c.nbody() + c.ntet());
+    });
+    if (b->d_order) cudaFree(b->d_order);
+    if (b->d_queue) cudaFree(b->d_queue);
+    cudaMalloc(&b->d_order, std::max<size_t>(order.size(), 1) * sizeof(int));
+    cudaMalloc(&b->d_queue, sizeof(int));
+    if (!order.empty())
+        cudaMemcpy(b->d_order, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice);
+    b->nlive = (int)order.size();
+    b->packed = true;
+    return 0;
+}
+
+int batch_launch_shape(AvbdBatch* b) {
+    int threads = b->threads > 0 ? b->threads : 128;
+    int sms = 148;
+    cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
+    int per_sm = 0;
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_step, threads, 0);
+    if (per_sm < 1) per_sm = 1;
+    if (b->ctas_per_sm > 0) per_sm = std::min(per_sm, b->ctas_per_sm);
+    b->threads = threads;
+    b->ctas_per_sm = per_sm;
+    b->grid = sms * per_sm;
+    return 0;
+}
+
+int batch_build_graph(AvbdBatch* b) {
+    batch_drop_graph(b);
+    cudaGraph_t g;
+    if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return AVBD_ERR_CUDA;
+    cudaMemsetAsync(b->d_queue, 0, sizeof(int), b->stream);
+    k_batch_step<<<b->grid, b->threads, 0, b->stream>>>(b->P.W, b->d_order, b->nlive, b->d_queue);
+    if (cudaStreamEndCapture(b->stream, &g) != cudaSuccess) return AVBD_ERR_CUDA;
+    cudaError_t e = cudaGraphInstantiate(&b->graph, g, 0);
+    cudaGraphDestroy(g);
+    return e == cudaSuccess ? 0 : AVBD_ERR_CUDA;
+}
+
+}  // namespace
+
+// ===========================================================================
+// C-ABI
+// ===========================================================================
+extern "C" {
+
+void avbd_default_params(AvbdParams* p) {
+    if (!p) return;
+    p->num_iterations = 10;
+    p->step_value = 1.0f / 60.0f;
+    p->alpha = 0.95f;
+    p->beta = 100000.0f;
+    p->gamma = 0.99f;
+    p->on_penetration_penalty = 0.f;
+    p->post_stabilization = 1;
+    p->projection_mode = AVBD_PROJECT_ABSOLUTE;
+    p->trust_region_rho = 0.f;
+}
+
+const char* avbd_status_string(int32_t code) {
+    switch (code) {
+        case AVBD_STATUS_OK: return "ok";
+        case AVBD_STATUS_EXPLODED: return "exploded";
+        case AVBD_STATUS_NAN: return "nan";
+        case AVBD_STATUS_CAPACITY: return "capacity";
+        case AVBD_STATUS_TIMEOUT: return "timeout";
+        case AVBD_ERR_INVALID: return "invalid argument";
+        case AVBD_ERR_CUDA: return "cuda error";
+        case AVBD_ERR_NOMEM: return "out of memory";
+        case AVBD_ERR_STATE: return "invalid state";
+        case AVBD_ERR_NODEVICE: return "no cuda device";
+        default: return "unknown";
+    }
+}
+
+int32_t avbd_world_create(const AvbdParams* params, int32_t device, AvbdWorld** out) {
+    if (!out) return AVBD_ERR_INVALID;
+    AvbdParams p;
+    avbd_default_params(&p);
+    if (params) {
+        if (!valid_params(params)) return AVBD_ERR_INVALID;
+        p = *params;
+    }
+    int r = device_ready(device);
+    if (r) return r;
+    AvbdWorld* w = new (std::nothrow) AvbdWorld();
+    if (!w) return AVBD_ERR_NOMEM;
+    w->params = p;
+    w->device = device;
+    *out = w;
+    return 0;
+}
+
+int32_t avbd_world_destroy(AvbdWorld* w) {
+    if (!w) return AVBD_ERR_INVALID;
+    cudaSetDevice(w->device);
+    if (w->stream) {
+        cudaStreamSynchronize(w->stream);
+        for (auto& e : w->ev) cudaEventDestroy(e);
+        cudaStreamDestroy(w->stream);
+    }
+    delete w;
+    return 0;
+}
+
+int32_t avbd_world_clear(AvbdWorld* w) {
+    if (!w) return AVBD_ERR_INVALID;
+    w->h.clear();
+    w->P.release();
+    w->uploaded = false;
+    w->stopped = false;
+    return 0;
+}
+
+int32_t avbd_set_params(AvbdWorld* w, const AvbdParams* p) {
+    if (!w || !valid_params(p)) return AVBD_ERR_INVALID;
+    w->params = *p;
+    return 0;
+}
+
+int32_t avbd_get_params(const AvbdWorld* w, AvbdParams* out) {
+    if (!w || !out) return AVBD_ERR_INVALID;
+    *out = w->params;
+    return 0;
+}
+
+#define AVBD_STAGING_ONLY(w) \
+    if (!(w)) return AVBD_ERR_INVALID; \
+    if ((w)->uploaded) return AVBD_ERR_STATE;
+
+int32_t avbd_add_body(AvbdWorld* w, int32_t model, float density, float friction, const float pos[3],
+                      const float scale[3], const float vel[3], const float quat[4], const float omega[3],
+                      int32_t is_static) {
+    AVBD_STAGING_ONLY(w);
+    if (!pos || !scale || !vel || !quat || !omega || model < 0 || model > 2) return AVBD_ERR_INVALID;
+    return w->h.add_body(model, density, friction, pos, scale, vel, quat, omega, is_static != 0);
+}
+
+int32_t avbd_add_particle(AvbdWorld* w, float mass, float friction, const float pos[3], const float vel[3],
+                          int32_t is_static) {
+    AVBD_STAGING_ONLY(w);
+    if (!pos || !vel) return AVBD_ERR_INVALID;
+    return w->h.add_particle(mass, friction, pos, vel, is_static != 0);
+}
+
+int32_t avbd_set_body_static(AvbdWorld* w, int32_t body, int32_t is_static) {
+    AVBD_STAGING_ONLY(w);
+    return w->h.set_static(body, is_static != 0) ? AVBD_ERR_INVALID : 0;
+}
+
+int32_t avbd_add_spring(AvbdWorld* w, int32_t a, const float rA[3], int32_t b, const float rB[3], float k,
+                        float rest, int32_t is_rope, float fracture) {
+    AVBD_STAGING_ONLY(w);
+    if (!rA || !rB) return AVBD_ERR_INVALID;
+    int r = w->h.add_spring(a, rA, b, rB, k, rest, is_rope != 0, fracture);
+    return r < 0 ? AVBD_ERR_INVALID : r;
+}
+
+int32_t avbd_add_joint(AvbdWorld* w, int32_t a, const float rA[3], int32_t b, const float rB[3],
+                       const float stiffness[6], const float fracture[6]) {
+    AVBD_STAGING_ONLY(w);
+    if (!rA || !rB || !stiffness || !fracture) return AVBD_ERR_INVALID;
+    int r = w->h.add_joint(a, rA, b, rB, stiffness, fracture);
+    return r < 0 ? AVBD_ERR_INVALID : r;
+}
+
+int32_t avbd_add_neohookean_tet(AvbdWorld* w, const int32_t v[4], float E, float nu) {
+    AVBD_STAGING_ONLY(w);
+    if (!v) return AVBD_ERR_INVALID;
+    int r = w->h.add_nh_tet(v, E, nu);
+    return r < 0 ? AVBD_ERR_INVALID : r;
+}
+
+int32_t avbd_add_stvk_tri(AvbdWorld* w, const int32_t v[3], float E, float nu) {
+    AVBD_STAGING_ONLY(w);
+    if (!v) return AVBD_ERR_INVALID;
+    int r = w->h.add_stvk_tri(v, E, nu);
+    return r < 0 ? AVBD_ERR_INVALID : r;
+}
+
+int32_t avbd_make_tet_volume(AvbdWorld* w, float ox, float oy, float oz, int32_t nx, int32_t ny, int32_t nz,
+                             float cell, float E, float nu, float pm, float friction, int32_t pin) {
+    AVBD_STAGING_ONLY(w);
+    int r = w->h.make_tet_volume(ox, oy, oz, nx, ny, nz, cell, E, nu, pm, friction, pin != 0);
+    return r < 0 ? AVBD_ERR_INVALID : r;
+}
+
+int32_t avbd_step(AvbdWorld* w) {
+    if (!w) return AVBD_ERR_INVALID;
+    return world_step(w);
+}
+
+int32_t avbd_step_dt(AvbdWorld* w, float dt, int32_t iterations) {
+    if (!w || !(dt > 0.f) || iterations < 0) return AVBD_ERR_INVALID;
+    w->params.step_value = dt;
+    w->params.num_iterations = iterations;
+    return world_step(w);
+}
+
+int32_t avbd_num_bodies(const AvbdWorld* w) { return w ? w->h.nbody() : AVBD_ERR_INVALID; }
+int32_t avbd_num_dynamic_bodies(const AvbdWorld* w) { return w ? w->h.ndynamic() : AVBD_ERR_INVALID; }
+int32_t avbd_emergency_stop(const AvbdWorld* w) { return w ? (w->stopped ? 1 : 0) : AVBD_ERR_INVALID; }
+
+int32_t avbd_get_state(AvbdWorld* w, float* pos, float* quat, float* vel, float* omega) {
+    if (!w) return AVBD_ERR_INVALID;
+    const int n = w->h.nbody();
+    if (!w->uploaded) {
+        for (int i = 0; i < n; ++i) {
+            const float4 p = w->h.pos[i], q = w->h.rot[i], v = w->h.vel[i], o = w->h.omega[i];
+            if (pos) { pos[3 * i] = p.x; pos[3 * i + 1] = p.y; pos[3 * i + 2] = p.z; }
+            if (quat) { quat[4 * i] = q.w; quat[4 * i + 1] = q.x; quat[4 * i + 2] = q.y; quat[4 * i + 3] = q.z; }
+            if (vel) { vel[3 * i] = v.x; vel[3 * i + 1] = v.y; vel[3 * i + 2] = v.z; }
+            if (omega) { omega[3 * i] = o.x; omega[3 * i + 1] = o.y; omega[3 * i + 2] = o.z; }
+        }
+        return n;
+    }
+    cudaSetDevice(w->device);
+    std::vector<float4> buf(n);
+    const World& W = w->P.W;
+    auto fetch = [&](const float4* src, float* dst, int comps, bool quat_order) -> int {
+        if (!dst) return 0;
+        if (cudaMemcpy(buf.data(), src, n * sizeof(float4), cudaMemcpyDeviceToHost) != cudaSuccess) return -1;
+        for (int i = 0; i < n; ++i) {
+            const float4 x = buf[i];
+            if (quat_order) { dst[4 * i] = x.w; dst[4 * i + 1] = x.x; dst[4 * i + 2] = x.y; dst[4 * i + 3] = x.z; }
+            else { dst[comps * i] = x.x; dst[comps * i + 1] = x.y; dst[comps * i + 2] = x.z; }
+        }
+        return 0;
+    };
+    if (fetch(W.pos, pos, 3, false) || fetch(W.rot, quat, 4, true) || fetch(W.vel, vel, 3, false) ||
+        fetch(W.omega, omega, 3, false))
+        return AVBD_ERR_CUDA;
+    return n;
+}
+
+int32_t avbd_set_state(AvbdWorld* w, const float* pos, const float* quat, const float* vel, const float* omega) {
+    if (!w) return AVBD_ERR_INVALID;
+    const int n = w->h.nbody();
+    for (int i = 0; i < n; ++i) {
+        if (pos) { w->h.pos[i].x = pos[3 * i]; w->h.pos[i].y = pos[3 * i + 1]; w->h.pos[i].z = pos[3 * i + 2]; }
+        if (quat) {
+            w->h.rot[i].w = quat[4 * i]; w->h.rot[i].x = quat[4 * i + 1];
+            w->h.rot[i].y = quat[4 * i + 2]; w->h.rot[i].z = quat[4 * i + 3];
+        }
+        if (vel) { w->h.vel[i].x = vel[3 * i]; w->h.vel[i].y = vel[3 * i + 1]; w->h.vel[i].z = vel[3 * i + 2]; }
+        if (omega) {
+            w->h.omega[i].x = omega[3 * i]; w->h.omega[i].y = omega[3 * i + 1]; w->h.omega[i].z = omega[3 * i + 2];
+        }
+    }
+    if (w->uploaded) {
+        cudaSetDevice(w->device);
+        const World& W = w->P.W;
+        if (pos) cudaMemcpy(W.pos, w->h.pos.data(), n * sizeof(float4), cudaMemcpyHostToDevice);
+        if (quat) cudaMemcpy(W.rot, w->h.rot.data(), n * sizeof(float4), cudaMemcpyHostToDevice);
+        if (vel) cudaMemcpy(W.vel, w->h.vel.data(), n * sizeof(float4), cudaMemcpyHostToDevice);
+        if (omega) cudaMemcpy(W.omega, w->h.omega.data(), n * sizeof(float4), cudaMemcpyHostToDevice);
+    }
+    return 0;
+}
+
+int32_t avbd_get_contacts(AvbdWorld* w, int32_t max, int32_t* pairs, int32_t* counts, uint32_t* ids, float* data) {
+    if (!w) return AVBD_ERR_INVALID;
+    if (!w->uploaded) return 0;
+    cudaSetDevice(w->device);
+    SceneState st;
+    cudaMemcpy(&st, w->P.d_sstate, sizeof(SceneState), cudaMemcpyDeviceToHost);
+    const int cur = st.cur, nc = st.ncand[cur];
+    const World& W = w->P.W;
+    std::vector<int2> cp(nc);
+    std::vector<int> cn(nc), kb(nc);
+    cudaMemcpy(cp.data(), W.cpair[cur], nc * sizeof(int2), cudaMemcpyDeviceToHost);
+    cudaMemcpy(cn.data(), W.cn[cur], nc * sizeof(int), cudaMemcpyDeviceToHost);
+    cudaMemcpy(kb.data(), W.kbase[cur], nc * sizeof(int), cudaMemcpyDeviceToHost);
+    const int nk = st.kused[cur];
+    std::vector<uint32_t> kid(nk);
+    std::vector<float4> rA(nk), rB(nk), kn(nk), pen(nk), lam(nk);
+    if (nk > 0) {
+        cudaMemcpy(kid.data(), W.kid[cur], nk * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+        cudaMemcpy(rA.data(), W.krA[cur], nk * sizeof(float4), cudaMemcpyDeviceToHost);
+        cudaMemcpy(rB.data(), W.krB[cur], nk * sizeof(float4), cudaMemcpyDeviceToHost);
+        cudaMemcpy(kn.data(), W.kn[cur], nk * sizeof(float4), cudaMemcpyDeviceToHost);
+        cudaMemcpy(pen.data(), W.kpen[cur], nk * sizeof(float4), cudaMemcpyDeviceToHost);
+        cudaMemcpy(lam.data(), W.klam[cur], nk * sizeof(float4), cudaMemcpyDeviceToHost);
+    }
+    int m = 0;
+    for (int c = 0; c < nc; ++c) {
+        if (cn[c] == 0) continue;
+        if (m < max) {
+            if (pairs) { pairs[2 * m] = cp[c].x; pairs[2 * m + 1] = cp[c].y; }
+            if (counts) counts[m] = cn[c];
+            for (int k = 0; k < 8; ++k) {
+                if (ids) ids[8 * m + k] = k < cn[c] ? kid[kb[c] + k] : 0xFFFFFFFFu;
+                if (data) {
+                    float* d = data + (size_t)(8 * m + k) * 16;
+                    std::memset(d, 0, 16 * sizeof(float));
+                    if (k < cn[c]) {
+                        const int o = kb[c] + k;
+                        d[0] = rA[o].w;
+                        d[1] = -kn[o].x; d[2] = -kn[o].y; d[3] = -kn[o].z;
+                        d[4] = rA[o].x; d[5] = rA[o].y; d[6] = rA[o].z;
+                        d[7] = rB[o].x; d[8] = rB[o].y; d[9] = rB[o].z;
+                        d[10] = pen[o].x; d[11] = pen[o].y; d[12] = pen[o].z;
+                        d[13] = lam[o].x; d[14] = lam[o].y; d[15] = lam[o].z;
+                    }
+                }
+            }
+        }
+        ++m;
+    }
+    return m;
+}
+
+int32_t avbd_get_colours(AvbdWorld* w, int32_t* colours) {
+    if (!w || !colours) return AVBD_ERR_INVALID;
+    const int n = w->h.nbody();
+    if (!w->uploaded) {
+        for (int i = 0; i < n; ++i) colours[i] = -1;
+        return 0;
+    }
+    cudaSetDevice(w->device);
+    cudaMemcpy(colours, w->P.W.colour, n * sizeof(int), cudaMemcpyDeviceToHost);
+    for (int i = 0; i < n; ++i) if (colours[i] < 0) colours[i] = -1;
+    return w->ncolours;
+}
+
+int32_t avbd_get_timings(const AvbdWorld* w, AvbdTimings* out) {
+    if (!w || !out) return AVBD_ERR_INVALID;
+    *out = w->timings;
+    return 0;
+}
+
+int32_t avbd_collide(AvbdWorld* w, int32_t a, int32_t b, uint32_t* ids, float* data) {
+    if (!w || a < 0 || b < 0 || a >= w->h.nbody() || b >= w->h.nbody()) return AVBD_ERR_INVALID;
+    if (!w->uploaded) {
+        int r = upload(w);
+        if (r) return r;
+    }
+    cudaSetDevice(w->device);
+    uint32_t* d_ids = nullptr;
+    float* d_data = nullptr;
+    int* d_n = nullptr;
+    cudaMalloc(&d_ids, 8 * sizeof(uint32_t));
+    cudaMalloc(&d_data, 8 * 13 * sizeof(float));
+    cudaMalloc(&d_n, sizeof(int));
+    k_collide<<<1, 32, 0, w->stream>>>(w->P.W, a, b, d_ids, d_data, d_n);
+    int n = 0;
+    cudaStreamSynchronize(w->stream);
+    cudaMemcpy(&n, d_n, sizeof(int), cudaMemcpyDeviceToHost);
+    if (ids) cudaMemcpy(ids, d_ids, 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost);
+    if (data) cudaMemcpy(data, d_data, 8 * 13 * sizeof(float), cudaMemcpyDeviceToHost);
+    cudaFree(d_ids);
+    cudaFree(d_data);
+    cudaFree(d_n);
+    return cudaGetLastError() == cudaSuccess ? n : AVBD_ERR_CUDA;
+}
+
+// ---------------------------------------------------------------------------
+// Batch
+// ---------------------------------------------------------------------------
+int32_t avbd_batch_create(const AvbdParams* params, int32_t device, AvbdBatch** out) {
+    if (!out) return AVBD_ERR_INVALID;
+    AvbdParams p;
+    avbd_default_params(&p);
+    if (params) {
+        if (!valid_params(params)) return AVBD_ERR_INVALID;
+        p = *params;
+    }
+    int r = device_ready(device);
+    if (r) return r;
+    AvbdBatch* b = new (std::nothrow) AvbdBatch();
+    if (!b) return AVBD_ERR_NOMEM;
+    b->params = p;
+    b->device = device;
+    *out = b;
+    return 0;
+}
+
+int32_t avbd_batch_destroy(AvbdBatch* b) {
+    if (!b) return AVBD_ERR_INVALID;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    batch_drop_graph(b);
+    if (b->d_order) cudaFree(b->d_order);
+    if (b->d_queue) cudaFree(b->d_queue);
+    if (b->e0) cudaEventDestroy(b->e0);
+    if (b->e1) cudaEventDestroy(b->e1);
+    if (b->stream) cudaStreamDestroy(b->stream);
+    delete b;
+    return 0;
+}
+
+int32_t avbd_batch_add_scene(AvbdBatch* b, const AvbdWorld* w) {
+    if (!b || !w) return AVBD_ERR_INVALID;
+    if (b->packed) return AVBD_ERR_STATE;
+    b->scenes.push_back(w->h);
+    b->live.push_back(1);
+    return (int)b->scenes.size() - 1;
+}
+
+int32_t avbd_batch_remove_scene(AvbdBatch* b, int32_t scene) {
+    if (!b || scene < 0 || scene >= (int)b->scenes.size()) return AVBD_ERR_INVALID;
+    b->live[scene] = 0;
+    if (b->packed) {
+        // drop it from the work queue; its pool regions stay reserved until the batch is rebuilt
+        std::vector<int> order;
+        for (size_t i = 0; i < b->scenes.size(); ++i) if (b->live[i]) order.push_back((int)i);
+        std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+            return (b->scenes[x].nbody() + b->scenes[x].ntet()) > (b->scenes[y].nbody() + b->scenes[y].ntet());
+        });
+        cudaSetDevice(b->device);
+        if (!order.empty())
+            cudaMemcpy(b->d_order, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice);
+        b->nlive = (int)order.size();
+        batch_drop_graph(b);
+    }
+    return 0;
+}
+
+int32_t avbd_batch_step(AvbdBatch* b, int32_t steps) {
+    if (!b || steps < 0) return AVBD_ERR_INVALID;
+    int r;
+    if (!b->packed && (r = batch_pack(b))) return r;
+    cudaSetDevice(b->device);
+    if (!b->grid) batch_launch_shape(b);
+    b->P.W.P = to_params(b->params);
+    if (!b->graph && (r = batch_build_graph(b))) return r;
+    cudaEventRecord(b->e0, b->stream);
+    for (int i = 0; i < steps; ++i)
+        if (cudaGraphLaunch(b->graph, b->stream) != cudaSuccess) return AVBD_ERR_CUDA;
+    cudaEventRecord(b->e1, b->stream);
+    if (cudaStreamSynchronize(b->stream) != cudaSuccess) return AVBD_ERR_CUDA;
+    cudaEventElapsedTime(&b->last_ms, b->e0, b->e1);
+    return cudaGetLastError() == cudaSuccess ? AVBD_STATUS_OK : AVBD_ERR_CUDA;
+}
+
+int32_t avbd_batch_num_scenes(const AvbdBatch* b) { return b ? (int)b->scenes.size() : AVBD_ERR_INVALID; }
+
+int32_t avbd_batch_scene_status(AvbdBatch* b, int32_t scene) {
+    if (!b || scene < 0 || scene >= (int)b->scenes.size()) return AVBD_ERR_INVALID;
+    if (!b->packed) return AVBD_STATUS_OK;
+    cudaSetDevice(b->device);
+    SceneState st;
+    if (cudaMemcpy(&st, b->P.d_sstate + scene, sizeof(SceneState), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return AVBD_ERR_CUDA;
+    return st.status;
+}
+
+int32_t avbd_batch_scene_info(AvbdBatch* b, int32_t scene, int32_t out[6]) {
+    if (!b || !out || scene < 0 || scene >= (int)b->scenes.size()) return AVBD_ERR_INVALID;
+    if (!b->packed) { for (int i = 0; i < 6; ++i) out[i] = 0; return 0; }
+    cudaSetDevice(b->device);
+    SceneState st;
+    if (cudaMemcpy(&st, b->P.d_sstate + scene, sizeof(SceneState), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return AVBD_ERR_CUDA;
+    out[0] = st.status; out[1] = st.ncolours; out[2] = st.ncand[st.cur]; out[3] = st.kused[st.cur];
+    out[4] = st.ninc; out[5] = st.step;
+    return 0;
+}
+
+int32_t avbd_batch_scene_bodies(const AvbdBatch* b, int32_t scene) {
+    if (!b || scene < 0 || scene >= (int)b->scenes.size()) return AVBD_ERR_INVALID;
+    return b->scenes[scene].nbody();
+}
+
+int64_t avbd_batch_dynamic_bodies(const AvbdBatch* b) {
+    if (!b) return AVBD_ERR_INVALID;
+    int64_t n = 0;
+    for (size_t i = 0; i < b->scenes.size(); ++i)
+        if (b->live[i]) n += b->scenes[i].ndynamic();
+    return n;
+}
+
+int32_t avbd_batch_get_state(AvbdBatch* b, int32_t scene, float* pos, float* quat, float* vel, float* omega) {
+    if (!b || scene < 0 || scene >= (int)b->scenes.size()) return AVBD_ERR_INVALID;
+    const HostScene& h = b->scenes[scene];
+    const int n = h.nbody();
+    if (!b->packed) return 0;
+    cudaSetDevice(b->device);
+    const int b0 = b->descs[scene].body0;
+    std::vector<float4> buf(n);
+    const World& W = b->P.W;
+    auto fetch = [&](const float4* src, float* dst, bool q) {
+        if (!dst) return;
+        cudaMemcpy(buf.data(), src + b0, n * sizeof(float4), cudaMemcpyDeviceToHost);
+        for (int i = 0; i < n; ++i) {
+            const float4 x = buf[i];
+            if (q) { dst[4 * i] = x.w; dst[4 * i + 1] = x.x; dst[4 * i + 2] = x.y; dst[4 * i + 3] = x.z; }
+            else { dst[3 * i] = x.x; dst[3 * i + 1] = x.y; dst[3 * i + 2] = x.z; }
+        }
+    };
+    fetch(W.pos, pos, false);
+    fetch(W.rot, quat, true);
+    fetch(W.vel, vel, false);
+    fetch(W.omega, omega, false);
+    return n;
+}
+
+int32_t avbd_batch_get_all_poses(AvbdBatch* b, float* pos, float* quat, int64_t max_bodies) {
+    if (!b || !b->packed) return AVBD_ERR_STATE;
+    cudaSetDevice(b->device);
+    const int n = b->P.nb;
+    if (n > max_bodies) return AVBD_ERR_INVALID;
+    const World& W = b->P.W;
+    if (pos && cudaMemcpyAsync(pos, W.pos, n * sizeof(float4), cudaMemcpyDeviceToHost, b->stream) != cudaSuccess)
+        return AVBD_ERR_CUDA;
+    if (quat && cudaMemcpyAsync(quat, W.rot, n * sizeof(float4), cudaMemcpyDeviceToHost, b->stream) != cudaSuccess)
+        return AVBD_ERR_CUDA;
+    if (cudaStreamSynchronize(b->stream) != cudaSuccess) return AVBD_ERR_CUDA;
+    return n;
+}
+
+int64_t avbd_scene_footprint_bytes(const AvbdWorld* w) {
+    if (!w) return AVBD_ERR_INVALID;
+    int cc, kc;
+    scene_caps(w->h, cc, kc);
+    const int64_t nb = w->h.nbody();
+    int64_t bytes = nb * (16 * 15 + 4 * 16);
+    bytes += (int64_t)w->h.nforce() * (16 * 8 + 4 * 36 + 8);
+    bytes += (int64_t)w->h.ntet() * (16 + 36 + 48 + 16) + (int64_t)w->h.ntri() * (16 + 16 + 24 + 16);
+    bytes += 2 * (int64_t)cc * (8 + 4 + 4 + 4) + 2 * (int64_t)kc * (4 + 16 * 9);
+    bytes += 4 * (int64_t)(2 * cc + 8 * nb);
+    return bytes;
+}
+
+int32_t avbd_batch_set_launch(AvbdBatch* b, int32_t threads, int32_t ctas_per_sm) {
+    if (!b || threads < 0 || ctas_per_sm < 0 || (threads && (threads % 32 || threads > 256))) return AVBD_ERR_INVALID;
+    b->threads = threads;
+    b->ctas_per_sm = ctas_per_sm;
+    b->grid = 0;
+    batch_drop_graph(b);
+    return 0;
+}
+
+int32_t avbd_batch_get_launch(const AvbdBatch* b, int32_t* threads, int32_t* ctas_per_sm) {
+    if (!b) return AVBD_ERR_INVALID;
+    if (threads) *threads = b->threads;
+    if (ctas_per_sm) *ctas_per_sm = b->ctas_per_sm;
+    return 0;
+}
+
+float avbd_batch_last_ms(const AvbdBatch* b) { return b ? b->last_ms : -1.f; }
+
+}  // extern "C"

@@ -1,0 +1,337 @@
+// Per-(vertex, element) energy terms of the FEM energies, in registers:
+//   * Neo-Hookean tet: SkyePhyX src/physics/neohookeanfem.cpp:40-110 with
+//     NeoHookeanMath (src/helpers/math.cpp:10-231);
+//   * StVK triangle membrane: src/physics/stvkfem.cpp:38-86 with STVKMath
+//     (src/helpers/math.cpp:234-357).
+// The 3x3 SVD is one-sided (Hestenes) Jacobi and the symmetric eigenproblem
+// cyclic Jacobi (Golub & Van Loan, "Matrix Computations", 8.4-8.6); both
+// produce the decompositions the reference asks Eigen for (sorted singular
+// values, rotation-signed U/V; ascending eigenvalues).  The projected Hessian
+// is a spectral function, so it does not depend on the basis each solver picks.
+#pragma once
+#include "avbd_common.cuh"
+
+namespace avbd {
+
+AVBD_HD float det3(const M3& m) {
+    // first-column cofactor expansion
+    return m3(m, 0, 0) * (m3(m, 1, 1) * m3(m, 2, 2) - m3(m, 1, 2) * m3(m, 2, 1)) -
+           m3(m, 1, 0) * (m3(m, 0, 1) * m3(m, 2, 2) - m3(m, 0, 2) * m3(m, 2, 1)) +
+           m3(m, 2, 0) * (m3(m, 0, 1) * m3(m, 1, 2) - m3(m, 0, 2) * m3(m, 1, 1));
+}
+
+AVBD_HD void jacobi_cs(float app, float aqq, float apq, float& c, float& s) {
+    float tau = (aqq - app) / (2.f * apq);
+    float t = (tau >= 0.f ? 1.f : -1.f) / (fabsf(tau) + sqrtf(1.f + tau * tau));
+    c = 1.f / sqrtf(1.f + t * t);
+    s = t * c;
+}
+
+AVBD_HD void rot_cols(V3& a, V3& b, float c, float s) {
+    V3 na = c * a - s * b;
+    V3 nb = s * a + c * b;
+    a = na;
+    b = nb;
+}
+
+AVBD_HD void swap3(V3& a, V3& b) { V3 t = a; a = b; b = t; }
+AVBD_HD void swapf(float& a, float& b) { float t = a; a = b; b = t; }
+
+// F = U diag(S) V^T, S sorted decreasing, U and V rotations after the sign
+// fix of NeoHookeanMath::svd (math.cpp:13-35).
+AVBD_HD void svd3(const M3& F, M3& U, V3& S, M3& V) {
+    V3 a0 = F.c[0], a1 = F.c[1], a2 = F.c[2];
+    V3 v0 = v3(1, 0, 0), v1 = v3(0, 1, 0), v2 = v3(0, 0, 1);
+    const float eps = 1.1920929e-07f;
+    for (int sweep = 0; sweep < 64; ++sweep) {
+        bool rotated = false;
+#define AVBD_SVD_PAIR(ap, aq, vp, vq)                                           \
+        {                                                                       \
+            float al = sqnorm(ap), be = sqnorm(aq), ga = dot(ap, aq);           \
+            if (!(ga == 0.f || fabsf(ga) <= eps * sqrtf(al * be))) {            \
+                float c, s;                                                     \
+                jacobi_cs(al, be, ga, c, s);                                    \
+                rot_cols(ap, aq, c, s);                                         \
+                rot_cols(vp, vq, c, s);                                         \
+                rotated = true;                                                 \
+            }                                                                   \
+        }
+        AVBD_SVD_PAIR(a0, a1, v0, v1)
+        AVBD_SVD_PAIR(a0, a2, v0, v2)
+        AVBD_SVD_PAIR(a1, a2, v1, v2)
+#undef AVBD_SVD_PAIR
+        if (!rotated) break;
+    }
+    float s0 = norm(a0), s1 = norm(a1), s2 = norm(a2);
+    // stable sort by decreasing singular value (bubble network)
+    if (s0 < s1) { swapf(s0, s1); swap3(a0, a1); swap3(v0, v1); }
+    if (s1 < s2) { swapf(s1, s2); swap3(a1, a2); swap3(v1, v2); }
+    if (s0 < s1) { swapf(s0, s1); swap3(a0, a1); swap3(v0, v1); }
+    const float tiny = 1.17549435e-38f;
+    V3 u0 = s0 > tiny ? a0 / s0 : v3(1, 0, 0);
+    V3 u1 = s1 > tiny ? a1 / s1 : v3(0, 1, 0);
+    V3 u2 = s2 > tiny ? a2 / s2 : cross(u0, u1);
+    U.c[0] = u0; U.c[1] = u1; U.c[2] = u2;
+    V.c[0] = v0; V.c[1] = v1; V.c[2] = v2;
+    S = v3(s0, s1, s2);
+    if (det3(U) < 0.f) { U.c[2] = -U.c[2]; S.z = -S.z; }
+    if (det3(V) < 0.f) { V.c[2] = -V.c[2]; S.z = -S.z; }
+}
+
+// Symmetric 3x3 eigen-decomposition, eigenvalues increasing (cyclic Jacobi).
+// A given by its entries; eigenvectors returned as columns of Q.
+AVBD_HD void eig3(float a00, float a11, float a22, float a01, float a02, float a12, V3& w, M3& Q) {
+    float A[3][3] = {{a00, a01, a02}, {a01, a11, a12}, {a02, a12, a22}};
+    float Vm[3][3] = {{1, 0, 0}, {0, 1, 0}, {0, 0, 1}};
+    const float eps = 1.1920929e-07f;
+    for (int sweep = 0; sweep < 64; ++sweep) {
+        bool rotated = false;
+#pragma unroll
+        for (int pq = 0; pq < 3; ++pq) {
+            const int p = pq == 2 ? 1 : 0;
+            const int q = pq == 0 ? 1 : 2;
+            float apq = A[p][q];
+            if (apq == 0.f) continue;
+            if (fabsf(apq) <= eps * 0.5f * sqrtf(fabsf(A[p][p] * A[q][q]))) {
+                A[p][q] = A[q][p] = 0.f;
+                continue;
+            }
+            float c, s;
+            jacobi_cs(A[p][p], A[q][q], apq, c, s);
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                float akp = A[k][p], akq = A[k][q];
+                A[k][p] = c * akp - s * akq;
+                A[k][q] = s * akp + c * akq;
+            }
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                float apk = A[p][k], aqk = A[q][k];
+                A[p][k] = c * apk - s * aqk;
+                A[q][k] = s * apk + c * aqk;
+            }
+            A[p][q] = A[q][p] = 0.f;
+#pragma unroll
+            for (int k = 0; k < 3; ++k) {
+                float vkp = Vm[k][p], vkq = Vm[k][q];
+                Vm[k][p] = c * vkp - s * vkq;
+                Vm[k][q] = s * vkp + c * vkq;
+            }
+            rotated = true;
+        }
+        if (!rotated) break;
+    }
+    float e0 = A[0][0], e1 = A[1][1], e2 = A[2][2];
+    V3 q0 = v3(Vm[0][0], Vm[1][0], Vm[2][0]);
+    V3 q1 = v3(Vm[0][1], Vm[1][1], Vm[2][1]);
+    V3 q2 = v3(Vm[0][2], Vm[1][2], Vm[2][2]);
+    if (e1 < e0) { swapf(e0, e1); swap3(q0, q1); }
+    if (e2 < e1) { swapf(e1, e2); swap3(q1, q2); }
+    if (e1 < e0) { swapf(e0, e1); swap3(q0, q1); }
+    w = v3(e0, e1, e2);
+    Q.c[0] = q0; Q.c[1] = q1; Q.c[2] = q2;
+}
+
+// Symmetric 2x2 eigen-decomposition, eigenvalues increasing.
+AVBD_HD void eig2(float a00, float a11, float a01, float& w0, float& w1, float& c00, float& c10, float& c01,
+                  float& c11) {
+    float p00 = a00, p11 = a11, p01 = a01;
+    float x0 = 1.f, y0 = 0.f, x1 = 0.f, y1 = 1.f;   // columns (x0,y0), (x1,y1)
+    const float eps = 1.1920929e-07f;
+    if (p01 != 0.f && !(fabsf(p01) <= eps * 0.5f * sqrtf(fabsf(p00 * p11)))) {
+        float c, s;
+        jacobi_cs(p00, p11, p01, c, s);
+        float n00 = c * (c * p00 - s * p01) - s * (c * p01 - s * p11);
+        float n11 = s * (s * p00 + c * p01) + c * (s * p01 + c * p11);
+        p00 = n00;
+        p11 = n11;
+        x0 = c; y0 = -s; x1 = s; y1 = c;
+    }
+    if (p11 < p00) {
+        w0 = p11; w1 = p00;
+        c00 = x1; c10 = y1; c01 = x0; c11 = y0;
+    } else {
+        w0 = p00; w1 = p11;
+        c00 = x0; c10 = y0; c01 = x1; c11 = y1;
+    }
+}
+
+// ProjectEigenvalues (math.cpp:137-171)
+AVBD_HD void project_eigenvalues(float* ev, int count, int mode, float rho, float threshold = 0.01f,
+                                 float epsilon = 1e-6f) {
+    bool use_abs = false;
+    if (mode == 0) {
+        for (int i = 0; i < count; ++i) ev[i] = fmaxf(epsilon, ev[i]);
+        return;
+    } else if (mode == 1) {
+        use_abs = true;
+    } else {
+        use_abs = fabsf(rho - 1.f) > threshold;
+        if (!use_abs) {
+            for (int i = 0; i < count; ++i) ev[i] = fmaxf(epsilon, ev[i]);
+            return;
+        }
+    }
+    for (int i = 0; i < count; ++i) {
+        ev[i] = fabsf(ev[i]);
+        if (ev[i] < epsilon) ev[i] = epsilon;
+    }
+}
+
+// Symmetric 3x3 accumulator (upper part implied).
+struct S3 { float xx, yy, zz, xy, xz, yz; };
+AVBD_HD void s3_zero(S3& h) { h.xx = h.yy = h.zz = h.xy = h.xz = h.yz = 0.f; }
+AVBD_HD void s3_add_outer(S3& h, float lam, V3 w) {
+    h.xx += lam * (w.x * w.x); h.yy += lam * (w.y * w.y); h.zz += lam * (w.z * w.z);
+    h.xy += lam * (w.y * w.x); h.xz += lam * (w.z * w.x); h.yz += lam * (w.z * w.y);
+}
+
+// NeoHookeanFEM::ComputeEnergyTerms for vertex `role` of the tet
+// (neohookeanfem.cpp:40-83, HandleInvertedElement :86-110).
+AVBD_HD void neohookean_terms(V3 p0, V3 p1, V3 p2, V3 p3, const float* DmInv, V3 gradN, float restVolume, float mu,
+                              float lambda, int mode, float rho, V3& grad, S3& H) {
+    M3 Ds;
+    Ds.c[0] = p1 - p0; Ds.c[1] = p2 - p0; Ds.c[2] = p3 - p0;
+    M3 F;
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+        F.c[j] = Ds.c[0] * DmInv[3 * j + 0] + Ds.c[1] * DmInv[3 * j + 1] + Ds.c[2] * DmInv[3 * j + 2];
+    const float J = det3(F);
+    // cofactor matrix of F (math.cpp:67-78)
+    const float f00 = m3(F, 0, 0), f01 = m3(F, 0, 1), f02 = m3(F, 0, 2);
+    const float f10 = m3(F, 1, 0), f11 = m3(F, 1, 1), f12 = m3(F, 1, 2);
+    const float f20 = m3(F, 2, 0), f21 = m3(F, 2, 1), f22 = m3(F, 2, 2);
+    M3 cof;
+    cof.c[0] = v3(f11 * f22 - f12 * f21, -(f01 * f22 - f02 * f21), f01 * f12 - f02 * f11);
+    cof.c[1] = v3(-(f10 * f22 - f12 * f20), f00 * f22 - f02 * f20, -(f00 * f12 - f02 * f10));
+    cof.c[2] = v3(f10 * f21 - f11 * f20, -(f00 * f21 - f01 * f20), f00 * f11 - f01 * f10);
+    if (J <= 1e-6f) {
+        const float stiff = mu + lambda;
+        V3 dJ = matvec(cof, gradN);
+        float pm = stiff * (1e-6f - J);
+        grad = (-restVolume * pm) * dJ;
+        float d = restVolume * stiff;
+        H.xx = d; H.yy = d; H.zz = d; H.xy = 0.f; H.xz = 0.f; H.yz = 0.f;
+        return;
+    }
+    const float logJ = logf(J);
+    const float scalar = (lambda * logJ - mu) / J;
+    M3 P;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) P.c[j] = mu * F.c[j] + scalar * cof.c[j];
+    grad = matvec(P, gradN) * restVolume;
+
+    M3 U, V;
+    V3 S;
+    svd3(F, U, S, V);
+    // ComputeEnergyHessian (math.cpp:86-134)
+    const float s0 = S.x, s1 = S.y, s2 = S.z;
+    float ev[9];
+    const float dPhi = (lambda * logJ - mu) / J;
+    ev[3] = mu + dPhi * s2; ev[4] = mu + dPhi * s1; ev[5] = mu + dPhi * s0;
+    ev[6] = mu - dPhi * s2; ev[7] = mu - dPhi * s1; ev[8] = mu - dPhi * s0;
+    const float diagExtra = mu + lambda * (1.0f - logJ);
+    V3 w;
+    M3 Q;
+    eig3(mu + diagExtra / (s0 * s0), mu + diagExtra / (s1 * s1), mu + diagExtra / (s2 * s2), lambda * s2 / J,
+         lambda * s1 / J, lambda * s0 / J, w, Q);
+    ev[0] = w.x; ev[1] = w.y; ev[2] = w.z;
+    project_eigenvalues(ev, 9, mode, rho);
+    // ReconstructVertexHessian (math.cpp:174-230)
+    const float vg0 = dot(V.c[0], gradN), vg1 = dot(V.c[1], gradN), vg2 = dot(V.c[2], gradN);
+    s3_zero(H);
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        V3 c = Q.c[k];
+        V3 ww = (c.x * vg0) * U.c[0] + (c.y * vg1) * U.c[1] + (c.z * vg2) * U.c[2];
+        s3_add_outer(H, ev[k], ww);
+    }
+    const float is2 = 0.70710678118f;
+    s3_add_outer(H, ev[3], is2 * (vg1 * U.c[0] - vg0 * U.c[1]));
+    s3_add_outer(H, ev[4], is2 * (vg2 * U.c[0] - vg0 * U.c[2]));
+    s3_add_outer(H, ev[5], is2 * (vg2 * U.c[1] - vg1 * U.c[2]));
+    s3_add_outer(H, ev[6], is2 * (vg1 * U.c[0] + vg0 * U.c[1]));
+    s3_add_outer(H, ev[7], is2 * (vg2 * U.c[0] + vg0 * U.c[2]));
+    s3_add_outer(H, ev[8], is2 * (vg2 * U.c[1] + vg1 * U.c[2]));
+    H.xx *= restVolume; H.yy *= restVolume; H.zz *= restVolume;
+    H.xy *= restVolume; H.xz *= restVolume; H.yz *= restVolume;
+}
+
+// STVKFEM::ComputeEnergyTerms for vertex `role` of the triangle
+// (stvkfem.cpp:38-86) with STVKMath (math.cpp:234-357).
+// DmInv2D column-major (m00, m10, m01, m11); gradN is 2D.
+AVBD_HD void stvk_terms(V3 p0, V3 p1, V3 p2, float4 DmInv, float gnx, float gny, float restArea, float mu,
+                        float lambda, int mode, float rho, V3& grad, S3& H) {
+    V3 e0 = p1 - p0, e1 = p2 - p0;
+    // F (3x2) = Ds (3x2) * DmInv (2x2)
+    V3 F0 = e0 * DmInv.x + e1 * DmInv.y;
+    V3 F1 = e0 * DmInv.z + e1 * DmInv.w;
+    const float stiff = mu + lambda;
+    if (norm(cross(e0, e1)) < 2.f * restArea * 0.01f) {
+        V3 P0 = stiff * F0, P1 = stiff * F1;
+        grad = restArea * (P0 * gnx + P1 * gny);
+        float d = restArea * stiff;
+        H.xx = d; H.yy = d; H.zz = d; H.xy = 0.f; H.xz = 0.f; H.yz = 0.f;
+        return;
+    }
+    // L = 0.5 (F^T F - I)
+    const float c00 = dot(F0, F0), c01 = dot(F0, F1), c11 = dot(F1, F1);
+    const float L00 = 0.5f * (c00 - 1.f), L01 = 0.5f * c01, L11 = 0.5f * (c11 - 1.f);
+    const float trL = L00 + L11;
+    // P = F (2 mu L + lambda trL I)
+    const float S00 = 2.f * mu * L00 + lambda * trL, S01 = 2.f * mu * L01, S11 = 2.f * mu * L11 + lambda * trL;
+    V3 P0 = F0 * S00 + F1 * S01;
+    V3 P1 = F0 * S01 + F1 * S11;
+    grad = restArea * (P0 * gnx + P1 * gny);
+
+    // SVD of the 3x2 F: one Jacobi rotation on the two columns
+    V3 a0 = F0, a1 = F1;
+    float vx0 = 1.f, vy0 = 0.f, vx1 = 0.f, vy1 = 1.f;
+    const float eps = 1.1920929e-07f;
+    for (int sweep = 0; sweep < 64; ++sweep) {
+        float al = sqnorm(a0), be = sqnorm(a1), ga = dot(a0, a1);
+        if (ga == 0.f || fabsf(ga) <= eps * sqrtf(al * be)) break;
+        float c, s;
+        jacobi_cs(al, be, ga, c, s);
+        rot_cols(a0, a1, c, s);
+        float nx0 = c * vx0 - s * vx1, ny0 = c * vy0 - s * vy1;
+        float nx1 = s * vx0 + c * vx1, ny1 = s * vy0 + c * vy1;
+        vx0 = nx0; vy0 = ny0; vx1 = nx1; vy1 = ny1;
+    }
+    float s0 = norm(a0), s1 = norm(a1);
+    if (s0 < s1) {
+        swapf(s0, s1); swap3(a0, a1);
+        swapf(vx0, vx1); swapf(vy0, vy1);
+    }
+    const float tiny = 1.17549435e-38f;
+    V3 u0 = s0 > tiny ? a0 / s0 : v3(1, 0, 0);
+    V3 u1 = s1 > tiny ? a1 / s1 : v3(0, 1, 0);
+    if (vx0 * vy1 - vx1 * vy0 < 0.f) { vx1 = -vx1; vy1 = -vy1; s1 = -s1; }   // math.cpp:246-250
+
+    // ComputeEnergyHessian (math.cpp:285-321)
+    float ev[4];
+    const float trS = s0 * s0 + s1 * s1;
+    const float d0 = s0 * (mu * (s0 * s0 - 1.f) + 0.5f * lambda * (trS - 2.f));
+    const float d1 = s1 * (mu * (s1 * s1 - 1.f) + 0.5f * lambda * (trS - 2.f));
+    ev[2] = (s0 + s1 > 1e-8f) ? (d0 + d1) / (s0 + s1) : -(mu + lambda);
+    ev[3] = (fabsf(s0 - s1) > 1e-8f) ? (d0 - d1) / (s0 - s1) : (3.f * mu + 2.f * lambda) * s0 * s0 - mu - lambda;
+    const float A00 = 3.f * mu * s0 * s0 + 0.5f * lambda * (3.f * s0 * s0 + s1 * s1) - mu - lambda;
+    const float A11 = 3.f * mu * s1 * s1 + 0.5f * lambda * (3.f * s1 * s1 + s0 * s0) - mu - lambda;
+    const float A01 = lambda * s0 * s1;
+    float q00, q10, q01, q11;
+    eig2(A00, A11, A01, ev[0], ev[1], q00, q10, q01, q11);
+    project_eigenvalues(ev, 4, mode, rho);
+    // ReconstructVertexHessian (math.cpp:324-356)
+    const float vg0 = vx0 * gnx + vy0 * gny;
+    const float vg1 = vx1 * gnx + vy1 * gny;
+    s3_zero(H);
+    s3_add_outer(H, ev[0], (q00 * vg0) * u0 + (q10 * vg1) * u1);
+    s3_add_outer(H, ev[1], (q01 * vg0) * u0 + (q11 * vg1) * u1);
+    const float is2 = 0.70710678118f;
+    s3_add_outer(H, ev[2], is2 * (vg1 * u0 - vg0 * u1));
+    s3_add_outer(H, ev[3], is2 * (vg1 * u0 + vg0 * u1));
+    H.xx *= restArea; H.yy *= restArea; H.zz *= restArea;
+    H.xy *= restArea; H.xz *= restArea; H.yz *= restArea;
+}
+
+}  // namespace avbd

@@ -1,0 +1,377 @@
+// Step drivers.  Block-cooperative functions (scans, incidence build,
+// Jones-Plassmann colouring, colour lists) run on one CTA per scene; the
+// persistent batched kernel strings every phase of a scene's step together on
+// one CTA, and the single-scene path launches the same per-item functions as
+// grid-wide kernels between them.
+#pragma once
+#include "avbd_phases.cuh"
+
+namespace avbd {
+
+constexpr unsigned kFull = 0xffffffffu;
+
+// Exclusive scan of in[0, n) into out[0, n) by one CTA; returns the total.
+// in and out may alias.
+__device__ int block_exclusive_scan(const int* in, int* out, int n) {
+    __shared__ int warp_tot[32];
+    __shared__ int carry;
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = (blockDim.x + 31) >> 5;
+    if (threadIdx.x == 0) carry = 0;
+    __syncthreads();
+    for (int base = 0; base < n; base += blockDim.x) {
+        const int i = base + threadIdx.x;
+        const int v = i < n ? in[i] : 0;
+        int x = v;
+#pragma unroll
+        for (int o = 1; o < 32; o <<= 1) {
+            int y = __shfl_up_sync(kFull, x, o);
+            if (lane >= o) x += y;
+        }
+        if (lane == 31) warp_tot[warp] = x;
+        __syncthreads();
+        if (warp == 0) {
+            int w = lane < nwarps ? warp_tot[lane] : 0;
+#pragma unroll
+            for (int o = 1; o < 32; o <<= 1) {
+                int y = __shfl_up_sync(kFull, w, o);
+                if (lane >= o) w += y;
+            }
+            warp_tot[lane] = w;
+        }
+        __syncthreads();
+        const int prefix = carry + (warp > 0 ? warp_tot[warp - 1] : 0);
+        if (i < n) out[i] = prefix + x - v;
+        __syncthreads();
+        if (threadIdx.x == blockDim.x - 1) carry = prefix + x;
+        __syncthreads();
+    }
+    const int total = carry;
+    __syncthreads();
+    return total;
+}
+
+// ---------------------------------------------------------------------------
+// Incidence (CSR) of one scene: per body
+//   [static forces][manifolds as body B, by slot][manifolds as body A][energies]
+// which follows Mesh::forces then Mesh::energies (solver.cpp:395-435).
+// ---------------------------------------------------------------------------
+__device__ int owned_live(const World& W, int cur, int b, int base_slot) {
+    const int c0 = W.cand_off[b] + base_slot, c1 = c0 + W.cand_cnt[b];
+    int n = 0;
+    for (int c = c0; c < c1; ++c) n += W.cn[cur][c] > 0 ? 1 : 0;
+    return n;
+}
+
+// Insertion sort of manifold entries by (birth step, slot).
+__device__ __forceinline__ void sort_manifold_entries(const World& W, int cur, uint32_t* seg, int n) {
+    for (int i = 1; i < n; ++i) {
+        const uint32_t v = seg[i];
+        const int bv = W.cbirth[cur][ent_index(v)];
+        int j = i - 1;
+        while (j >= 0) {
+            const uint32_t u = seg[j];
+            const int bu = W.cbirth[cur][ent_index(u)];
+            if (bu < bv || (bu == bv && ent_index(u) < ent_index(v))) break;
+            seg[j + 1] = u;
+            --j;
+        }
+        seg[j + 1] = v;
+    }
+}
+
+// Returns false (and sets need_inc) when the scene's incidence region is too small.
+__device__ bool build_incidence(const World& W, const SceneDesc& sc, SceneState* st, int cur) {
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int b0 = sc.body0, b1 = sc.body0 + sc.nbody;
+    const int ncand = st->ncand[cur];
+    for (int b = b0 + tid; b < b1; b += nt) W.cntB[b] = 0;
+    __syncthreads();
+    for (int c = sc.cand0 + tid; c < sc.cand0 + ncand; c += nt)
+        if (W.cn[cur][c] > 0) atomicAdd(&W.cntB[W.cpair[cur][c].y], 1);
+    __syncthreads();
+    for (int b = b0 + tid; b < b1; b += nt) {
+        const int ns = W.sinc_off[b + 1] - W.sinc_off[b];
+        W.inc_cnt[b] = ns + W.cntB[b] + owned_live(W, cur, b, sc.cand0);
+    }
+    __syncthreads();
+    const int total = block_exclusive_scan(W.inc_cnt + b0, W.inc_off + b0, sc.nbody);
+    if (total > sc.inccap) {
+        if (tid == 0) { st->need_inc = total; }
+        return false;
+    }
+    for (int b = b0 + tid; b < b1; b += nt) {
+        const int off = sc.inc0 + W.inc_off[b];
+        W.inc_off[b] = off;
+        const int s0 = W.sinc_off[b], nf = W.sinc_nf[b], ns = W.sinc_off[b + 1] - s0;
+        int k = off;
+        for (int e = 0; e < nf; ++e) W.inc[k++] = W.sinc[s0 + e];
+        k += W.cntB[b];
+        const int c0 = W.cand_off[b] + sc.cand0, c1 = c0 + W.cand_cnt[b];
+        for (int c = c0; c < c1; ++c)
+            if (W.cn[cur][c] > 0) W.inc[k++] = ent_make(kEntManifold, 0, (uint32_t)c);
+        for (int e = nf; e < ns; ++e) W.inc[k++] = W.sinc[s0 + e];
+        W.bcur[b] = 0;
+    }
+    __syncthreads();
+    for (int c = sc.cand0 + tid; c < sc.cand0 + ncand; c += nt) {
+        if (W.cn[cur][c] == 0) continue;
+        const int B = W.cpair[cur][c].y;
+        const int p = atomicAdd(&W.bcur[B], 1);
+        W.inc[W.inc_off[B] + W.sinc_nf[B] + p] = ent_make(kEntManifold, 1, (uint32_t)c);
+    }
+    __syncthreads();
+    // order each body's manifolds as Mesh::forces holds them: by creation step,
+    // then by pair (creation order within a broadphase pass)
+    for (int b = b0 + tid; b < b1; b += nt) {
+        uint32_t* seg = W.inc + W.inc_off[b] + W.sinc_nf[b];
+        const int n = W.inc_cnt[b] - (W.sinc_off[b + 1] - W.sinc_off[b]);
+        sort_manifold_entries(W, cur, seg, n);
+    }
+    if (tid == 0) st->ninc = total;
+    __syncthreads();
+    return true;
+}
+
+// ---------------------------------------------------------------------------
+// Jones-Plassmann first-fit colouring of the dynamic bodies of one scene.
+// Priority = (hash(local index), local index), smaller first.  A body takes
+// the smallest colour not used by its smaller-priority neighbours once all of
+// them are coloured, which equals sequential greedy colouring in priority
+// order whatever the thread schedule (each body's colour depends only on the
+// final colours of its smaller-priority neighbours).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ bool prio_less(uint32_t ha, int la, uint32_t hb, int lb) {
+    return ha != hb ? ha < hb : la < lb;
+}
+
+template <typename Fn>
+__device__ __forceinline__ void for_each_neighbour(const World& W, int cur, int b, Fn fn) {
+    const int e0 = W.inc_off[b], e1 = e0 + W.inc_cnt[b];
+    for (int e = e0; e < e1; ++e) {
+        const uint32_t ent = W.inc[e];
+        const uint32_t kind = ent_kind(ent), idx = ent_index(ent);
+        if (kind == kEntManifold) {
+            const int2 ab = W.cpair[cur][idx];
+            fn(ab.x == b ? ab.y : ab.x);
+        } else if (kind == kEntForce) {
+            if (W.ftype[idx] & kForceRemoved) continue;
+            const int2 ab = W.fbody[idx];
+            const int o = ab.x == b ? ab.y : ab.x;
+            if (o >= 0) fn(o);
+        } else if (kind == kEntTet) {
+            if (W.tparam[idx].w != 0.f) continue;
+            const int4 v = W.tidx[idx];
+            if (v.x != b) fn(v.x);
+            if (v.y != b) fn(v.y);
+            if (v.z != b) fn(v.z);
+            if (v.w != b) fn(v.w);
+        } else {
+            if (W.rparam[idx].w != 0.f) continue;
+            const int4 v = W.ridx[idx];
+            if (v.x != b) fn(v.x);
+            if (v.y != b) fn(v.y);
+            if (v.z != b) fn(v.z);
+        }
+    }
+}
+
+// Returns false (status TIMEOUT or CAPACITY set) if colouring could not finish.
+__device__ bool colour_scene(const World& W, const SceneDesc& sc, SceneState* st, int scene, int cur) {
+    __shared__ int s_remaining, s_progress, s_maxc;
+    __shared__ int s_count[kMaxColours + 1];
+    const int tid = threadIdx.x, nt = blockDim.x;
+    const int b0 = sc.body0, b1 = sc.body0 + sc.nbody;
+    volatile int* col = W.colour;
+    for (int b = b0 + tid; b < b1; b += nt) col[b] = (W.flags[b] & (kBodyStatic | kBodyRemoved)) ? -2 : -1;
+    if (tid == 0) s_maxc = 0;
+    __syncthreads();
+    const int max_rounds = sc.nbody + 2;
+    for (int round = 0;; ++round) {
+        if (tid == 0) { s_remaining = 0; s_progress = 0; }
+        __syncthreads();
+        for (int b = b0 + tid; b < b1; b += nt) {
+            if (col[b] != -1) continue;
+            const int lb = W.local[b];
+            const uint32_t hb = colour_priority((uint32_t)lb);
+            bool ready = true;
+            for_each_neighbour(W, cur, b, [&](int n) {
+                if (!ready) return;
+                const int cn = col[n];
+                if (cn == -2) return;
+                const int ln = W.local[n];
+                if (prio_less(colour_priority((uint32_t)ln), ln, hb, lb) && cn < 0) ready = false;
+            });
+            if (!ready) { s_remaining = 1; continue; }
+            int chosen = -1;
+            for (int base = 0; base < kMaxColours && chosen < 0; base += 64) {
+                unsigned long long used = 0ull;
+                for_each_neighbour(W, cur, b, [&](int n) {
+                    const int cn = col[n];
+                    if (cn < base || cn >= base + 64) return;
+                    const int ln = W.local[n];
+                    if (prio_less(colour_priority((uint32_t)ln), ln, hb, lb)) used |= 1ull << (cn - base);
+                });
+                if (~used) chosen = base + __ffsll((long long)~used) - 1;
+            }
+            if (chosen < 0 || chosen >= kMaxColours) {
+                st->status = kStatusCapacity;
+                chosen = kMaxColours - 1;
+            }
+            col[b] = chosen;
+            atomicMax(&s_maxc, chosen + 1);
+            s_progress = 1;
+        }
+        __syncthreads();
+        const int remaining = s_remaining, progress = s_progress;
+        __syncthreads();   // every thread has read the flags before thread 0 resets them
+        if (!remaining) break;
+        if (!progress || round > max_rounds) {
+            if (tid == 0) st->status = kStatusTimeout;
+            __syncthreads();
+            return false;
+        }
+    }
+    const int ncol = s_maxc;
+    __syncthreads();
+    // colour lists: counting sort of the dynamic bodies by colour
+    for (int c = tid; c <= ncol; c += nt) s_count[c] = 0;
+    __syncthreads();
+    for (int b = b0 + tid; b < b1; b += nt) {
+        const int c = col[b];
+        if (c >= 0) atomicAdd(&s_count[c], 1);
+    }
+    __syncthreads();
+    int* cs = W.col_start + (size_t)scene * (kMaxColours + 1);
+    if (tid == 0) {
+        int acc = 0;
+        for (int c = 0; c < ncol; ++c) { cs[c] = acc; acc += s_count[c]; s_count[c] = cs[c]; }
+        cs[ncol] = acc;
+        st->ncolours = ncol;
+    }
+    __syncthreads();
+    for (int b = b0 + tid; b < b1; b += nt) {
+        const int c = col[b];
+        if (c >= 0) W.col_list[b0 + atomicAdd(&s_count[c], 1)] = b;
+    }
+    __syncthreads();
+    return st->status == kStatusOk;
+}
+
+// ---------------------------------------------------------------------------
+// Whole step of one scene on one CTA (batched path).
+// ---------------------------------------------------------------------------
+__device__ void scene_step(const World& W, int scene) {
+    const SceneDesc sc = W.scenes[scene];
+    SceneState* st = W.sstate + scene;
+    const int tid = threadIdx.x, nt = blockDim.x;
+    __shared__ int s_flags;
+    if (st->status != kStatusOk && st->status != kStatusCapacity && st->status != kStatusTimeout) return;
+    __syncthreads();
+    if (tid == 0) { st->status = kStatusOk; st->need_cand = 0; st->need_k = 0; st->need_inc = 0; }
+    const int old = st->cur, cur = old ^ 1;
+    const int b0 = sc.body0, b1 = sc.body0 + sc.nbody;
+    // 1. broadphase: count, scan, capacity check, write
+    for (int b = b0 + tid; b < b1; b += nt) W.cand_cnt[b] = broadphase_body(W, sc, b, nullptr, 0);
+    __syncthreads();
+    const int ncand = block_exclusive_scan(W.cand_cnt + b0, W.cand_off + b0, sc.nbody);
+    if (ncand > sc.candcap) {
+        if (tid == 0) { st->status = kStatusCapacity; st->need_cand = ncand; }
+        return;
+    }
+    for (int b = b0 + tid; b < b1; b += nt)
+        broadphase_body(W, sc, b, W.cpair[cur] + sc.cand0 + W.cand_off[b], W.cand_cnt[b]);
+    if (tid == 0) st->kused[cur] = 0;
+    __syncthreads();
+    // 2. narrowphase + manifold warm start into the other table
+    const int old_count = st->ncand[old];
+    for (int c = sc.cand0 + tid; c < sc.cand0 + ncand; c += nt) narrowphase_slot(W, sc, st, c, cur, old_count);
+    __syncthreads();
+    if (st->need_k) {
+        if (tid == 0) { st->status = kStatusCapacity; st->need_k = st->kused[cur]; }
+        return;
+    }
+    if (tid == 0) { st->ncand[cur] = ncand; st->cur = cur; }
+    // 2b. joints / springs warm start
+    for (int f = sc.force0 + tid; f < sc.force0 + sc.nforce; f += nt) force_init(W, f);
+    __syncthreads();
+    // incidence
+    if (!build_incidence(W, sc, st, cur)) {
+        if (tid == 0) st->status = kStatusCapacity;
+        return;
+    }
+    // colouring
+    if (!colour_scene(W, sc, st, scene, cur)) return;
+    // 4. prediction
+    for (int b = b0 + tid; b < b1; b += nt) predict_body(W, b);
+    __syncthreads();
+    const int ncol = st->ncolours;
+    const int* cs = W.col_start + (size_t)scene * (kMaxColours + 1);
+    // 5. iterations
+    for (int it = 0; it < W.P.num_iterations; ++it) {
+        for (int c = 0; c < ncol; ++c) {
+            const int e = cs[c + 1];
+            for (int i = cs[c] + tid; i < e; i += nt) primal_body(W, cur, W.col_list[b0 + i], W.P.alpha, false);
+            __syncthreads();
+        }
+        if (tid == 0) s_flags = 0;
+        __syncthreads();
+        for (int f = sc.force0 + tid; f < sc.force0 + sc.nforce; f += nt)
+            if (dual_force(W, f, W.P.alpha)) s_flags = 1;
+        for (int c = sc.cand0 + tid; c < sc.cand0 + ncand; c += nt) dual_manifold(W, cur, c, W.P.alpha);
+        __syncthreads();
+        const int fractured = s_flags;
+        __syncthreads();
+        if (fractured) {
+            for (int c = sc.cand0 + tid; c < sc.cand0 + ncand; c += nt) fracture_reset_slot(W, cur, c);
+            __syncthreads();
+            for (int b = b0 + tid; b < b1; b += nt) W.reset_flag[b] = 0;
+            __syncthreads();
+        }
+    }
+    // 6. velocities, explosion, out of bounds
+    if (tid == 0) s_flags = 0;
+    __syncthreads();
+    for (int b = b0 + tid; b < b1; b += nt) {
+        const int r = velocity_body(W, b);
+        if (r) atomicOr(&s_flags, r);
+    }
+    __syncthreads();
+    const int vf = s_flags;
+    __syncthreads();
+    if (vf & 1) { if (tid == 0) st->status = kStatusExploded; return; }
+    if (vf & 2) { if (tid == 0) st->status = kStatusNan; return; }
+    if (vf & 4) {
+        // RemoveBody of every out-of-bounds body (solver.cpp:530-534, geometry.cpp:11-25)
+        for (int b = b0 + tid; b < b1; b += nt) {
+            const int fl = W.flags[b];
+            if ((fl & (kBodyStatic | kBodyRemoved)) != 0) continue;
+            const float4 p = W.pos[b];
+            if (p.x < kBoundMin || p.x > kBoundMax || p.y < kBoundMin || p.y > kBoundMax || p.z < kBoundMin ||
+                p.z > kBoundMax) {
+                W.flags[b] = fl | kBodyRemoved;
+                for (int e = W.sinc_off[b]; e < W.sinc_off[b + 1]; ++e) {
+                    const uint32_t ent = W.sinc[e];
+                    const uint32_t k = ent_kind(ent), idx = ent_index(ent);
+                    if (k == kEntForce) atomicOr(&W.ftype[idx], kForceRemoved);
+                    else if (k == kEntTet) W.tparam[idx].w = 1.f;
+                    else if (k == kEntTri) W.rparam[idx].w = 1.f;
+                }
+            }
+        }
+        __syncthreads();
+    }
+    if (tid == 0) st->step += 1;
+    // 7. post-stabilisation
+    if (W.P.post_stabilization) {
+        for (int c = 0; c < ncol; ++c) {
+            const int e = cs[c + 1];
+            for (int i = cs[c] + tid; i < e; i += nt) {
+                const int b = W.col_list[b0 + i];
+                if (!(W.flags[b] & kBodyRemoved)) primal_body(W, cur, b, 0.f, true);
+            }
+            __syncthreads();
+        }
+    }
+}
+
+}  // namespace avbd

@@ -1,0 +1,271 @@
+"""Python mirror of the reference ``Solver`` API over the CUDA C-ABI.
+
+``Solver`` keeps the method names and argument meaning of SkyePhyX's
+``Solver`` (src/physics/solver.hpp:22-94) and of the Force/Energy
+constructors it is given (``Spring``, ``Joint``, ``NeoHookeanFEM``,
+``STVKFEM``); ``step()`` replaces ``Solver::Step()``.  ``Batch`` advances
+many independent scenes per persistent-kernel launch.  Every step runs on
+the GPU; without a CUDA device the constructors raise ``AvbdError``.
+"""
+from __future__ import annotations
+
+import ctypes as C
+
+import numpy as np
+
+from ._lib import AvbdError, AvbdParams, AvbdTimings, STATUS, check, default_params, load
+
+INF = float("inf")
+
+
+def _f(a, n):
+    arr = np.ascontiguousarray(np.asarray(a, dtype=np.float32).reshape(-1))
+    if arr.size != n:
+        raise ValueError(f"expected {n} floats, got {arr.size}")
+    return arr
+
+
+def _fp(a):
+    return a.ctypes.data_as(C.POINTER(C.c_float))
+
+
+class Solver:
+    """One scene (the reference's Solver) stepped on one GPU."""
+
+    def __init__(self, iterations=10, dt=1.0 / 60.0, alpha=0.95, beta=100000.0, gamma=0.99,
+                 on_penetration_penalty=0.0, post_stabilization=True, projection_mode=1, device=0):
+        self._lib = load()
+        self._p = default_params(num_iterations=int(iterations), step_value=float(dt), alpha=float(alpha),
+                                 beta=float(beta), gamma=float(gamma),
+                                 on_penetration_penalty=float(on_penetration_penalty),
+                                 post_stabilization=int(bool(post_stabilization)),
+                                 projection_mode=int(projection_mode))
+        h = C.c_void_p()
+        check(self._lib.avbd_world_create(C.byref(self._p), int(device), C.byref(h)), "avbd_world_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.avbd_world_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    @property
+    def handle(self):
+        return self._h
+
+    # ---- parameters (solver.hpp:69-84) ----
+    def set_params(self, **kw):
+        for k, v in kw.items():
+            setattr(self._p, k, v)
+        check(self._lib.avbd_set_params(self._h, C.byref(self._p)), "avbd_set_params")
+
+    @property
+    def params(self) -> AvbdParams:
+        return self._p
+
+    # ---- scene building ----
+    def add_body(self, model_type, density, friction, pos, scale, vel=(0, 0, 0), quat=(1, 0, 0, 0),
+                 omega=(0, 0, 0), is_static=False):
+        """Solver::AddBody (solver.cpp:50-101); quat is (w, x, y, z). Returns the body id."""
+        p, s, v, q, w = _f(pos, 3), _f(scale, 3), _f(vel, 3), _f(quat, 4), _f(omega, 3)
+        return check(self._lib.avbd_add_body(self._h, int(model_type), float(density), float(friction), _fp(p),
+                                             _fp(s), _fp(v), _fp(q), _fp(w), int(bool(is_static))), "add_body")
+
+    def add_particle(self, mass, friction, pos, vel=(0, 0, 0), is_static=False):
+        """Solver::AddParticle (solver.cpp:119-131)."""
+        p, v = _f(pos, 3), _f(vel, 3)
+        return check(self._lib.avbd_add_particle(self._h, float(mass), float(friction), _fp(p), _fp(v),
+                                                 int(bool(is_static))), "add_particle")
+
+    def set_static(self, body, is_static=True):
+        return check(self._lib.avbd_set_body_static(self._h, int(body), int(bool(is_static))), "set_static")
+
+    def add_spring(self, a, rA, b, rB, stiffness, rest_length=-1.0, is_rope=False, fracture=INF):
+        """Spring (force.hpp:95); a = -1 anchors rA in world space. Returns the force id."""
+        ra, rb = _f(rA, 3), _f(rB, 3)
+        return check(self._lib.avbd_add_spring(self._h, int(a), _fp(ra), int(b), _fp(rb), float(stiffness),
+                                               float(rest_length), int(bool(is_rope)), float(fracture)),
+                     "add_spring")
+
+    def add_joint(self, a, rA, b, rB, stiffness=(INF,) * 6, fracture=(INF,) * 6):
+        """Joint (force.hpp:119-122). Returns the force id."""
+        ra, rb, k, fr = _f(rA, 3), _f(rB, 3), _f(stiffness, 6), _f(fracture, 6)
+        return check(self._lib.avbd_add_joint(self._h, int(a), _fp(ra), int(b), _fp(rb), _fp(k), _fp(fr)),
+                     "add_joint")
+
+    def add_neohookean_tet(self, v, E, nu):
+        """NeoHookeanFEM (energy.hpp:50-52). Returns the energy id."""
+        iv = (C.c_int32 * 4)(*[int(x) for x in v])
+        return check(self._lib.avbd_add_neohookean_tet(self._h, iv, float(E), float(nu)), "add_neohookean_tet")
+
+    def add_stvk_tri(self, v, E, nu):
+        """STVKFEM (energy.hpp:90-92). Returns the energy id."""
+        iv = (C.c_int32 * 3)(*[int(x) for x in v])
+        return check(self._lib.avbd_add_stvk_tri(self._h, iv, float(E), float(nu)), "add_stvk_tri")
+
+    def make_tet_volume(self, ox, oy, oz, nx, ny, nz, cell, E, nu, particle_mass=1.0, friction=0.5,
+                        pin_min_x=False):
+        """GeometryHelpers::makeTetVolume (geometry.cpp:30-94). Returns the first particle id."""
+        return check(self._lib.avbd_make_tet_volume(self._h, float(ox), float(oy), float(oz), int(nx), int(ny),
+                                                    int(nz), float(cell), float(E), float(nu),
+                                                    float(particle_mass), float(friction), int(bool(pin_min_x))),
+                     "make_tet_volume")
+
+    # ---- stepping ----
+    def step(self):
+        """Solver::Step(); returns the status name ('ok', 'exploded', ...)."""
+        r = check(self._lib.avbd_step(self._h), "avbd_step")
+        return STATUS.get(r, str(r))
+
+    def step_dt(self, dt, iterations):
+        r = check(self._lib.avbd_step_dt(self._h, float(dt), int(iterations)), "avbd_step_dt")
+        self._p.step_value = float(dt)
+        self._p.num_iterations = int(iterations)
+        return STATUS.get(r, str(r))
+
+    # ---- readback ----
+    @property
+    def num_bodies(self):
+        return self._lib.avbd_num_bodies(self._h)
+
+    @property
+    def num_dynamic(self):
+        return self._lib.avbd_num_dynamic_bodies(self._h)
+
+    @property
+    def emergency_stop(self):
+        return bool(self._lib.avbd_emergency_stop(self._h))
+
+    def get_state(self):
+        n = self.num_bodies
+        pos = np.zeros((n, 3), np.float32)
+        quat = np.zeros((n, 4), np.float32)
+        vel = np.zeros((n, 3), np.float32)
+        omega = np.zeros((n, 3), np.float32)
+        check(self._lib.avbd_get_state(self._h, _fp(pos), _fp(quat), _fp(vel), _fp(omega)), "get_state")
+        return pos, quat, vel, omega
+
+    def set_state(self, pos=None, quat=None, vel=None, omega=None):
+        n = self.num_bodies
+        arrs = [None if a is None else _f(a, n * k) for a, k in ((pos, 3), (quat, 4), (vel, 3), (omega, 3))]
+        check(self._lib.avbd_set_state(self._h, *[None if a is None else _fp(a) for a in arrs]), "set_state")
+
+    def contacts(self):
+        """Live manifolds: {(A, B): (ids, data[n, 16])}, data as the oracle reports it."""
+        n = check(self._lib.avbd_get_contacts(self._h, 0, None, None, None, None), "get_contacts")
+        m = max(n, 1)
+        pairs = np.zeros((m, 2), np.int32)
+        counts = np.zeros(m, np.int32)
+        ids = np.zeros((m, 8), np.uint32)
+        data = np.zeros((m, 8, 16), np.float32)
+        check(self._lib.avbd_get_contacts(self._h, n, pairs.ctypes.data_as(C.POINTER(C.c_int32)),
+                                          counts.ctypes.data_as(C.POINTER(C.c_int32)),
+                                          ids.ctypes.data_as(C.POINTER(C.c_uint32)), _fp(data)), "get_contacts")
+        return {(int(pairs[k, 0]), int(pairs[k, 1])): ([int(x) for x in ids[k, :counts[k]]], data[k, :counts[k]].copy())
+                for k in range(n)}
+
+    def colours(self):
+        c = np.zeros(self.num_bodies, np.int32)
+        k = check(self._lib.avbd_get_colours(self._h, c.ctypes.data_as(C.POINTER(C.c_int32))), "get_colours")
+        return c, k
+
+    def timings(self) -> dict:
+        t = AvbdTimings()
+        check(self._lib.avbd_get_timings(self._h, C.byref(t)), "get_timings")
+        return {name: getattr(t, name) for name, _ in AvbdTimings._fields_}
+
+    def collide(self, a, b):
+        """CollisionSpace::CollisionBoxBox on the device for bodies a, b as they stand."""
+        ids = np.zeros(8, np.uint32)
+        data = np.zeros((8, 13), np.float32)
+        n = check(self._lib.avbd_collide(self._h, int(a), int(b), ids.ctypes.data_as(C.POINTER(C.c_uint32)),
+                                         _fp(data)), "collide")
+        return [int(x) for x in ids[:n]], data[:n].copy()
+
+    def footprint_bytes(self):
+        return self._lib.avbd_scene_footprint_bytes(self._h)
+
+
+class Batch:
+    """Many independent scenes advanced by one persistent kernel per step."""
+
+    def __init__(self, iterations=10, dt=1.0 / 60.0, device=0, **kw):
+        self._lib = load()
+        self._p = default_params(num_iterations=int(iterations), step_value=float(dt))
+        for k, v in kw.items():
+            setattr(self._p, k, v)
+        h = C.c_void_p()
+        check(self._lib.avbd_batch_create(C.byref(self._p), int(device), C.byref(h)), "avbd_batch_create")
+        self._h = h
+
+    def close(self):
+        if getattr(self, "_h", None):
+            self._lib.avbd_batch_destroy(self._h)
+            self._h = None
+
+    def __del__(self):
+        try:
+            self.close()
+        except Exception:
+            pass
+
+    def add_scene(self, solver: Solver) -> int:
+        """Copies a staged (never stepped) Solver scene into the batch."""
+        return check(self._lib.avbd_batch_add_scene(self._h, solver.handle), "batch_add_scene")
+
+    def remove_scene(self, scene: int):
+        check(self._lib.avbd_batch_remove_scene(self._h, int(scene)), "batch_remove_scene")
+
+    def step(self, steps: int = 1) -> str:
+        r = check(self._lib.avbd_batch_step(self._h, int(steps)), "batch_step")
+        return STATUS.get(r, str(r))
+
+    @property
+    def num_scenes(self):
+        return self._lib.avbd_batch_num_scenes(self._h)
+
+    @property
+    def dynamic_bodies(self) -> int:
+        return int(self._lib.avbd_batch_dynamic_bodies(self._h))
+
+    def scene_status(self, scene: int) -> str:
+        r = check(self._lib.avbd_batch_scene_status(self._h, int(scene)), "scene_status")
+        return STATUS.get(r, str(r))
+
+    def scene_info(self, scene: int) -> dict:
+        out = (C.c_int32 * 6)()
+        check(self._lib.avbd_batch_scene_info(self._h, int(scene), out), "scene_info")
+        keys = ("status", "colours", "candidates", "contacts", "incidence", "steps")
+        return dict(zip(keys, list(out)))
+
+    def get_state(self, scene: int):
+        n = check(self._lib.avbd_batch_scene_bodies(self._h, int(scene)), "scene_bodies")
+        pos = np.zeros((n, 3), np.float32)
+        quat = np.zeros((n, 4), np.float32)
+        vel = np.zeros((n, 3), np.float32)
+        omega = np.zeros((n, 3), np.float32)
+        check(self._lib.avbd_batch_get_state(self._h, int(scene), _fp(pos), _fp(quat), _fp(vel), _fp(omega)),
+              "batch_get_state")
+        return pos, quat, vel, omega
+
+    def set_launch(self, threads_per_cta=0, ctas_per_sm=0):
+        check(self._lib.avbd_batch_set_launch(self._h, int(threads_per_cta), int(ctas_per_sm)), "set_launch")
+
+    def launch(self):
+        t = C.c_int32()
+        c = C.c_int32()
+        check(self._lib.avbd_batch_get_launch(self._h, C.byref(t), C.byref(c)), "get_launch")
+        return t.value, c.value
+
+    @property
+    def last_ms(self) -> float:
+        return float(self._lib.avbd_batch_last_ms(self._h))
+
+
+__all__ = ["Solver", "Batch", "AvbdError", "INF"]
