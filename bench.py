@@ -1,0 +1,394 @@
+"""AVBD throughput on one B200 (or N, one process per GPU): body-iterations/s.
+
+Workload (default): the batched scene mix — 4,096 independent seeded scenes
+per step, box counts log-uniform 8-2,048 (stacks and piles on a ground box),
+25% Neo-Hookean blocks of 500-5,000 tets (0.2 m cell), dt = 1/60 s,
+10 iterations, FP32; one persistent kernel per step, replayed from a CUDA
+graph.  A body-iteration is one primal block update of one dynamic body in
+one of the iteration sweeps (the post-stabilisation sweep is extra work and
+is not counted).
+
+Printed JSON line (rank 0): value = device throughput with scenes resident;
+e2e = the same metric through the public C-ABI with the batch uploaded from
+host memory and every step's poses read back to pinned host memory inside
+the timed region; plain_gpu = the single-scene GPU path on a sample of the
+same scenes, one scene at a time; roofline of the persistent kernel; clocks
+sampled during the timed region; cpu_baseline = the reference step (the
+oracle build of the reference's own sources) on the host cores.
+
+    python bench.py [--gpus N] [--steps K] [--warmup W] [--impl reference]
+"""
+from __future__ import annotations
+
+import argparse
+import json
+import os
+import subprocess
+import sys
+import threading
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+sys.path.insert(0, ROOT)
+
+METRIC = "AVBD body-iters/s batched+served vs plain GPU at 1e-4 tol; p50/p99 latency"
+UNIT = "body-iters/s"
+ITERS = 10
+
+# per-iteration algorithmic bytes of the step (compulsory reads + writes)
+BYTES_BODY = 160       # pose, last pose, inertial pose, mass/inertia read; pose written
+BYTES_CONTACT = 216    # J rows (n, t1, t2 and both arms), C0, friction, pair/ids, penalty+lambda r/w
+BYTES_JOINT = 264
+BYTES_SPRING = 48
+BYTES_TET = 64         # indices, Dm^-1, rest volume, Lame parameters
+
+
+def measured_peaks():
+    path = os.path.join(ROOT, "MEASURED_PEAKS.json")
+    if os.path.exists(path):
+        with open(path) as f:
+            d = json.load(f)
+        return float(d.get("hbm_gbs", 6650.0)), "measured"
+    return 6650.0, "fallback"
+
+
+class ClockSampler:
+    """nvidia-smi clocks and throttle reasons sampled during the timed region."""
+
+    FIELDS = ("index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,"
+              "clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,"
+              "clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap")
+
+    def __init__(self, gpu_index: int):
+        self.gpu = gpu_index
+        self.proc = None
+        self.lines = []
+        self._t = None
+
+    def start(self):
+        try:
+            self.proc = subprocess.Popen(
+                ["nvidia-smi", f"--id={self.gpu}", f"--query-gpu={self.FIELDS}", "--format=csv,noheader,nounits",
+                 "-lms", "100"], stdout=subprocess.PIPE, stderr=subprocess.DEVNULL, text=True)
+            self._t = threading.Thread(target=self._read, daemon=True)
+            self._t.start()
+        except OSError:
+            self.proc = None
+
+    def _read(self):
+        for line in self.proc.stdout:
+            self.lines.append(line.strip())
+
+    def stop(self):
+        if self.proc is None:
+            return {"sm_mhz": None, "sm_max_mhz": None, "reasons": ["nvidia-smi unavailable"]}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except subprocess.TimeoutExpired:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ["hw_slowdown", "hw_thermal_slowdown", "sw_thermal_slowdown", "sw_power_cap"]
+        for ln in self.lines:
+            parts = [p.strip() for p in ln.split(",")]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for nm, v in zip(names, parts[5:9]):
+                if v.lower() == "active":
+                    reasons.add(nm)
+        return {"sm_mhz": float(np.median(sm)) if sm else None, "sm_max_mhz": smax, "reasons": sorted(reasons),
+                "samples": len(sm)}
+
+
+def build_batch(specs, config_base=4):
+    """Stages every scene and adds it to a Batch; returns (batch, staged, counts)."""
+    from skyephyx_b200 import Batch, Solver, scenes
+    batch = Batch(iterations=ITERS)
+    staged = []
+    counts = dict(dynamic=0, joints=0, springs=0, tets=0, bodies=0)
+    for sp in specs:
+        s = Solver(iterations=ITERS)
+        cnt = _Counter(s)
+        scenes.build_spec(cnt, sp, config=config_base)
+        batch.add_scene(s)
+        staged.append(s)
+        counts["dynamic"] += s.num_dynamic
+        counts["bodies"] += s.num_bodies
+        counts["joints"] += cnt.joints
+        counts["springs"] += cnt.springs
+        counts["tets"] += cnt.tets
+    return batch, staged, counts
+
+
+class _Counter:
+    """Forwards scene calls to a solver and counts forces and energies."""
+
+    def __init__(self, s):
+        self.s = s
+        self.joints = self.springs = self.tets = 0
+
+    def __getattr__(self, name):
+        return getattr(self.s, name)
+
+    def add_joint(self, *a, **k):
+        self.joints += 1
+        return self.s.add_joint(*a, **k)
+
+    def add_spring(self, *a, **k):
+        self.springs += 1
+        return self.s.add_spring(*a, **k)
+
+    def make_tet_volume(self, ox, oy, oz, nx, ny, nz, *a, **k):
+        self.tets += 5 * (nx - 1) * (ny - 1) * (nz - 1)
+        return self.s.make_tet_volume(ox, oy, oz, nx, ny, nz, *a, **k)
+
+
+def pinned(shape):
+    try:
+        import torch
+        return torch.empty(shape, dtype=torch.float32, pin_memory=True).numpy()
+    except Exception:
+        return np.empty(shape, np.float32)
+
+
+def run_plain_sample(specs, steps, warmup):
+    """The single-scene GPU path on each sampled scene in turn (host-synchronous steps)."""
+    from skyephyx_b200 import Solver, scenes
+    total_iters = 0
+    total_s = 0.0
+    for sp in specs:
+        s = Solver(iterations=ITERS)
+        scenes.build_spec(s, sp)
+        for _ in range(warmup):
+            s.step()
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            s.step()
+        total_s += time.perf_counter() - t0
+        total_iters += s.num_dynamic * ITERS * steps
+        s.close()
+    return total_iters / total_s, total_iters, total_s
+
+
+def cpu_baseline(specs, steps, threads):
+    """The reference step (oracle build of the reference sources, Release-like flags) on host threads."""
+    from oracle import oracle
+    from skyephyx_b200 import scenes
+    sols = []
+    dyn = 0
+    for sp in specs:
+        o = oracle.OracleSolver(iterations=ITERS, fast=True)
+        scenes.build_spec(o, sp)
+        sols.append(o)
+        dyn += o.num_dynamic
+    oracle.step_many(sols, 1, threads, coloured=False, fast=True)   # warm-up step
+    ms = oracle.step_many(sols, steps, threads, coloured=False, fast=True)
+    return dyn * ITERS * steps / (ms / 1e3), dyn, ms
+
+
+def dist_env():
+    ws = int(os.environ.get("WORLD_SIZE", "1"))
+    rank = int(os.environ.get("RANK", "0"))
+    local = int(os.environ.get("LOCAL_RANK", "0"))
+    return ws, rank, local
+
+
+def reference_arm(args):
+    """Times the reference's own CPU step on the host cores (bounded sample per step)."""
+    ws, rank, _ = dist_env()
+    if rank != 0:
+        return
+    from skyephyx_b200 import scenes
+    specs = scenes.batch_mix_specs(n_scenes=args.scenes)
+    sample = specs[: args.cpu_scenes]
+    threads = os.cpu_count() or 1
+    from oracle import oracle
+    sols = []
+    dyn = 0
+    for sp in sample:
+        o = oracle.OracleSolver(iterations=ITERS, fast=True)
+        scenes.build_spec(o, sp)
+        sols.append(o)
+        dyn += o.num_dynamic
+    oracle.step_many(sols, args.warmup, threads, coloured=False, fast=True)
+    ms = oracle.step_many(sols, args.steps, threads, coloured=False, fast=True)
+    v = dyn * ITERS * args.steps / (ms / 1e3)
+    line = {
+        "impl": "reference", "metric": METRIC, "value": v, "unit": UNIT, "n_gpus": args.gpus, "steps": args.steps,
+        "warmup": args.warmup, "ms_per_step": ms / args.steps, "higher_is_better": True, "scaling": "weak",
+        "vs_baseline": None, "dtype": "f32", "data": "synthetic (seeded scene generator)",
+        "config": {"workload": f"batched mix of {args.scenes} scenes (reference CPU step on a {len(sample)}-scene "
+                               f"sample per step)", "iterations": ITERS, "dt": 1.0 / 60.0},
+        "cpu_baseline": {"value": v, "unit": UNIT, "cores": threads, "kind": "reference",
+                         "sample": f"first {len(sample)} scenes of the mix ({dyn} dynamic bodies), "
+                                   f"{args.steps} steps, one Solver per scene on {threads} threads"},
+        "e2e": {"value": v, "unit": UNIT, "h2d_bytes_per_step": 0, "d2h_bytes_per_step": 0},
+    }
+    print(json.dumps(line), flush=True)
+
+
+def main():
+    ap = argparse.ArgumentParser()
+    ap.add_argument("--gpus", type=int, default=1)
+    ap.add_argument("--steps", type=int, default=10)
+    ap.add_argument("--warmup", type=int, default=3)
+    ap.add_argument("--impl", default="ours", choices=["ours", "reference"])
+    ap.add_argument("--scenes", type=int, default=4096)
+    ap.add_argument("--plain-scenes", type=int, default=24)
+    ap.add_argument("--cpu-scenes", type=int, default=128)
+    ap.add_argument("--no-cpu", action="store_true")
+    args = ap.parse_args()
+    if args.warmup < 3:
+        args.warmup = 3
+
+    if args.impl == "reference":
+        reference_arm(args)
+        return
+
+    ws, rank, local = dist_env()
+    dist = None
+    if ws > 1:
+        import datetime
+        import torch
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
+    device = local
+
+    from skyephyx_b200 import scenes
+    specs = scenes.batch_mix_specs(n_scenes=args.scenes)
+    if ws > 1:   # weak scaling: every rank runs its own seeded mix of the same size
+        specs = [(k, n, i + rank * args.scenes) for (k, n, i) in specs]
+
+    t_build = time.perf_counter()
+    batch, staged, counts = build_batch(specs)
+    build_s = time.perf_counter() - t_build
+
+    # ---- e2e: upload from host + steps + per-step pose readback to pinned host memory ----
+    nb_total = counts["bodies"]
+    pos_h = pinned((nb_total, 4))
+    rot_h = pinned((nb_total, 4))
+
+    def barrier():
+        if dist is not None:
+            dist.barrier()
+
+    barrier()
+    t0 = time.perf_counter()
+    batch.step(1)                                 # packs + uploads the staged scenes, first step
+    for _ in range(args.steps - 1):
+        batch.step(1)
+        batch._lib.avbd_batch_get_all_poses(batch._h, pos_h.ctypes.data_as(_fp_t()),
+                                            rot_h.ctypes.data_as(_fp_t()), nb_total)
+    batch._lib.avbd_batch_get_all_poses(batch._h, pos_h.ctypes.data_as(_fp_t()), rot_h.ctypes.data_as(_fp_t()),
+                                        nb_total)
+    e2e_s = time.perf_counter() - t0
+    e2e_s = _max_over_ranks(dist, e2e_s)
+    body_iters_step = counts["dynamic"] * ITERS
+    e2e_value = ws * body_iters_step * args.steps / e2e_s
+    upload_bytes = sum(s.footprint_bytes() for s in staged)
+    d2h_step = 2 * nb_total * 16
+
+    # ---- device throughput: scenes resident, K steps of one persistent kernel each ----
+    batch.step(args.warmup)
+    clocks = ClockSampler(device)
+    clocks.start()
+    time.sleep(0.3)
+    barrier()
+    tw = time.perf_counter()
+    batch.step(args.steps)
+    wall = time.perf_counter() - tw
+    dev_ms = batch.last_ms
+    barrier()
+    time.sleep(0.2)
+    clk = clocks.stop()
+    dev_ms = _max_over_ranks(dist, dev_ms)
+    ms_per_step = dev_ms / args.steps
+    value = ws * body_iters_step / (ms_per_step / 1e3)
+
+    # statuses and live contacts after the timed steps
+    ncontacts = 0
+    bad = {}
+    for i in range(len(specs)):
+        info = batch.scene_info(i)
+        ncontacts += info["contacts"]
+        if info["status"] != 0:
+            bad[info["status"]] = bad.get(info["status"], 0) + 1
+    alg_bytes = ITERS * (BYTES_BODY * counts["dynamic"] + BYTES_CONTACT * ncontacts + BYTES_JOINT * counts["joints"]
+                         + BYTES_SPRING * counts["springs"] + BYTES_TET * counts["tets"])
+    peak, peak_kind = measured_peaks()
+    achieved = alg_bytes / (ms_per_step / 1e3) / 1e9
+    threads, ctas = batch.launch()
+
+    if rank != 0:
+        if dist is not None:
+            dist.barrier()
+            dist.destroy_process_group()
+        return
+
+    # ---- plain single-scene GPU path on a sample of the same scenes ----
+    plain_specs = specs[: args.plain_scenes]
+    plain_v, plain_iters, plain_s = run_plain_sample(plain_specs, steps=3, warmup=1)
+
+    cpu = None
+    if not args.no_cpu:
+        cpu_specs = specs[: args.cpu_scenes]
+        threads_cpu = os.cpu_count() or 1
+        cv, cdyn, cms = cpu_baseline(cpu_specs, steps=3, threads=threads_cpu)
+        cpu = {"value": cv, "unit": UNIT, "cores": threads_cpu, "kind": "reference",
+               "sample": f"first {len(cpu_specs)} scenes of the mix ({cdyn} dynamic bodies), 3 steps, "
+                         f"reference Solver::Step per scene on {threads_cpu} threads"}
+
+    line = {
+        "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
+        "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
+        "dtype": "f32", "data": "synthetic (seeded scene generator; no public dataset)",
+        "config": {"workload": f"batched mix: {len(specs)} scenes, box counts log-uniform 8-2048, 25% Neo-Hookean "
+                               f"blocks of 500-5000 tets; dt=1/60, {ITERS} iterations",
+                   "scenes": len(specs), "dynamic_bodies": counts["dynamic"], "tets": counts["tets"],
+                   "live_contacts": ncontacts, "l2": "working set larger than L2 (126 MB)",
+                   "launch": {"threads_per_cta": threads, "ctas_per_sm": ctas}, "parallelism": f"scenes x{ws}"},
+        "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(upload_bytes / args.steps),
+                "d2h_bytes_per_step": d2h_step,
+                "note": "batch upload from host memory on the first step, every step's poses read back"},
+        "gpu_launches": args.steps,
+        "plain_gpu": {"value": plain_v, "unit": UNIT, "sample": f"first {len(plain_specs)} scenes, 3 steps each",
+                      "batched_over_plain": value / plain_v if plain_v else None},
+        "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
+                     "traffic": None, "peak_kind": peak_kind,
+                     "algorithmic_bytes_per_launch": alg_bytes},
+        "clocks": clk,
+        "cpu_baseline": cpu,
+        "status_counts": bad,
+        "build_s": build_s,
+        "wall_ms_per_step": wall * 1e3 / args.steps,
+    }
+    print(json.dumps(line), flush=True)
+    if dist is not None:
+        dist.barrier()
+        dist.destroy_process_group()
+
+
+def _fp_t():
+    import ctypes
+    return ctypes.POINTER(ctypes.c_float)
+
+
+def _max_over_ranks(dist, x):
+    if dist is None:
+        return x
+    import torch
+    t = torch.tensor([float(x)], device="cuda")
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+if __name__ == "__main__":
+    main()

@@ -94,6 +94,12 @@ int32_t avbd_get_params(const AvbdWorld* w, AvbdParams* out);
 int32_t avbd_add_body(AvbdWorld* w, int32_t model_type, float density, float friction, const float pos[3],
                       const float scale[3], const float vel[3], const float quat_wxyz[4], const float omega[3],
                       int32_t is_static);
+/* n calls of Solver::AddBody with one model type, from arrays (density[n],
+ * friction[n], pos[3n], scale[3n], quat_wxyz[4n], is_static[n]; vel/omega
+ * [3n] may be NULL for zero). Returns the id of the first body. */
+int32_t avbd_add_bodies(AvbdWorld* w, int32_t n, int32_t model_type, const float* density, const float* friction,
+                        const float* pos, const float* scale, const float* vel, const float* quat_wxyz,
+                        const float* omega, const int32_t* is_static);
 /* Solver::AddParticle (solver.cpp:119-131): a 0.1 m cube with zero inertia. */
 int32_t avbd_add_particle(AvbdWorld* w, float mass, float friction, const float pos[3], const float vel[3],
                           int32_t is_static);

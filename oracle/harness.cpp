@@ -370,6 +370,19 @@ int orc_add_box(void* h, int model_type, float density, float friction, const fl
     return (int)o->bodies.size() - 1;
 }
 
+// n x Solver::AddBody from arrays (vel / omega may be null = zero).
+int orc_add_bodies(void* h, int n, int model_type, const float* density, const float* friction, const float* pos,
+                   const float* scale, const float* vel, const float* quat, const float* omega, const int* is_static) {
+    const float zero[3] = {0.f, 0.f, 0.f};
+    int first = -1;
+    for (int i = 0; i < n; ++i) {
+        int id = orc_add_box(h, model_type, density[i], friction[i], pos + 3 * i, scale + 3 * i,
+                             vel ? vel + 3 * i : zero, quat + 4 * i, omega ? omega + 3 * i : zero, is_static[i]);
+        if (i == 0) first = id;
+    }
+    return first;
+}
+
 // Solver::AddParticle (solver.cpp:119-131).
 int orc_add_particle(void* h, float mass, float friction, const float* pos, const float* vel, int is_static) {
     Orc* o = static_cast<Orc*>(h);

@@ -52,6 +52,7 @@ def _lib(fast: bool = False):
                             C.c_int], None),
         "orc_add_box": ([vp, C.c_int, C.c_float, C.c_float, fp, fp, fp, fp, fp, C.c_int], C.c_int),
         "orc_add_particle": ([vp, C.c_float, C.c_float, fp, fp, C.c_int], C.c_int),
+        "orc_add_bodies": ([vp, C.c_int, C.c_int, fp, fp, fp, fp, fp, fp, fp, ip], C.c_int),
         "orc_set_static": ([vp, C.c_int, C.c_int], C.c_int),
         "orc_add_spring": ([vp, C.c_int, fp, C.c_int, fp, C.c_float, C.c_float, C.c_int, C.c_float], C.c_int),
         "orc_add_joint": ([vp, C.c_int, fp, C.c_int, fp, fp, fp], C.c_int),
@@ -125,6 +126,15 @@ class OracleSolver:
         p, s, v, q, w = _f(pos, 3), _f(scale, 3), _f(vel, 3), _f(quat, 4), _f(omega, 3)
         return self._lib.orc_add_box(self._h, int(model_type), float(density), float(friction), _fp(p), _fp(s),
                                      _fp(v), _fp(q), _fp(w), int(bool(is_static)))
+
+    def add_bodies(self, model_type, density, friction, pos, scale, quat, is_static, vel=None, omega=None):
+        c = lambda a: None if a is None else np.ascontiguousarray(np.asarray(a, np.float32).reshape(-1))
+        arrs = [c(pos), c(scale), c(quat), c(density), c(friction), c(vel), c(omega)]
+        n = arrs[0].size // 3
+        st = np.ascontiguousarray(np.asarray(is_static, np.int32).reshape(-1))
+        ptr = [None if a is None else _fp(a) for a in arrs]
+        return self._lib.orc_add_bodies(self._h, n, int(model_type), ptr[3], ptr[4], ptr[0], ptr[1], ptr[5], ptr[2],
+                                        ptr[6], st.ctypes.data_as(C.POINTER(C.c_int)))
 
     def add_particle(self, mass, friction, pos, vel=(0, 0, 0), is_static=False):
         p, v = _f(pos, 3), _f(vel, 3)

@@ -55,6 +55,7 @@ SIGNATURES = [
     ("avbd_set_params", [_V, C.POINTER(AvbdParams)], C.c_int32),
     ("avbd_get_params", [_V, C.POINTER(AvbdParams)], C.c_int32),
     ("avbd_add_body", [_V, C.c_int32, C.c_float, C.c_float, _F, _F, _F, _F, _F, C.c_int32], C.c_int32),
+    ("avbd_add_bodies", [_V, C.c_int32, C.c_int32, _F, _F, _F, _F, _F, _F, _F, _I], C.c_int32),
     ("avbd_add_particle", [_V, C.c_float, C.c_float, _F, _F, C.c_int32], C.c_int32),
     ("avbd_set_body_static", [_V, C.c_int32, C.c_int32], C.c_int32),
     ("avbd_add_spring", [_V, C.c_int32, _F, C.c_int32, _F, C.c_float, C.c_float, C.c_int32, C.c_float], C.c_int32),

@@ -322,8 +322,8 @@ struct Pools {
 // Capacity policy of one scene.
 void scene_caps(const HostScene& h, int& candcap, int& kcap) {
     const int n = h.nbody();
-    candcap = 8 * n + 64;
-    kcap = 16 * n + 128;
+    candcap = 16 * n + 64;   // a body in a column stack overlaps ~18 circumscribed spheres (owns ~9)
+    kcap = 24 * n + 128;
 }
 
 template <typename T>
@@ -821,6 +821,20 @@ int32_t avbd_add_body(AvbdWorld* w, int32_t model, float density, float friction
     AVBD_STAGING_ONLY(w);
     if (!pos || !scale || !vel || !quat || !omega || model < 0 || model > 2) return AVBD_ERR_INVALID;
     return w->h.add_body(model, density, friction, pos, scale, vel, quat, omega, is_static != 0);
+}
+
+int32_t avbd_add_bodies(AvbdWorld* w, int32_t n, int32_t model, const float* density, const float* friction,
+                        const float* pos, const float* scale, const float* vel, const float* quat, const float* omega,
+                        const int32_t* is_static) {
+    AVBD_STAGING_ONLY(w);
+    if (n < 0 || !density || !friction || !pos || !scale || !quat || !is_static || model < 0 || model > 2)
+        return AVBD_ERR_INVALID;
+    const float zero[3] = {0.f, 0.f, 0.f};
+    const int first = w->h.nbody();
+    for (int i = 0; i < n; ++i)
+        w->h.add_body(model, density[i], friction[i], pos + 3 * i, scale + 3 * i, vel ? vel + 3 * i : zero,
+                      quat + 4 * i, omega ? omega + 3 * i : zero, is_static[i] != 0);
+    return first;
 }
 
 int32_t avbd_add_particle(AvbdWorld* w, float mass, float friction, const float pos[3], const float vel[3],

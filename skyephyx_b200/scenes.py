@@ -28,14 +28,16 @@ def f32(x):
 
 
 def v3(x, y, z):
-    return np.array([x, y, z], np.float32)
+    """A 3-vector rounded to float32 once (a tuple of the float32 values)."""
+    return (float(np.float32(x)), float(np.float32(y)), float(np.float32(z)))
 
 
 def quat_axis_angle(axis, angle):
     axis = np.asarray(axis, np.float64)
     axis = axis / np.linalg.norm(axis)
     h = 0.5 * angle
-    return np.array([math.cos(h), *(math.sin(h) * axis)], np.float32)   # (w, x, y, z)
+    q = np.array([math.cos(h), *(math.sin(h) * axis)], np.float32)   # (w, x, y, z)
+    return tuple(float(v) for v in q)
 
 
 def rng_for(config: int, scene: int = 0) -> np.random.Generator:
@@ -55,13 +57,30 @@ def pyramid_wall(s, rows=20, density=1000.0, friction=0.5, pitch=1.05, x0=0.0, z
     box (100 x 1 x 100 m, top at y = 0); the reference has no plane collider."""
     if ground:
         _ground(s, 50.0, 50.0, 0.0, friction)
-    ids = []
+    pos = []
     for r in range(rows):
         n = rows - r
         for k in range(n):
-            x = x0 + (k - 0.5 * (n - 1)) * pitch
-            ids.append(s.add_body(CUBE, density, friction, v3(x, 0.5 + r, z0), v3(1, 1, 1)))
-    return ids
+            pos.append((x0 + (k - 0.5 * (n - 1)) * pitch, 0.5 + r, z0))
+    return _bulk_boxes(s, np.array(pos), np.ones((len(pos), 3)), None, density, friction)
+
+
+def _bulk_boxes(s, pos, scale, yaw, density, friction):
+    """Adds boxes (float32-rounded) through the solver's bulk insert; returns their ids."""
+    n = len(pos)
+    if n == 0:
+        return []
+    pos = np.asarray(pos, np.float32)
+    scale = np.asarray(scale, np.float32)
+    quat = np.zeros((n, 4), np.float32)
+    quat[:, 0] = 1.0
+    if yaw is not None:
+        h = 0.5 * np.asarray(yaw, np.float64)
+        quat[:, 0] = np.cos(h)
+        quat[:, 2] = np.sin(h)
+    first = s.add_bodies(CUBE, np.full(n, density, np.float32), np.full(n, friction, np.float32), pos, scale, quat,
+                         np.zeros(n, np.int32))
+    return list(range(first, first + n))
 
 
 def fem_block(s, nx=41, ny=11, nz=11, cell=0.05, E=1e5, nu=0.3, density=1000.0, origin=(0.0, 0.0, 0.0),
@@ -85,20 +104,14 @@ def mixed_large(s, n_boxes=32768, n_chains=64, links=32, n_springs=2048, seed_sc
         s.add_body(CUBE, 1.0, 0.5, v3(x, 15, z), v3(sx, 30, sz), is_static=True)
     pitch = 1.6
     nxz = 50
-    ny = max(1, int(math.ceil(n_boxes / (nxz * nxz))))
-    boxes = []
-    for j in range(ny):
-        for k in range(nxz):
-            for i in range(nxz):
-                if len(boxes) >= n_boxes:
-                    break
-                edge = rng.uniform(0.5, 1.5, 3)
-                jit = rng.uniform(-0.05, 0.05, 3)
-                yaw = rng.uniform(-0.1, 0.1)
-                pos = ((i - 0.5 * (nxz - 1)) * pitch + jit[0], 0.8 + j * pitch + jit[1],
-                       (k - 0.5 * (nxz - 1)) * pitch + jit[2])
-                boxes.append(s.add_body(CUBE, 1000.0, 0.5, v3(*pos), edge.astype(np.float32),
-                                        quat=quat_axis_angle((0, 1, 0), yaw)))
+    idx = np.arange(n_boxes)
+    i, k, j = idx % nxz, (idx // nxz) % nxz, idx // (nxz * nxz)
+    edge = rng.uniform(0.5, 1.5, (n_boxes, 3))
+    jit = rng.uniform(-0.05, 0.05, (n_boxes, 3))
+    yaw = rng.uniform(-0.1, 0.1, n_boxes)
+    pos = np.stack([(i - 0.5 * (nxz - 1)) * pitch + jit[:, 0], 0.8 + j * pitch + jit[:, 1],
+                    (k - 0.5 * (nxz - 1)) * pitch + jit[:, 2]], axis=1)
+    boxes = _bulk_boxes(s, pos, edge, yaw, 1000.0, 0.5)
     # horizontal hinge chains from world anchors at y = 45 (links 1.0 x 0.3 x 0.3 m)
     for c in range(n_chains):
         cx = -0.5 * links
@@ -120,38 +133,26 @@ def mixed_large(s, n_boxes=32768, n_chains=64, links=32, n_springs=2048, seed_sc
 
 
 def rigid_pile(s, n_boxes, rng, stack=True):
-    """A batched rigid scene: `n_boxes` unit-ish boxes as a stack of columns
-    (stack=True) or a loose jittered pile, on a static ground box."""
+    """A batched rigid scene: `n_boxes` boxes as columns of unit cubes resting
+    on each other (stack=True) or a loose jittered pile of boxes with edges
+    U[0.6, 1.0] m and yaw U[-0.3, 0.3] rad dropped in place, on a static ground box."""
     _ground(s, 20.0, 20.0, 0.0)
+    idx = np.arange(n_boxes)
     if stack:
         cols = max(1, int(math.ceil(math.sqrt(n_boxes / 8.0))))
-        placed = 0
-        lvl = 0
-        while placed < n_boxes:
-            for ci in range(cols):
-                for cj in range(cols):
-                    if placed >= n_boxes:
-                        break
-                    x = (ci - 0.5 * (cols - 1)) * 1.1
-                    z = (cj - 0.5 * (cols - 1)) * 1.1
-                    s.add_body(CUBE, 1000.0, 0.5, v3(x, 0.5 + lvl * 1.0, z), v3(1, 1, 1))
-                    placed += 1
-            lvl += 1
-    else:
-        side = max(1, int(math.ceil(n_boxes ** (1.0 / 3.0))))
-        placed = 0
-        for j in range(side * 4):
-            for k in range(side):
-                for i in range(side):
-                    if placed >= n_boxes:
-                        break
-                    e = rng.uniform(0.6, 1.0, 3)
-                    jit = rng.uniform(-0.05, 0.05, 3)
-                    pos = ((i - 0.5 * (side - 1)) * 1.3 + jit[0], 0.6 + j * 1.3 + jit[1],
-                           (k - 0.5 * (side - 1)) * 1.3 + jit[2])
-                    s.add_body(CUBE, 1000.0, 0.5, v3(*pos), e.astype(np.float32),
-                               quat=quat_axis_angle((0, 1, 0), rng.uniform(-0.3, 0.3)))
-                    placed += 1
+        per = cols * cols
+        lvl, c = idx // per, idx % per
+        ci, cj = c // cols, c % cols
+        pos = np.stack([(ci - 0.5 * (cols - 1)) * 1.1, 0.5 + lvl * 1.0, (cj - 0.5 * (cols - 1)) * 1.1], axis=1)
+        return _bulk_boxes(s, pos, np.ones((n_boxes, 3)), None, 1000.0, 0.5)
+    side = max(1, int(math.ceil(n_boxes ** (1.0 / 3.0))))
+    i, k, j = idx % side, (idx // side) % side, idx // (side * side)
+    e = rng.uniform(0.6, 1.0, (n_boxes, 3))
+    jit = rng.uniform(-0.05, 0.05, (n_boxes, 3))
+    yaw = rng.uniform(-0.3, 0.3, n_boxes)
+    pos = np.stack([(i - 0.5 * (side - 1)) * 1.3 + jit[:, 0], 0.6 + j * 1.3 + jit[:, 1],
+                    (k - 0.5 * (side - 1)) * 1.3 + jit[:, 2]], axis=1)
+    return _bulk_boxes(s, pos, e, yaw, 1000.0, 0.5)
 
 
 def fem_scene(s, n_tets, rng):
@@ -237,8 +238,8 @@ def level_mass_springs(s):
 def level_joint_playground(s):
     """levels.h:203-329: hinge pendulum + rope bridge with one breakable link
     (fracture 2000) and three falling weights."""
-    cs = v3(2.0, 0.7, 0.7)
-    anchor = v3(0, 5, 0)
+    cs = np.array(v3(2.0, 0.7, 0.7), np.float32)
+    anchor = np.array(v3(0, 5, 0), np.float32)
     last = -1
     spawn = np.array([anchor[0] + cs[0] / 2, anchor[1], anchor[2]], np.float32)
     for i in range(5):
@@ -246,13 +247,13 @@ def level_joint_playground(s):
         s.add_joint(last, v3(0.5, 0, 0) if last >= 0 else anchor, b, v3(-0.5, 0, 0), HINGE)
         last = b
         spawn[0] += cs[0]
-    start = v3(-10, 5, -5)
-    cs = v3(2.0, 0.5, 3.0)
+    start = np.array(v3(-10, 5, -5), np.float32)
+    cs = np.array(v3(2.0, 0.5, 3.0), np.float32)
     n_links, spacing = 12, 1.0
     last = -1
     spawn = np.array([start[0] + cs[0] / 2, start[1], start[2]], np.float32)
     z_edge, z_world = 0.5, 0.5 * cs[2]
-    left = start - v3(spacing, 0, 0)
+    left = start - np.array(v3(spacing, 0, 0), np.float32)
     for i in range(n_links):
         b = s.add_body(CUBE, 1.0, 0.5, spawn.copy(), cs)
         fracture = 2000.0 if i == 6 else INF
@@ -261,15 +262,16 @@ def level_joint_playground(s):
             if last >= 0:
                 ra, rb = v3(0.5, 0, zs * z_edge), v3(-0.5, 0, zs * z_edge)
             else:
-                ra, rb = left + v3(0, 0, zs * z_world), v3(-0.5, 0, zs * z_edge)
+                ra, rb = left + np.array(v3(0, 0, zs * z_world), np.float32), v3(-0.5, 0, zs * z_edge)
             s.add_spring(last, ra, b, rb, 5000.0, -1.0, False, fracture)
         last = b
         spawn[0] += cs[0] + spacing
-    end = start + v3(cs[0] * n_links + (n_links - 1) * spacing, 0, 0)
-    right = end + v3(spacing, 0, 0)
+    end = start + np.array(v3(cs[0] * n_links + (n_links - 1) * spacing, 0, 0), np.float32)
+    right = end + np.array(v3(spacing, 0, 0), np.float32)
     for side in range(2):
         zs = 1.0 if side == 0 else -1.0
-        s.add_spring(-1, right + v3(0, 0, zs * z_world), last, v3(0.5, 0, zs * z_edge), INF, -1.0, False)
+        s.add_spring(-1, right + np.array(v3(0, 0, zs * z_world), np.float32), last, v3(0.5, 0, zs * z_edge), INF,
+                     -1.0, False)
     cx = float((start[0] + end[0]) * 0.5)
     bz = float(start[2])
     for (dx, y) in ((-0.5, 10.0), (0.5, 16.0), (0.0, 23.0)):

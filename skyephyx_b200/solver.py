@@ -18,14 +18,36 @@ from ._lib import AvbdError, AvbdParams, AvbdTimings, STATUS, check, default_par
 INF = float("inf")
 
 
+_FLOAT_ARRAYS = {n: C.c_float * n for n in (3, 4, 6)}
+
+
+class _Floats:
+    """A small float32 argument: a ctypes array (tuples) or a numpy buffer."""
+    __slots__ = ("buf", "size")
+
+    def __init__(self, buf, size):
+        self.buf = buf
+        self.size = size
+
+
 def _f(a, n):
+    if isinstance(a, (tuple, list)) and len(a) == n and n in _FLOAT_ARRAYS:
+        return _Floats(_FLOAT_ARRAYS[n](*a), n)
     arr = np.ascontiguousarray(np.asarray(a, dtype=np.float32).reshape(-1))
     if arr.size != n:
         raise ValueError(f"expected {n} floats, got {arr.size}")
     return arr
 
 
+def _bulk(pos, scale, quat, density, friction, vel=None, omega=None):
+    """Contiguous float32 buffers for a bulk body insert."""
+    c = lambda a: None if a is None else np.ascontiguousarray(np.asarray(a, np.float32).reshape(-1))
+    return [c(pos), c(scale), c(quat), c(density), c(friction), c(vel), c(omega)]
+
+
 def _fp(a):
+    if isinstance(a, _Floats):
+        return C.cast(a.buf, C.POINTER(C.c_float))
     return a.ctypes.data_as(C.POINTER(C.c_float))
 
 
@@ -76,6 +98,17 @@ class Solver:
         p, s, v, q, w = _f(pos, 3), _f(scale, 3), _f(vel, 3), _f(quat, 4), _f(omega, 3)
         return check(self._lib.avbd_add_body(self._h, int(model_type), float(density), float(friction), _fp(p),
                                              _fp(s), _fp(v), _fp(q), _fp(w), int(bool(is_static))), "add_body")
+
+    def add_bodies(self, model_type, density, friction, pos, scale, quat, is_static, vel=None, omega=None):
+        """n x Solver::AddBody from arrays (pos/scale/vel/omega [n,3], quat [n,4] w x y z,
+        density/friction/is_static [n]). Returns the first body id."""
+        arrs = _bulk(pos, scale, quat, density, friction, vel, omega)
+        n = arrs[0].shape[0] // 3
+        st = np.ascontiguousarray(np.asarray(is_static, np.int32).reshape(-1))
+        ptr = [None if a is None else _fp(a) for a in arrs]
+        return check(self._lib.avbd_add_bodies(self._h, n, int(model_type), ptr[3], ptr[4], ptr[0], ptr[1], ptr[5],
+                                               ptr[2], ptr[6], st.ctypes.data_as(C.POINTER(C.c_int32))),
+                     "add_bodies")
 
     def add_particle(self, mass, friction, pos, vel=(0, 0, 0), is_static=False):
         """Solver::AddParticle (solver.cpp:119-131)."""
