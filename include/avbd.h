@@ -156,6 +156,23 @@ int32_t avbd_get_timings(const AvbdWorld* w, AvbdTimings* out);
  * rA, rB, position); returns the contact count. Kernel-level parity check. */
 int32_t avbd_collide(AvbdWorld* w, int32_t body_a, int32_t body_b, uint32_t* ids, float* data);
 
+/* Allocation-free variant of avbd_collide for up to
+ * AVBD_COLLIDE_NOALLOC_MAX_PAIRS pairs (body_a[i], body_b[i]) per call. It has
+ * no counterpart in the reference. It is for callers that may not allocate
+ * device memory during a call (fixed memory budgets, custom pools, hosts
+ * where cudaMalloc/cudaFree would synchronise or fail): its device scratch is
+ * one fixed array of about 1.9 MB that every GPU loading this library holds
+ * until exit. Outputs go to caller-owned host buffers: ids[8n] (unused =
+ * 0xFFFFFFFF), data[8*13*n] (as avbd_collide), counts[n]. The world must have
+ * been uploaded (stepped, or avbd_collide called, once). The first call on a
+ * device looks up the scratch address, so make it before any stream capture.
+ * Calls share the scratch: calls that overlap on the GPU (several threads, or
+ * several worlds on one device) race. More pairs than the maximum, or an
+ * unknown body id, return AVBD_ERR_INVALID. */
+#define AVBD_COLLIDE_NOALLOC_MAX_PAIRS 4096
+int32_t avbd_collide_noalloc(AvbdWorld* w, int32_t n, const int32_t* body_a, const int32_t* body_b, uint32_t* ids,
+                             float* data, int32_t* counts);
+
 /* ---------------------------------------------------------------------------
  * Batched: many independent scenes advanced by one persistent kernel per step
  * (no reference counterpart; each scene behaves as its own Solver).

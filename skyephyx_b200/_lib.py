@@ -75,6 +75,7 @@ SIGNATURES = [
     ("avbd_get_colours", [_V, _I], C.c_int32),
     ("avbd_get_timings", [_V, C.POINTER(AvbdTimings)], C.c_int32),
     ("avbd_collide", [_V, C.c_int32, C.c_int32, _U, _F], C.c_int32),
+    ("avbd_collide_noalloc", [_V, C.c_int32, _I, _I, _U, _F, _I], C.c_int32),
     ("avbd_batch_create", [C.POINTER(AvbdParams), C.c_int32, C.POINTER(_V)], C.c_int32),
     ("avbd_batch_destroy", [_V], C.c_int32),
     ("avbd_batch_add_scene", [_V, _V], C.c_int32),

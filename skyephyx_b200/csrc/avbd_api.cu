@@ -1242,3 +1242,100 @@ int32_t avbd_batch_get_launch(const AvbdBatch* b, int32_t* threads, int32_t* cta
 float avbd_batch_last_ms(const AvbdBatch* b) { return b ? b->last_ms : -1.f; }
 
 }  // extern "C"
+
+// ===========================================================================
+// Allocation-free box-box collision queries.
+//
+// For callers that must not allocate device memory during a call: code
+// running under a fixed memory budget or a custom pool, hosts that forbid
+// cudaMalloc/cudaFree on their hot path (they synchronise the device and can
+// fail), and libraries embedded in another runtime that owns all allocations.
+// The scratch lives in one file-scope device array of fixed size instead.
+// ===========================================================================
+namespace {
+
+constexpr int kNoAllocMaxPairs = AVBD_COLLIDE_NOALLOC_MAX_PAIRS;
+
+struct NoAllocScratch {
+    int32_t body_a[kNoAllocMaxPairs];
+    int32_t body_b[kNoAllocMaxPairs];
+    int counts[kNoAllocMaxPairs];
+    uint32_t ids[kNoAllocMaxPairs * 8];
+    float data[kNoAllocMaxPairs * 8 * 13];
+};
+
+// Shared by every call on a device; it keeps the last call's contents.
+static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
+
+// Device address of g_noalloc_scratch per device, looked up once per device.
+constexpr int kNoAllocMaxDevices = 64;
+NoAllocScratch* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+
+__global__ void k_collide_pairs_noalloc(World W, NoAllocScratch* s, int n, int nbody) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
+        const int2 ab = make_int2(s->body_a[i], s->body_b[i]);
+        uint32_t* ids = s->ids + 8 * i;
+        float* data = s->data + 8 * 13 * i;
+        int cnt = 0;
+        if (ab.x >= 0 && ab.y >= 0 && ab.x < nbody && ab.y < nbody) {
+            Collision col;
+            collide_box_box(v3(W.pos[ab.x]), q4(W.rot[ab.x]), v3(W.scale[ab.x]), v3(W.pos[ab.y]), q4(W.rot[ab.y]),
+                            v3(W.scale[ab.y]), col);
+            cnt = col.n;
+            for (int k = 0; k < col.n; ++k) {
+                const Contact& c = col.c[k];
+                float* d = data + 13 * k;
+                ids[k] = c.id;
+                d[0] = c.penetration;
+                d[1] = c.normal.x; d[2] = c.normal.y; d[3] = c.normal.z;
+                d[4] = c.rA.x; d[5] = c.rA.y; d[6] = c.rA.z;
+                d[7] = c.rB.x; d[8] = c.rB.y; d[9] = c.rB.z;
+                d[10] = c.position.x; d[11] = c.position.y; d[12] = c.position.z;
+            }
+        }
+        // slots past the contact count keep nothing from an earlier call
+        for (int k = cnt; k < 8; ++k) {
+            ids[k] = 0xFFFFFFFFu;
+            for (int q = 0; q < 13; ++q) data[13 * k + q] = 0.f;
+        }
+        s->counts[i] = ab.x >= 0 && ab.y >= 0 && ab.x < nbody && ab.y < nbody ? cnt : -1;
+    }
+}
+
+}  // namespace
+
+extern "C" int32_t avbd_collide_noalloc(AvbdWorld* w, int32_t n, const int32_t* body_a, const int32_t* body_b,
+                                        uint32_t* ids, float* data, int32_t* counts) {
+    if (!w || n < 0 || (n > 0 && (!body_a || !body_b || !ids || !data || !counts))) return AVBD_ERR_INVALID;
+    if (n > kNoAllocMaxPairs) {
+        std::fprintf(stderr, "avbd_collide_noalloc: %d pairs exceed the maximum of %d per call\n", n,
+                     kNoAllocMaxPairs);
+        return AVBD_ERR_INVALID;
+    }
+    if (!w->uploaded) return AVBD_ERR_STATE;   // the world must already live on the device
+    if (w->device < 0 || w->device >= kNoAllocMaxDevices) return AVBD_ERR_INVALID;
+    if (cudaSetDevice(w->device) != cudaSuccess) return AVBD_ERR_CUDA;
+    if (!g_noalloc_ptr[w->device]) {
+        // one-time set-up on this device (with the device current): the host
+        // name g_noalloc_scratch is only a stand-in, the kernel needs this address
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return AVBD_ERR_CUDA;
+        g_noalloc_ptr[w->device] = static_cast<NoAllocScratch*>(p);
+    }
+    if (n == 0) return 0;
+    NoAllocScratch* s = g_noalloc_ptr[w->device];
+    cudaStream_t st = w->stream;
+    if (cudaMemcpyAsync(s->body_a, body_a, n * sizeof(int32_t), cudaMemcpyHostToDevice, st) != cudaSuccess ||
+        cudaMemcpyAsync(s->body_b, body_b, n * sizeof(int32_t), cudaMemcpyHostToDevice, st) != cudaSuccess)
+        return AVBD_ERR_CUDA;
+    k_collide_pairs_noalloc<<<(n + 127) / 128, 128, 0, st>>>(w->P.W, s, n, w->h.nbody());
+    if (cudaGetLastError() != cudaSuccess) return AVBD_ERR_CUDA;
+    if (cudaMemcpyAsync(counts, s->counts, n * sizeof(int32_t), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaMemcpyAsync(ids, s->ids, (size_t)n * 8 * sizeof(uint32_t), cudaMemcpyDeviceToHost, st) != cudaSuccess ||
+        cudaMemcpyAsync(data, s->data, (size_t)n * 8 * 13 * sizeof(float), cudaMemcpyDeviceToHost, st) != cudaSuccess)
+        return AVBD_ERR_CUDA;
+    if (cudaStreamSynchronize(st) != cudaSuccess) return AVBD_ERR_CUDA;
+    for (int i = 0; i < n; ++i)
+        if (counts[i] < 0) return AVBD_ERR_INVALID;
+    return 0;
+}

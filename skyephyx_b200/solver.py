@@ -221,6 +221,21 @@ class Solver:
                                          _fp(data)), "collide")
         return [int(x) for x in ids[:n]], data[:n].copy()
 
+    def collide_noalloc(self, body_a, body_b):
+        """avbd_collide over many pairs without any device allocation (fixed
+        device scratch). Returns (ids[n, 8], data[n, 8, 13], counts[n])."""
+        a = np.ascontiguousarray(np.asarray(body_a, np.int32))
+        b = np.ascontiguousarray(np.asarray(body_b, np.int32))
+        n = a.size
+        ids = np.zeros((n, 8), np.uint32)
+        data = np.zeros((n, 8, 13), np.float32)
+        counts = np.zeros(n, np.int32)
+        ip = C.POINTER(C.c_int32)
+        check(self._lib.avbd_collide_noalloc(self._h, n, a.ctypes.data_as(ip), b.ctypes.data_as(ip),
+                                             ids.ctypes.data_as(C.POINTER(C.c_uint32)), _fp(data),
+                                             counts.ctypes.data_as(ip)), "collide_noalloc")
+        return ids, data, counts
+
     def footprint_bytes(self):
         return self._lib.avbd_scene_footprint_bytes(self._h)
 
