@@ -262,10 +262,7 @@ def main():
         dist.init_process_group("nccl", timeout=datetime.timedelta(seconds=120))
     device = local
 
-    from skyephyx_b200 import scenes
-    specs = scenes.batch_mix_specs(n_scenes=args.scenes)
-    if ws > 1:   # weak scaling: every rank runs its own seeded mix of the same size
-        specs = [(k, n, i + rank * args.scenes) for (k, n, i) in specs]
+    specs = rank_specs(args.scenes, rank, ws)
 
     t_build = time.perf_counter()
     batch, staged, counts = build_batch(specs)
@@ -381,11 +378,23 @@ def _fp_t():
     return ctypes.POINTER(ctypes.c_float)
 
 
+def rank_specs(n_scenes, rank, world_size):
+    """Weak scaling: every rank runs its own seeded mix of n_scenes scenes
+    (scene seeds offset by rank, so no two ranks simulate the same scene)."""
+    from skyephyx_b200 import scenes
+    specs = scenes.batch_mix_specs(n_scenes=n_scenes)
+    if world_size > 1:
+        specs = [(k, n, i + rank * n_scenes) for (k, n, i) in specs]
+    return specs
+
+
 def _max_over_ranks(dist, x):
+    """MAX of a per-rank timing over all ranks (device tensor under NCCL, host tensor under gloo)."""
     if dist is None:
         return x
     import torch
-    t = torch.tensor([float(x)], device="cuda")
+    dev = "cuda" if dist.get_backend() == "nccl" else "cpu"
+    t = torch.tensor([float(x)], device=dev)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
