@@ -107,9 +107,10 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
-def build_batch(specs, config_base=4):
-    """Stages every scene and adds it to a Batch; returns (batch, staged, counts)."""
-    from skyephyx_b200 import Batch, Solver, scenes
+def build_batch(specs, config_base=4, tuned=None):
+    """Stages every scene and adds it to a Batch with the autotuned launch
+    shape for this mix; returns (batch, staged, counts)."""
+    from skyephyx_b200 import Batch, Solver, autotune, scenes
     batch = Batch(iterations=ITERS)
     staged = []
     counts = dict(dynamic=0, joints=0, springs=0, tets=0, bodies=0)
@@ -124,6 +125,10 @@ def build_batch(specs, config_base=4):
         counts["joints"] += cnt.joints
         counts["springs"] += cnt.springs
         counts["tets"] += cnt.tets
+    nfem = sum(1 for sp in specs if sp[0] == "fem")
+    cfg = tuned or autotune.lookup(autotune.signature(len(specs), nfem, counts["bodies"]))
+    autotune.apply(batch, cfg)
+    counts["launch"] = cfg
     return batch, staged, counts
 
 
@@ -332,7 +337,7 @@ def main():
 
     # ---- plain single-scene GPU path on a sample of the same scenes ----
     plain_specs = specs[: args.plain_scenes]
-    plain_v, plain_iters, plain_s = run_plain_sample(plain_specs, steps=3, warmup=1)
+    plain_v = run_plain_sample(plain_specs, steps=3, warmup=1)[0] if plain_specs else None
 
     cpu = None
     if not args.no_cpu:
@@ -351,13 +356,17 @@ def main():
                                f"blocks of 500-5000 tets; dt=1/60, {ITERS} iterations",
                    "scenes": len(specs), "dynamic_bodies": counts["dynamic"], "tets": counts["tets"],
                    "live_contacts": ncontacts, "l2": "working set larger than L2 (126 MB)",
-                   "launch": {"threads_per_cta": threads, "ctas_per_sm": ctas}, "parallelism": f"scenes x{ws}"},
+                   "launch": {"threads_per_cta": threads, "ctas_per_sm": ctas,
+                              "register_variant": counts["launch"]["variant"],
+                              "lanes_per_body": {"rigid": counts["launch"]["rigid_group"],
+                                                 "fem": counts["launch"]["fem_group"]}},
+                   "parallelism": f"scenes x{ws}"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(upload_bytes / args.steps),
                 "d2h_bytes_per_step": d2h_step,
                 "note": "batch upload from host memory on the first step, every step's poses read back"},
         "gpu_launches": args.steps,
         "plain_gpu": {"value": plain_v, "unit": UNIT, "sample": f"first {len(plain_specs)} scenes, 3 steps each",
-                      "batched_over_plain": value / plain_v if plain_v else None},
+                      "batched_over_plain": value / plain_v if plain_v else None} if plain_v else None,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
                      "traffic": None, "peak_kind": peak_kind,
                      "algorithmic_bytes_per_launch": alg_bytes},

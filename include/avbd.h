@@ -204,10 +204,18 @@ int64_t avbd_scene_footprint_bytes(const AvbdWorld* w);
 /* Per-scene counters after the last step: status, colours, candidate pairs,
  * contact points, incidence entries, steps taken (6 values). */
 int32_t avbd_batch_scene_info(AvbdBatch* b, int32_t scene, int32_t out[6]);
-/* Launch shape of the persistent kernel: threads per CTA and CTAs per SM
- * (0 = autotuned choice). */
+/* Launch shape of the persistent kernel: threads per CTA (32..256) and CTAs
+ * per SM (0 = as many as fit). */
 int32_t avbd_batch_set_launch(AvbdBatch* b, int32_t threads_per_cta, int32_t ctas_per_sm);
 int32_t avbd_batch_get_launch(const AvbdBatch* b, int32_t* threads_per_cta, int32_t* ctas_per_sm);
+/* Register budget of the persistent kernel build: 1 (about 156 registers per
+ * thread) .. 4 (64, some spilling); trades spills for resident warps. */
+int32_t avbd_batch_set_kernel(AvbdBatch* b, int32_t register_variant);
+/* Lanes that share one body's primal update (1, 2, 4, 8, 16 or 32), for rigid
+ * scenes and for FEM scenes; before the first step (autotuner knob). */
+int32_t avbd_batch_set_groups(AvbdBatch* b, int32_t rigid_group, int32_t fem_group);
+/* Same knob for a single world (0 = by scene kind); before the first step. */
+int32_t avbd_set_group(AvbdWorld* w, int32_t group);
 /* Device time of the last avbd_batch_step call in ms. */
 float avbd_batch_last_ms(const AvbdBatch* b);
 

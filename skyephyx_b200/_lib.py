@@ -91,7 +91,10 @@ SIGNATURES = [
     ("avbd_scene_footprint_bytes", [_V], C.c_int64),
     ("avbd_batch_set_launch", [_V, C.c_int32, C.c_int32], C.c_int32),
     ("avbd_batch_get_launch", [_V, _I, _I], C.c_int32),
+    ("avbd_batch_set_kernel", [_V, C.c_int32], C.c_int32),
     ("avbd_batch_last_ms", [_V], C.c_float),
+    ("avbd_batch_set_groups", [_V, C.c_int32, C.c_int32], C.c_int32),
+    ("avbd_set_group", [_V, C.c_int32], C.c_int32),
 ]
 
 

@@ -41,7 +41,12 @@ __global__ void k_bp_write(World W, int cur) {
     for (int b = sc.body0 + blockIdx.x * blockDim.x + threadIdx.x; b < sc.body0 + sc.nbody;
          b += gridDim.x * blockDim.x)
         broadphase_body(W, sc, b, W.cpair[cur] + sc.cand0 + W.cand_off[b], W.cand_cnt[b]);
-    if (blockIdx.x == 0 && threadIdx.x == 0) { W.sstate[0].kused[cur] = 0; W.sstate[0].need_k = 0; }
+    if (blockIdx.x == 0 && threadIdx.x == 0) {
+        W.sstate[0].kused[cur] = 0;
+        W.sstate[0].need_k = 0;
+        W.sstate[0].nlive[cur] = 0;
+        W.sstate[0].nmatched = 0;
+    }
 }
 
 __global__ void k_narrow(World W, int cur, int ncand, int old_count) {
@@ -55,7 +60,7 @@ __global__ void k_force_init(World W) {
     const SceneDesc sc = W.scenes[0];
     for (int f = sc.force0 + blockIdx.x * blockDim.x + threadIdx.x; f < sc.force0 + sc.nforce;
          f += gridDim.x * blockDim.x)
-        force_init(W, f);
+        if (force_init(W, f)) atomicAdd(&W.sstate[0].topo, 1);
 }
 
 __global__ void k_incidence_colour(World W, int cur) {
@@ -65,7 +70,7 @@ __global__ void k_incidence_colour(World W, int cur) {
         if (threadIdx.x == 0) st->status = kStatusCapacity;
         return;
     }
-    colour_scene(W, sc, st, 0, cur);
+    colour_scene_cached(W, sc, st, 0, cur);
 }
 
 __global__ void k_predict(World W) {
@@ -75,11 +80,30 @@ __global__ void k_predict(World W) {
         predict_body(W, b);
 }
 
+// One colour of the primal sweep, groups of G lanes per body across the grid.
+template <int G>
 __global__ void k_primal(World W, int cur, int first, int count, float alpha, int write_stick) {
     const SceneDesc sc = W.scenes[0];
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < count; i += gridDim.x * blockDim.x) {
-        const int b = W.col_list[sc.body0 + first + i];
-        if (!(W.flags[b] & kBodyRemoved)) primal_body(W, cur, b, alpha, write_stick != 0);
+    const int t = blockIdx.x * blockDim.x + threadIdx.x;
+    const int lane = threadIdx.x % G, gid = t / G, ngroups = gridDim.x * blockDim.x / G;
+    for (int base = 0; base < count; base += ngroups) {
+        const int i = base + gid;
+        int b = i < count ? W.col_list[sc.body0 + first + i] : -1;
+        if (b >= 0 && (W.flags[b] & kBodyRemoved)) b = -1;
+        primal_group<G>(W, cur, b, alpha, write_stick != 0, lane);
+    }
+}
+
+void launch_primal(int group, const World& W, int cur, int first, int count, float alpha, int stick, cudaStream_t s) {
+    const int threads = kThreads;
+    const int blocks = std::max(1, std::min((count * group + threads - 1) / threads, 148 * 32));
+    switch (group) {
+        case 32: k_primal<32><<<blocks, threads, 0, s>>>(W, cur, first, count, alpha, stick); break;
+        case 16: k_primal<16><<<blocks, threads, 0, s>>>(W, cur, first, count, alpha, stick); break;
+        case 8: k_primal<8><<<blocks, threads, 0, s>>>(W, cur, first, count, alpha, stick); break;
+        case 4: k_primal<4><<<blocks, threads, 0, s>>>(W, cur, first, count, alpha, stick); break;
+        case 2: k_primal<2><<<blocks, threads, 0, s>>>(W, cur, first, count, alpha, stick); break;
+        default: k_primal<1><<<blocks, threads, 0, s>>>(W, cur, first, count, alpha, stick); break;
     }
 }
 
@@ -137,6 +161,7 @@ __global__ void k_remove_oob(World W) {
         if (p.x < kBoundMin || p.x > kBoundMax || p.y < kBoundMin || p.y > kBoundMax || p.z < kBoundMin ||
             p.z > kBoundMax) {
             W.flags[b] = fl | kBodyRemoved;
+            atomicAdd(&W.sstate[0].topo, 1);
             for (int e = W.sinc_off[b]; e < W.sinc_off[b + 1]; ++e) {
                 const uint32_t ent = W.sinc[e];
                 const uint32_t k = ent_kind(ent), idx = ent_index(ent);
@@ -169,7 +194,11 @@ __global__ void k_collide(World W, int a, int b, uint32_t* ids, float* data, int
 // Batched path: one persistent kernel per step; each CTA pulls scenes from a
 // size-ordered queue and runs a scene's whole step.
 // ===========================================================================
-__global__ void __launch_bounds__(256) k_batch_step(World W, const int* order, int nlive, int* queue) {
+// MINB sets the register budget (about 65536 / (256 * MINB) per thread):
+// 1 keeps the step in about 156 registers, 2 in 128, 3 in 80 and 4 in 64 with
+// some spilling, trading spills for resident warps.  The autotuner picks one.
+template <int MINB>
+__global__ void __launch_bounds__(256, MINB) k_batch_step(World W, const int* order, int nlive, int* queue) {
     __shared__ int s_q;
     for (;;) {
         if (threadIdx.x == 0) s_q = atomicAdd(queue, 1);
@@ -319,6 +348,12 @@ struct Pools {
     }
 };
 
+// Lanes per body in the primal sweep: FEM vertices gather about 20 tets each,
+// rigid bodies a handful of manifolds.
+int scene_group(const HostScene& h, int rigid_group, int fem_group) {
+    return (h.ntet() > 0 || h.ntri() > 0) ? fem_group : rigid_group;
+}
+
 // Capacity policy of one scene.
 void scene_caps(const HostScene& h, int& candcap, int& kcap) {
     const int n = h.nbody();
@@ -333,7 +368,7 @@ void put(T* dst, const std::vector<T>& src, size_t at = 0) {
 
 // Packs scenes into freshly allocated pools (state of each scene as staged).
 cudaError_t pack_scenes(Pools& P, const std::vector<const HostScene*>& sc, const std::vector<int>& candcaps,
-                        const std::vector<int>& kcaps, std::vector<SceneDesc>& descs) {
+                        const std::vector<int>& kcaps, const std::vector<int>& groups, std::vector<SceneDesc>& descs) {
     P.release();
     P.ns = (int)sc.size();
     P.nb = P.nf = P.nt = P.nr = P.ncand = P.nk = P.ninc = 0;
@@ -351,7 +386,7 @@ cudaError_t pack_scenes(Pools& P, const std::vector<const HostScene*>& sc, const
         d.cand0 = P.ncand; d.candcap = candcaps[i];
         d.k0 = P.nk; d.kcap = kcaps[i];
         d.ndynamic = h.ndynamic();
-        d.pad = 0;
+        d.group = groups[i];
         const size_t before = sent.size();
         h.build_static_incidence(soff, snf, sent, poff, partners, d.body0, d.force0, d.tet0, d.tri0);
         // static offsets were computed relative to this scene's start of sent
@@ -452,6 +487,7 @@ struct AvbdWorld {
     bool stopped = false;
     Pools P;
     std::vector<SceneDesc> descs;
+    int group = 0;   // lanes per body in the primal (0 = by scene kind)
     cudaStream_t stream = nullptr;
     cudaEvent_t ev[8] = {};
     AvbdTimings timings{};
@@ -479,7 +515,8 @@ int upload(AvbdWorld* w) {
     int cc, kc;
     scene_caps(w->h, cc, kc);
     std::vector<const HostScene*> sc{&w->h};
-    if (pack_scenes(w->P, sc, {cc}, {kc}, w->descs) != cudaSuccess) return AVBD_ERR_NOMEM;
+    const int g = w->group > 0 ? w->group : scene_group(w->h, 4, 8);
+    if (pack_scenes(w->P, sc, {cc}, {kc}, {g}, w->descs) != cudaSuccess) return AVBD_ERR_NOMEM;
     w->P.W.P = to_params(w->params);
     w->uploaded = true;
     return 0;
@@ -582,7 +619,7 @@ int world_step(AvbdWorld* w) {
     for (int it = 0; it < w->params.num_iterations; ++it) {
         for (int c = 0; c < ncol; ++c) {
             const int n = w->col_start[c + 1] - w->col_start[c];
-            if (n > 0) k_primal<<<blocks_for(n), kThreads, 0, s>>>(P.W, cur, w->col_start[c], n, alpha, 0);
+            if (n > 0) launch_primal(d.group, P.W, cur, w->col_start[c], n, alpha, 0, s);
         }
         if (d.nforce + ncand > 0) k_dual<<<blocks_for(d.nforce + ncand), kThreads, 0, s>>>(P.W, cur, ncand, alpha);
         if (has_fracture) {
@@ -610,7 +647,7 @@ int world_step(AvbdWorld* w) {
     if (w->params.post_stabilization) {
         for (int c = 0; c < ncol; ++c) {
             const int n = w->col_start[c + 1] - w->col_start[c];
-            if (n > 0) k_primal<<<blocks_for(n), kThreads, 0, s>>>(P.W, cur, w->col_start[c], n, 0.f, 1);
+            if (n > 0) launch_primal(d.group, P.W, cur, w->col_start[c], n, 0.f, 1, s);
         }
     }
     cudaEventRecord(w->ev[7], s);
@@ -648,6 +685,8 @@ struct AvbdBatch {
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaGraphExec_t graph = nullptr;
     int threads = 0, ctas_per_sm = 0;   // 0 = automatic
+    int group_rigid = 4, group_fem = 8;  // lanes per body in the primal sweep
+    int variant = 1;                     // register budget of the persistent kernel (1..4, see k_batch_step)
     int grid = 0;
     float last_ms = 0.f;
     std::vector<SceneState> st;
@@ -669,15 +708,16 @@ int batch_pack(AvbdBatch* b) {
     }
     batch_drop_graph(b);
     std::vector<const HostScene*> sc;
-    std::vector<int> cc, kc;
+    std::vector<int> cc, kc, gr;
     for (auto& h : b->scenes) {
         int c, k;
         scene_caps(h, c, k);
         sc.push_back(&h);
         cc.push_back(c);
         kc.push_back(k);
+        gr.push_back(scene_group(h, b->group_rigid, b->group_fem));
     }
-    if (pack_scenes(b->P, sc, cc, kc, b->descs) != cudaSuccess) return AVBD_ERR_NOMEM;
+    if (pack_scenes(b->P, sc, cc, kc, gr, b->descs) != cudaSuccess) return AVBD_ERR_NOMEM;
     b->P.W.P = to_params(b->params);
     // work queue: live scenes, largest first
     std::vector<int> order;
@@ -703,7 +743,17 @@ int batch_launch_shape(AvbdBatch* b) {
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
     int per_sm = 0;
-    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_step, threads, 0);
+    const size_t smem = kStagedBodies * sizeof(float4);
+    cudaFuncSetAttribute(k_batch_step<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_batch_step<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_batch_step<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaFuncSetAttribute(k_batch_step<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    switch (b->variant) {
+        case 4: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_step<4>, threads, smem); break;
+        case 3: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_step<3>, threads, smem); break;
+        case 2: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_step<2>, threads, smem); break;
+        default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_step<1>, threads, smem); break;
+    }
     if (per_sm < 1) per_sm = 1;
     if (b->ctas_per_sm > 0) per_sm = std::min(per_sm, b->ctas_per_sm);
     b->threads = threads;
@@ -717,7 +767,13 @@ int batch_build_graph(AvbdBatch* b) {
     cudaGraph_t g;
     if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return AVBD_ERR_CUDA;
     cudaMemsetAsync(b->d_queue, 0, sizeof(int), b->stream);
-    k_batch_step<<<b->grid, b->threads, 0, b->stream>>>(b->P.W, b->d_order, b->nlive, b->d_queue);
+    const size_t smem = kStagedBodies * sizeof(float4);
+    switch (b->variant) {
+        case 4: k_batch_step<4><<<b->grid, b->threads, smem, b->stream>>>(b->P.W, b->d_order, b->nlive, b->d_queue); break;
+        case 3: k_batch_step<3><<<b->grid, b->threads, smem, b->stream>>>(b->P.W, b->d_order, b->nlive, b->d_queue); break;
+        case 2: k_batch_step<2><<<b->grid, b->threads, smem, b->stream>>>(b->P.W, b->d_order, b->nlive, b->d_queue); break;
+        default: k_batch_step<1><<<b->grid, b->threads, smem, b->stream>>>(b->P.W, b->d_order, b->nlive, b->d_queue); break;
+    }
     if (cudaStreamEndCapture(b->stream, &g) != cudaSuccess) return AVBD_ERR_CUDA;
     cudaError_t e = cudaGraphInstantiate(&b->graph, g, 0);
     cudaGraphDestroy(g);
@@ -1232,6 +1288,14 @@ int32_t avbd_batch_set_launch(AvbdBatch* b, int32_t threads, int32_t ctas_per_sm
     return 0;
 }
 
+int32_t avbd_batch_set_kernel(AvbdBatch* b, int32_t register_variant) {
+    if (!b || register_variant < 1 || register_variant > 4) return AVBD_ERR_INVALID;
+    b->variant = register_variant;
+    b->grid = 0;
+    batch_drop_graph(b);
+    return 0;
+}
+
 int32_t avbd_batch_get_launch(const AvbdBatch* b, int32_t* threads, int32_t* ctas_per_sm) {
     if (!b) return AVBD_ERR_INVALID;
     if (threads) *threads = b->threads;
@@ -1240,6 +1304,23 @@ int32_t avbd_batch_get_launch(const AvbdBatch* b, int32_t* threads, int32_t* cta
 }
 
 float avbd_batch_last_ms(const AvbdBatch* b) { return b ? b->last_ms : -1.f; }
+
+static bool valid_group(int g) { return g == 1 || g == 2 || g == 4 || g == 8 || g == 16 || g == 32; }
+
+int32_t avbd_batch_set_groups(AvbdBatch* b, int32_t rigid_group, int32_t fem_group) {
+    if (!b || !valid_group(rigid_group) || !valid_group(fem_group)) return AVBD_ERR_INVALID;
+    if (b->packed) return AVBD_ERR_STATE;
+    b->group_rigid = rigid_group;
+    b->group_fem = fem_group;
+    return 0;
+}
+
+int32_t avbd_set_group(AvbdWorld* w, int32_t group) {
+    if (!w || (group != 0 && !valid_group(group))) return AVBD_ERR_INVALID;
+    if (w->uploaded) return AVBD_ERR_STATE;
+    w->group = group;
+    return 0;
+}
 
 }  // extern "C"
 
@@ -1339,3 +1420,18 @@ extern "C" int32_t avbd_collide_noalloc(AvbdWorld* w, int32_t n, const int32_t* 
         if (counts[i] < 0) return AVBD_ERR_INVALID;
     return 0;
 }
+
+#ifdef AVBD_PHASE_TIMING
+// Development builds only: read and reset the per-phase cycle counters.
+extern "C" int32_t avbd_debug_phase_cycles(unsigned long long* phases, unsigned long long* scenes, int32_t nscenes,
+                                           int32_t reset) {
+    if (phases) cudaMemcpyFromSymbol(phases, g_phase_cycles, sizeof(unsigned long long) * 32);
+    if (scenes && nscenes > 0)
+        cudaMemcpyFromSymbol(scenes, g_scene_cycles, sizeof(unsigned long long) * std::min(nscenes, 1 << 16));
+    if (reset) {
+        static unsigned long long zeros[32] = {};
+        cudaMemcpyToSymbol(g_phase_cycles, zeros, sizeof(zeros));
+    }
+    return 0;
+}
+#endif

@@ -103,7 +103,7 @@ struct SceneDesc {
     int k0, kcap;            // contact slots (bump-allocated per step)
     int inc0, inccap;        // incidence (CSR) entries
     int ndynamic;
-    int pad;
+    int group;               // lanes per body in the primal sweep (1, 2, 4, 8, 16, 32)
 };
 
 // Per-scene mutable counters (device).
@@ -119,7 +119,12 @@ struct SceneState {
     int need_k;
     int need_inc;
     int step;                // steps taken (stamps manifold creation)
-    int pad[3];
+    int nlive[2];            // live manifolds of each table
+    int nmatched;            // live manifolds this step whose pair was live last step
+    int topo;                // bumped when a force or body is removed
+    int coloured_topo;       // topo value the current colouring was made for
+    int colours_valid;       // the colour lists describe the current contact graph
+    int pad[2];
 };
 
 // Structure-of-arrays device world.  One instance is passed by value to kernels.

@@ -227,24 +227,49 @@ AVBD_HD void neohookean_terms(V3 p0, V3 p1, V3 p2, V3 p3, const float* DmInv, V3
     // ComputeEnergyHessian (math.cpp:86-134)
     const float s0 = S.x, s1 = S.y, s2 = S.z;
     float ev[9];
+    ev[0] = ev[1] = ev[2] = 0.f;
     const float dPhi = (lambda * logJ - mu) / J;
     ev[3] = mu + dPhi * s2; ev[4] = mu + dPhi * s1; ev[5] = mu + dPhi * s0;
     ev[6] = mu - dPhi * s2; ev[7] = mu - dPhi * s1; ev[8] = mu - dPhi * s0;
     const float diagExtra = mu + lambda * (1.0f - logJ);
-    V3 w;
-    M3 Q;
-    eig3(mu + diagExtra / (s0 * s0), mu + diagExtra / (s1 * s1), mu + diagExtra / (s2 * s2), lambda * s2 / J,
-         lambda * s1 / J, lambda * s0 / J, w, Q);
-    ev[0] = w.x; ev[1] = w.y; ev[2] = w.z;
-    project_eigenvalues(ev, 9, mode, rho);
-    // ReconstructVertexHessian (math.cpp:174-230)
+    // scaling block A (math.cpp:112-119)
+    const float a00 = mu + diagExtra / (s0 * s0), a11 = mu + diagExtra / (s1 * s1), a22 = mu + diagExtra / (s2 * s2);
+    const float a01 = lambda * s2 / J, a02 = lambda * s1 / J, a12 = lambda * s0 / J;
     const float vg0 = dot(V.c[0], gradN), vg1 = dot(V.c[1], gradN), vg2 = dot(V.c[2], gradN);
     s3_zero(H);
+    // Scaling modes: sum_k proj(lam_k) w_k w_k^T = M proj(A) M^T with M = [vg0 u0, vg1 u1, vg2 u2]
+    // (math.cpp:196-202).  When A is positive definite (all Cholesky pivots > 0) both ABSOLUTE and
+    // CLAMP projections leave it unchanged up to the 1e-6 floor, so proj(A) = A needs no eigensolve.
+    const float piv0 = a00;
+    const float l10 = a01 / piv0, l20 = a02 / piv0;
+    const float piv1 = a11 - l10 * a01;
+    const float l21 = (a12 - l20 * a01) / piv1;
+    const float piv2 = a22 - l20 * a02 - l21 * l21 * piv1;
+    if (piv0 > 0.f && piv1 > 0.f && piv2 > 0.f) {
+        const V3 m0 = vg0 * U.c[0], m1 = vg1 * U.c[1], m2 = vg2 * U.c[2];
+        // B = M A (columns), H += B M^T
+        const V3 b0 = a00 * m0 + a01 * m1 + a02 * m2;
+        const V3 b1 = a01 * m0 + a11 * m1 + a12 * m2;
+        const V3 b2 = a02 * m0 + a12 * m1 + a22 * m2;
+        H.xx += b0.x * m0.x + b1.x * m1.x + b2.x * m2.x;
+        H.yy += b0.y * m0.y + b1.y * m1.y + b2.y * m2.y;
+        H.zz += b0.z * m0.z + b1.z * m1.z + b2.z * m2.z;
+        H.xy += b0.y * m0.x + b1.y * m1.x + b2.y * m2.x;
+        H.xz += b0.z * m0.x + b1.z * m1.x + b2.z * m2.x;
+        H.yz += b0.z * m0.y + b1.z * m1.y + b2.z * m2.y;
+        project_eigenvalues(ev + 3, 6, mode, rho);
+    } else {
+        V3 w;
+        M3 Q;
+        eig3(a00, a11, a22, a01, a02, a12, w, Q);
+        ev[0] = w.x; ev[1] = w.y; ev[2] = w.z;
+        project_eigenvalues(ev, 9, mode, rho);
 #pragma unroll
-    for (int k = 0; k < 3; ++k) {
-        V3 c = Q.c[k];
-        V3 ww = (c.x * vg0) * U.c[0] + (c.y * vg1) * U.c[1] + (c.z * vg2) * U.c[2];
-        s3_add_outer(H, ev[k], ww);
+        for (int k = 0; k < 3; ++k) {
+            V3 c = Q.c[k];
+            V3 ww = (c.x * vg0) * U.c[0] + (c.y * vg1) * U.c[1] + (c.z * vg2) * U.c[2];
+            s3_add_outer(H, ev[k], ww);
+        }
     }
     const float is2 = 0.70710678118f;
     s3_add_outer(H, ev[3], is2 * (vg1 * U.c[0] - vg0 * U.c[1]));

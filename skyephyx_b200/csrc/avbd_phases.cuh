@@ -134,6 +134,24 @@ AVBD_HD int broadphase_body(const World& W, const SceneDesc& sc, int i, int2* ou
     return n;
 }
 
+// Same as broadphase_body with the scene's (position, radius) staged in
+// shared memory (radius = -inf marks a removed body).
+AVBD_HD int broadphase_body_staged(const World& W, const SceneDesc& sc, int i, const float4* sp, int2* out, int cap) {
+    const int li = i - sc.body0;
+    const float4 pi = sp[li];
+    if (isinf(pi.w)) return 0;
+    int n = 0;
+    for (int lj = li + 1; lj < sc.nbody; ++lj) {
+        const float4 pj = sp[lj];
+        if (!sphere_overlap(pi, pj, pi.w, pj.w)) continue;
+        const int j = sc.body0 + lj;
+        if (pair_constrained(W, 0, i, j)) continue;
+        if (out && n < cap) out[n] = make_int2(i, j);
+        ++n;
+    }
+    return n;
+}
+
 // ===========================================================================
 // Phase 2 (forces): Manifold::Initialize (manifold.cpp:32-194) on one
 // candidate slot, followed by the warm-start penalty decay (solver.cpp:274-291).
@@ -170,6 +188,7 @@ AVBD_HD void narrowphase_slot(const World& W, const SceneDesc& sc, SceneState* s
     const int base = sc.k0 + kofs;
     W.kbase[cur][slot] = base;
     W.cn[cur][slot] = col.n;
+    AVBD_ATOMIC_ADD(&st->nlive[cur], 1);
     const float fr = XSQRT(XMUL(W.friction[A], W.friction[B]));
     W.cfric[cur][slot] = fr;
     // previous contacts of the same pair
@@ -186,6 +205,7 @@ AVBD_HD void narrowphase_slot(const World& W, const SceneDesc& sc, SceneState* s
         }
     }
     W.cbirth[cur][slot] = birth;
+    if (on > 0) AVBD_ATOMIC_ADD(&st->nmatched, 1);
     const Params& P = W.P;
     const Q4 qA = q4(W.rot[A]), qB = q4(W.rot[B]);
     const M3 RA = xrotmat(qA), RB = xrotmat(qB);
@@ -269,12 +289,13 @@ AVBD_HD void joint_positions(const World& W, int f, V3& worldA, V3& worldB, Q4& 
     qB = q4(W.rot[ab.y]);
 }
 
-AVBD_HD void force_init(const World& W, int f) {
+// Returns true when the force is dropped this step (the contact graph changes).
+AVBD_HD bool force_init(const World& W, int f) {
     int t = W.ftype[f];
-    if (t & kForceRemoved) return;
+    if (t & kForceRemoved) return false;
     if (t & kForceDisabled) {   // Initialize() returns false -> RemoveForce
         W.ftype[f] = t | kForceRemoved;
-        return;
+        return true;
     }
     const int nrows = (t & 15) == kForceJoint ? 6 : 1;
     if ((t & 15) == kForceJoint) {
@@ -292,6 +313,7 @@ AVBD_HD void force_init(const World& W, int f) {
         if (np > kPenaltyMax) np = kPenaltyMax;
         W.fpen[i] = fminf(np, W.fk[i]);
     }
+    return false;
 }
 
 // Joint::ComputeConstraints (joint.cpp:97-124)
@@ -593,32 +615,38 @@ AVBD_HD void primal_spring(const World& W, int f, int b, Sys6& s) {
     for (int j = 0; j < 6; ++j) s.a[j][j] += G[j];
 }
 
-AVBD_HD void primal_body(const World& W, int cur, int b, float alpha, bool write_stick) {
+// Inertial term M/dt^2 and its right-hand side (solver.cpp:396-397).
+AVBD_HD void primal_init_mass(const World& W, int b, Sys6& s) {
     const float dt = W.P.dt;
     const float dt2 = dt * dt;
-    Sys6 s;
+    const float4 M0 = W.Mw0[b], M1 = W.Mw1[b];
+    const float m = M0.x / dt2;
+    s.a[0][0] = m; s.a[1][1] = m; s.a[2][2] = m;
+    s.a[3][3] = M0.y / dt2; s.a[4][4] = M0.z / dt2; s.a[5][5] = M0.w / dt2;
+    s.a[4][3] = M1.x / dt2; s.a[5][3] = M1.y / dt2; s.a[5][4] = M1.z / dt2;
+    const V3 dl = v3(W.pos[b]) - v3(W.ipos[b]);
+    const V3 da = rotation_difference(q4(W.rot[b]), q4(W.irot[b]));
+    s.r[0] = m * dl.x; s.r[1] = m * dl.y; s.r[2] = m * dl.z;
+    s.r[3] = s.a[3][3] * da.x + s.a[4][3] * da.y + s.a[5][3] * da.z;
+    s.r[4] = s.a[4][3] * da.x + s.a[4][4] * da.y + s.a[5][4] * da.z;
+    s.r[5] = s.a[5][3] * da.x + s.a[5][4] * da.y + s.a[5][5] * da.z;
+}
+
+AVBD_HD void sys_zero(Sys6& s) {
 #pragma unroll
     for (int i = 0; i < 6; ++i) {
         s.r[i] = 0.f;
 #pragma unroll
         for (int j = 0; j < 6; ++j) s.a[i][j] = 0.f;
     }
-    const float4 M0 = W.Mw0[b], M1 = W.Mw1[b];
-    const float m = M0.x / dt2;
-    s.a[0][0] = m; s.a[1][1] = m; s.a[2][2] = m;
-    s.a[3][3] = M0.y / dt2; s.a[4][4] = M0.z / dt2; s.a[5][5] = M0.w / dt2;
-    s.a[4][3] = M1.x / dt2; s.a[5][3] = M1.y / dt2; s.a[5][4] = M1.z / dt2;
-    const V3 pos = v3(W.pos[b]);
-    const Q4 rot = q4(W.rot[b]);
-    const V3 dl = pos - v3(W.ipos[b]);
-    const V3 da = rotation_difference(rot, q4(W.irot[b]));
-    s.r[0] = m * dl.x; s.r[1] = m * dl.y; s.r[2] = m * dl.z;
-    s.r[3] = s.a[3][3] * da.x + s.a[4][3] * da.y + s.a[5][3] * da.z;
-    s.r[4] = s.a[4][3] * da.x + s.a[4][4] * da.y + s.a[5][4] * da.z;
-    s.r[5] = s.a[5][3] * da.x + s.a[5][4] * da.y + s.a[5][5] * da.z;
+}
 
+// Adds the rows of incidence entries first, first + stride, ... of body b
+// (solver.cpp:399-435): forces (manifolds, joints, springs) then energies.
+AVBD_HD void primal_entries(const World& W, int cur, int b, float alpha, bool write_stick, int first, int stride,
+                            Sys6& s) {
     const int e0 = W.inc_off[b], e1 = e0 + W.inc_cnt[b];
-    for (int e = e0; e < e1; ++e) {
+    for (int e = e0 + first; e < e1; e += stride) {
         const uint32_t ent = W.inc[e];
         const uint32_t kind = ent_kind(ent), idx = ent_index(ent);
         if (kind == kEntManifold) {
@@ -657,8 +685,14 @@ AVBD_HD void primal_body(const World& W, int cur, int b, float alpha, bool write
             s.a[1][0] += H.xy; s.a[2][0] += H.xz; s.a[2][1] += H.yz;
         }
     }
+}
+
+// LDLT solve and pose update (solver.cpp:437-448).
+AVBD_HD void primal_finish(const World& W, int b, Sys6& s) {
     float x[6];
     ldlt_solve6(s, x);
+    const V3 pos = v3(W.pos[b]);
+    const Q4 rot = q4(W.rot[b]);
     const V3 npos = pos - v3(x[0], x[1], x[2]);
     const Q4 dq = quaternion_from_difference(v3(x[3], x[4], x[5]), -1.f);
     const Q4 nrot = qnormalize(qmul(dq, rot));
@@ -666,6 +700,15 @@ AVBD_HD void primal_body(const World& W, int cur, int b, float alpha, bool write
     W.rot[b] = f4(nrot);
     W.dlin[b] = f4(npos - v3(W.lpos[b]));
     W.dang[b] = f4(rotation_difference(nrot, q4(W.lrot[b])));
+}
+
+// One body by one thread, in the reference's summation order.
+AVBD_HD void primal_body(const World& W, int cur, int b, float alpha, bool write_stick) {
+    Sys6 s;
+    sys_zero(s);
+    primal_init_mass(W, b, s);
+    primal_entries(W, cur, b, alpha, write_stick, 0, 1, s);
+    primal_finish(W, b, s);
 }
 
 // ===========================================================================

@@ -6,9 +6,30 @@
 #pragma once
 #include "avbd_phases.cuh"
 
+// Optional per-phase cycle counters (development builds with -DAVBD_PHASE_TIMING
+// only; the hooks compile to nothing otherwise).
+#ifdef AVBD_PHASE_TIMING
+__device__ unsigned long long g_phase_cycles[2 * 16];
+__device__ unsigned long long g_scene_cycles[1 << 16];
+#define AVBD_PHASE_BEGIN(kind) long long _avbd_t0 = clock64(), _avbd_s0 = _avbd_t0; const int _avbd_kind = (kind);
+#define AVBD_PHASE(k)                                                                               \
+    if (threadIdx.x == 0) {                                                                         \
+        long long _t = clock64();                                                                   \
+        atomicAdd(&g_phase_cycles[_avbd_kind * 16 + (k)], (unsigned long long)(_t - _avbd_t0));     \
+        _avbd_t0 = _t;                                                                              \
+    }
+#define AVBD_PHASE_END(scene) \
+    if (threadIdx.x == 0 && (scene) < (1 << 16)) g_scene_cycles[(scene)] = (unsigned long long)(clock64() - _avbd_s0);
+#else
+#define AVBD_PHASE_BEGIN(kind)
+#define AVBD_PHASE(k)
+#define AVBD_PHASE_END(scene)
+#endif
+
 namespace avbd {
 
 constexpr unsigned kFull = 0xffffffffu;
+constexpr int kStagedBodies = 2560;   // bodies whose pose fits the broadphase's shared-memory stage (40 KB)
 
 // Exclusive scan of in[0, n) into out[0, n) by one CTA; returns the total.
 // in and out may alias.
@@ -80,7 +101,7 @@ __device__ __forceinline__ void sort_manifold_entries(const World& W, int cur, u
 }
 
 // Returns false (and sets need_inc) when the scene's incidence region is too small.
-__device__ bool build_incidence(const World& W, const SceneDesc& sc, SceneState* st, int cur) {
+__device__ __noinline__ bool build_incidence(const World& W, const SceneDesc& sc, SceneState* st, int cur) {
     const int tid = threadIdx.x, nt = blockDim.x;
     const int b0 = sc.body0, b1 = sc.body0 + sc.nbody;
     const int ncand = st->ncand[cur];
@@ -175,8 +196,83 @@ __device__ __forceinline__ void for_each_neighbour(const World& W, int cur, int 
     }
 }
 
+// ---------------------------------------------------------------------------
+// Primal update of one body by a group of G lanes (G divides 32, groups are
+// warp-aligned): lane l gathers incidence entries l, l+G, ...; the 27
+// accumulators (lower triangle + right-hand side) are summed across the group
+// by a butterfly; lane 0 adds nothing more and solves.  Every lane of a warp
+// must call this the same number of times (b < 0 for an idle group).
+// ---------------------------------------------------------------------------
+template <int G>
+__device__ __forceinline__ void primal_group(const World& W, int cur, int b, float alpha, bool write_stick, int lane) {
+    Sys6 s;
+    sys_zero(s);
+    if (b >= 0) {
+        if (lane == 0) primal_init_mass(W, b, s);
+        primal_entries(W, cur, b, alpha, write_stick, lane, G, s);
+    }
+    if (G > 1) {
+#pragma unroll
+        for (int off = G / 2; off >= 1; off >>= 1) {
+#pragma unroll
+            for (int i = 0; i < 6; ++i) {
+                s.r[i] += __shfl_xor_sync(kFull, s.r[i], off);
+#pragma unroll
+                for (int j = 0; j <= i; ++j) s.a[i][j] += __shfl_xor_sync(kFull, s.a[i][j], off);
+            }
+        }
+    }
+    if (b >= 0 && lane == 0) primal_finish(W, b, s);
+}
+
+// Sweeps the bodies list[0, n) with groups of G lanes of the calling CTA.
+template <int G>
+__device__ void primal_sweep_cta(const World& W, int cur, const int* list, int n, float alpha, bool write_stick) {
+    const int lane = threadIdx.x % G, gid = threadIdx.x / G, ngroups = blockDim.x / G;
+    for (int base = 0; base < n; base += ngroups) {
+        const int i = base + gid;
+        int b = i < n ? list[i] : -1;
+        if (b >= 0 && (W.flags[b] & kBodyRemoved)) b = -1;
+        primal_group<G>(W, cur, b, alpha, write_stick, lane);
+    }
+}
+
+__device__ __noinline__ void primal_sweep_cta_dispatch(const World& W, int cur, const int* list, int n, float alpha,
+                                                          bool write_stick, int group) {
+    switch (group) {
+        case 32: primal_sweep_cta<32>(W, cur, list, n, alpha, write_stick); break;
+        case 16: primal_sweep_cta<16>(W, cur, list, n, alpha, write_stick); break;
+        case 8: primal_sweep_cta<8>(W, cur, list, n, alpha, write_stick); break;
+        case 4: primal_sweep_cta<4>(W, cur, list, n, alpha, write_stick); break;
+        case 2: primal_sweep_cta<2>(W, cur, list, n, alpha, write_stick); break;
+        default: primal_sweep_cta<1>(W, cur, list, n, alpha, write_stick); break;
+    }
+}
+
+__device__ __noinline__ bool colour_scene(const World& W, const SceneDesc& sc, SceneState* st, int scene, int cur);
+
+// Keeps the previous step's colouring when the contact graph is unchanged:
+// the same number of live manifolds in both tables, every live one already
+// live last step, and no force or body removed since the colouring was made.
+// The colouring is a deterministic function of that graph, so reusing it is
+// exact.
+__device__ bool colour_scene_cached(const World& W, const SceneDesc& sc, SceneState* st, int scene, int cur) {
+    const int old = cur ^ 1;
+    const bool reuse = st->colours_valid && st->nlive[cur] == st->nlive[old] && st->nmatched == st->nlive[cur] &&
+                       st->topo == st->coloured_topo;
+    __syncthreads();
+    if (reuse) return true;
+    const bool ok = colour_scene(W, sc, st, scene, cur);
+    if (threadIdx.x == 0) {
+        st->colours_valid = ok ? 1 : 0;
+        st->coloured_topo = st->topo;
+    }
+    __syncthreads();
+    return ok;
+}
+
 // Returns false (status TIMEOUT or CAPACITY set) if colouring could not finish.
-__device__ bool colour_scene(const World& W, const SceneDesc& sc, SceneState* st, int scene, int cur) {
+__device__ __noinline__ bool colour_scene(const World& W, const SceneDesc& sc, SceneState* st, int scene, int cur) {
     __shared__ int s_remaining, s_progress, s_maxc;
     __shared__ int s_count[kMaxColours + 1];
     const int tid = threadIdx.x, nt = blockDim.x;
@@ -257,6 +353,23 @@ __device__ bool colour_scene(const World& W, const SceneDesc& sc, SceneState* st
     return st->status == kStatusOk;
 }
 
+// Phase loops of one scene kept out of line, so each gets its own register
+// allocation instead of the union of every inlined phase.
+__device__ __noinline__ void narrowphase_cta(const World& W, const SceneDesc& sc, SceneState* st, int cur, int ncand,
+                                             int old_count) {
+    for (int c = sc.cand0 + threadIdx.x; c < sc.cand0 + ncand; c += blockDim.x)
+        narrowphase_slot(W, sc, st, c, cur, old_count);
+}
+
+// Returns true if this thread saw a force fracture.
+__device__ __noinline__ bool dual_cta(const World& W, const SceneDesc& sc, int cur, int ncand) {
+    bool broke = false;
+    for (int f = sc.force0 + threadIdx.x; f < sc.force0 + sc.nforce; f += blockDim.x)
+        if (dual_force(W, f, W.P.alpha)) broke = true;
+    for (int c = sc.cand0 + threadIdx.x; c < sc.cand0 + ncand; c += blockDim.x) dual_manifold(W, cur, c, W.P.alpha);
+    return broke;
+}
+
 // ---------------------------------------------------------------------------
 // Whole step of one scene on one CTA (batched path).
 // ---------------------------------------------------------------------------
@@ -268,56 +381,77 @@ __device__ void scene_step(const World& W, int scene) {
     if (st->status != kStatusOk && st->status != kStatusCapacity && st->status != kStatusTimeout) return;
     __syncthreads();
     if (tid == 0) { st->status = kStatusOk; st->need_cand = 0; st->need_k = 0; st->need_inc = 0; }
+    AVBD_PHASE_BEGIN(sc.ntet > 0 ? 1 : 0);
     const int old = st->cur, cur = old ^ 1;
     const int b0 = sc.body0, b1 = sc.body0 + sc.nbody;
-    // 1. broadphase: count, scan, capacity check, write
-    for (int b = b0 + tid; b < b1; b += nt) W.cand_cnt[b] = broadphase_body(W, sc, b, nullptr, 0);
+    // 1. broadphase: count, scan, capacity check, write; positions and radii
+    //    staged in shared memory when the scene fits
+    extern __shared__ float4 s_bodies[];
+    const bool staged = sc.nbody <= kStagedBodies;
+    if (staged) {
+        for (int b = b0 + tid; b < b1; b += nt) {
+            float4 p = W.pos[b];
+            p.w = (W.flags[b] & kBodyRemoved) ? -INFINITY : W.scale[b].w;
+            s_bodies[b - b0] = p;
+        }
+        __syncthreads();
+    }
+    for (int b = b0 + tid; b < b1; b += nt)
+        W.cand_cnt[b] = staged ? broadphase_body_staged(W, sc, b, s_bodies, nullptr, 0)
+                               : broadphase_body(W, sc, b, nullptr, 0);
     __syncthreads();
     const int ncand = block_exclusive_scan(W.cand_cnt + b0, W.cand_off + b0, sc.nbody);
     if (ncand > sc.candcap) {
         if (tid == 0) { st->status = kStatusCapacity; st->need_cand = ncand; }
         return;
     }
-    for (int b = b0 + tid; b < b1; b += nt)
-        broadphase_body(W, sc, b, W.cpair[cur] + sc.cand0 + W.cand_off[b], W.cand_cnt[b]);
-    if (tid == 0) st->kused[cur] = 0;
+    for (int b = b0 + tid; b < b1; b += nt) {
+        int2* out = W.cpair[cur] + sc.cand0 + W.cand_off[b];
+        if (staged) broadphase_body_staged(W, sc, b, s_bodies, out, W.cand_cnt[b]);
+        else broadphase_body(W, sc, b, out, W.cand_cnt[b]);
+    }
+    if (tid == 0) { st->kused[cur] = 0; st->nlive[cur] = 0; st->nmatched = 0; }
     __syncthreads();
+    AVBD_PHASE(0);
     // 2. narrowphase + manifold warm start into the other table
     const int old_count = st->ncand[old];
-    for (int c = sc.cand0 + tid; c < sc.cand0 + ncand; c += nt) narrowphase_slot(W, sc, st, c, cur, old_count);
+    narrowphase_cta(W, sc, st, cur, ncand, old_count);
     __syncthreads();
     if (st->need_k) {
         if (tid == 0) { st->status = kStatusCapacity; st->need_k = st->kused[cur]; }
         return;
     }
     if (tid == 0) { st->ncand[cur] = ncand; st->cur = cur; }
+    AVBD_PHASE(1);
     // 2b. joints / springs warm start
-    for (int f = sc.force0 + tid; f < sc.force0 + sc.nforce; f += nt) force_init(W, f);
+    for (int f = sc.force0 + tid; f < sc.force0 + sc.nforce; f += nt)
+        if (force_init(W, f)) atomicAdd(&st->topo, 1);
     __syncthreads();
     // incidence
     if (!build_incidence(W, sc, st, cur)) {
         if (tid == 0) st->status = kStatusCapacity;
         return;
     }
+    AVBD_PHASE(2);
     // colouring
-    if (!colour_scene(W, sc, st, scene, cur)) return;
+    if (!colour_scene_cached(W, sc, st, scene, cur)) return;
+    AVBD_PHASE(3);
     // 4. prediction
     for (int b = b0 + tid; b < b1; b += nt) predict_body(W, b);
     __syncthreads();
+    AVBD_PHASE(4);
     const int ncol = st->ncolours;
     const int* cs = W.col_start + (size_t)scene * (kMaxColours + 1);
     // 5. iterations
     for (int it = 0; it < W.P.num_iterations; ++it) {
         for (int c = 0; c < ncol; ++c) {
-            const int e = cs[c + 1];
-            for (int i = cs[c] + tid; i < e; i += nt) primal_body(W, cur, W.col_list[b0 + i], W.P.alpha, false);
+            primal_sweep_cta_dispatch(W, cur, W.col_list + b0 + cs[c], cs[c + 1] - cs[c], W.P.alpha, false, sc.group);
             __syncthreads();
         }
+        AVBD_PHASE(5);
         if (tid == 0) s_flags = 0;
         __syncthreads();
-        for (int f = sc.force0 + tid; f < sc.force0 + sc.nforce; f += nt)
-            if (dual_force(W, f, W.P.alpha)) s_flags = 1;
-        for (int c = sc.cand0 + tid; c < sc.cand0 + ncand; c += nt) dual_manifold(W, cur, c, W.P.alpha);
+        if (dual_cta(W, sc, cur, ncand)) s_flags = 1;
         __syncthreads();
         const int fractured = s_flags;
         __syncthreads();
@@ -327,6 +461,7 @@ __device__ void scene_step(const World& W, int scene) {
             for (int b = b0 + tid; b < b1; b += nt) W.reset_flag[b] = 0;
             __syncthreads();
         }
+        AVBD_PHASE(6);
     }
     // 6. velocities, explosion, out of bounds
     if (tid == 0) s_flags = 0;
@@ -349,6 +484,7 @@ __device__ void scene_step(const World& W, int scene) {
             if (p.x < kBoundMin || p.x > kBoundMax || p.y < kBoundMin || p.y > kBoundMax || p.z < kBoundMin ||
                 p.z > kBoundMax) {
                 W.flags[b] = fl | kBodyRemoved;
+                atomicAdd(&st->topo, 1);
                 for (int e = W.sinc_off[b]; e < W.sinc_off[b + 1]; ++e) {
                     const uint32_t ent = W.sinc[e];
                     const uint32_t k = ent_kind(ent), idx = ent_index(ent);
@@ -361,17 +497,16 @@ __device__ void scene_step(const World& W, int scene) {
         __syncthreads();
     }
     if (tid == 0) st->step += 1;
+    AVBD_PHASE(7);
     // 7. post-stabilisation
     if (W.P.post_stabilization) {
         for (int c = 0; c < ncol; ++c) {
-            const int e = cs[c + 1];
-            for (int i = cs[c] + tid; i < e; i += nt) {
-                const int b = W.col_list[b0 + i];
-                if (!(W.flags[b] & kBodyRemoved)) primal_body(W, cur, b, 0.f, true);
-            }
+            primal_sweep_cta_dispatch(W, cur, W.col_list + b0 + cs[c], cs[c + 1] - cs[c], 0.f, true, sc.group);
             __syncthreads();
         }
     }
+    AVBD_PHASE(8);
+    AVBD_PHASE_END(scene);
 }
 
 }  // namespace avbd

@@ -236,6 +236,10 @@ class Solver:
                                              counts.ctypes.data_as(ip)), "collide_noalloc")
         return ids, data, counts
 
+    def set_group(self, group=0):
+        """Lanes per body in the primal sweep (0 = by scene kind); before the first step."""
+        check(self._lib.avbd_set_group(self._h, int(group)), "set_group")
+
     def footprint_bytes(self):
         return self._lib.avbd_scene_footprint_bytes(self._h)
 
@@ -302,8 +306,16 @@ class Batch:
               "batch_get_state")
         return pos, quat, vel, omega
 
+    def set_groups(self, rigid_group=4, fem_group=8):
+        """Lanes per body in the primal sweep for rigid and FEM scenes (before the first step)."""
+        check(self._lib.avbd_batch_set_groups(self._h, int(rigid_group), int(fem_group)), "set_groups")
+
     def set_launch(self, threads_per_cta=0, ctas_per_sm=0):
         check(self._lib.avbd_batch_set_launch(self._h, int(threads_per_cta), int(ctas_per_sm)), "set_launch")
+
+    def set_kernel(self, register_variant=1):
+        """Register budget of the persistent kernel build (1..4)."""
+        check(self._lib.avbd_batch_set_kernel(self._h, int(register_variant)), "set_kernel")
 
     def launch(self):
         t = C.c_int32()
