@@ -198,6 +198,37 @@ def cpu_baseline(specs, steps, threads):
     return dyn * ITERS * steps / (ms / 1e3), dyn, ms
 
 
+def serve_bench(rate, window, cap_s, budget_gb, launch=None, seed_base=0x5EED0005):
+    """Continuous batching at `rate` Poisson arrivals/s for `window` s: each
+    request is a seeded scene of the batched mix simulated for U{60..600}
+    steps; admission by free pool space in an HBM budget.  Returns throughput
+    and arrival-to-completion latency of the requests completed within
+    `window + cap_s` seconds, plus the backlog left."""
+    from skyephyx_b200 import Solver, scenes
+    from skyephyx_b200.serve import Request, Server, poisson_arrivals
+    arrivals = poisson_arrivals(rate, window, seed=seed_base)
+    rng = np.random.default_rng(seed_base + 1)
+    specs = scenes.batch_mix_specs(n_scenes=len(arrivals), config=5)
+    srv = Server(budget_bytes=int(budget_gb * (1 << 30)), max_scenes=16384, launch=launch, keep_results=False)
+    t_build = time.perf_counter()
+    for i, (t, sp) in enumerate(zip(arrivals, specs)):
+        s = Solver(iterations=ITERS)
+        scenes.build_spec(s, sp, config=5)
+        srv.submit(Request(rid=i, scene=s, steps=int(rng.integers(60, 601)), arrival=t))
+    build_s = time.perf_counter() - t_build
+    srv.start()
+    srv.run(until=window + cap_s)
+    elapsed = srv.clock()
+    st = srv.latency_stats()
+    backlog = len(srv.pending) + len(srv.active)
+    return {"offered_rate": rate, "window_s": window, "requests": len(arrivals),
+            "completed": st.get("completed", 0), "backlog": backlog,
+            "scenes_per_s": st.get("completed", 0) / elapsed, "body_iters_per_s": srv.body_iters / elapsed,
+            "p50_s": st.get("p50_s"), "p99_s": st.get("p99_s"), "ticks": srv.ticks, "elapsed_s": elapsed,
+            "keeps_up": backlog == 0 and elapsed <= window + 5.0, "budget_gb": budget_gb,
+            "build_s": build_s}
+
+
 def dist_env():
     ws = int(os.environ.get("WORLD_SIZE", "1"))
     rank = int(os.environ.get("RANK", "0"))
@@ -249,12 +280,22 @@ def main():
     ap.add_argument("--plain-scenes", type=int, default=24)
     ap.add_argument("--cpu-scenes", type=int, default=128)
     ap.add_argument("--no-cpu", action="store_true")
+    ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--serve-only", action="store_true")
+    ap.add_argument("--serve-rate", type=float, default=2000.0)
+    ap.add_argument("--serve-window", type=float, default=3.0)
     args = ap.parse_args()
     if args.warmup < 3:
         args.warmup = 3
 
     if args.impl == "reference":
         reference_arm(args)
+        return
+
+    if args.serve_only:
+        from skyephyx_b200 import autotune
+        launch = autotune.lookup(autotune.signature(args.scenes, args.scenes // 4, args.scenes * 420))
+        print(json.dumps({"served": serve_bench(args.serve_rate, args.serve_window, 30.0, 60.0, launch)}))
         return
 
     ws, rank, local = dist_env()
@@ -348,6 +389,15 @@ def main():
                "sample": f"first {len(cpu_specs)} scenes of the mix ({cdyn} dynamic bodies), 3 steps, "
                          f"reference Solver::Step per scene on {threads_cpu} threads"}
 
+    served = None
+    if not args.no_serve:
+        batch.close()
+        del staged
+        served = serve_bench(args.serve_rate, args.serve_window, 20.0, 60.0, launch=counts["launch"])
+        if not served["keeps_up"]:
+            # the rate the served loop sustains: completions/s while saturated
+            served["max_sustainable_rate"] = served["scenes_per_s"]
+
     line = {
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
@@ -371,6 +421,7 @@ def main():
                      "traffic": None, "peak_kind": peak_kind,
                      "algorithmic_bytes_per_launch": alg_bytes},
         "clocks": clk,
+        "served": served,
         "cpu_baseline": cpu,
         "status_counts": bad,
         "build_s": build_s,

@@ -179,15 +179,26 @@ int32_t avbd_collide_noalloc(AvbdWorld* w, int32_t n, const int32_t* body_a, con
  * ------------------------------------------------------------------------- */
 int32_t avbd_batch_create(const AvbdParams* params, int32_t device, AvbdBatch** out);
 int32_t avbd_batch_destroy(AvbdBatch* b);
+/* Reserves the batch's device pools: capacity for `bodies` bodies, `forces`
+ * joints+springs, `tets`, `tris` and `scenes` scene slots (contact and
+ * incidence tables are sized from the body count). Without a reservation the
+ * first step sizes the pools to the scenes added so far. */
+int32_t avbd_batch_reserve(AvbdBatch* b, int64_t bodies, int64_t forces, int64_t tets, int64_t tris,
+                           int32_t scenes);
 /* Copies the scene staged in `w` (built with the calls above, never stepped)
- * into the batch. Returns the scene id. Scenes added after the first step are
- * admitted at the next step. */
+ * into the batch and returns its scene id (ids of retired scenes are reused).
+ * Once the pools exist (a reservation or a first step) the scene is placed and
+ * uploaded at once and takes part from the next step on; AVBD_ERR_NOMEM means
+ * it does not fit in the free pool space now (nothing was changed). */
 int32_t avbd_batch_add_scene(AvbdBatch* b, const AvbdWorld* w);
-/* Retires a scene and frees its slots for later admissions. */
+/* Retires a scene and returns its pool space for later admissions. */
 int32_t avbd_batch_remove_scene(AvbdBatch* b, int32_t scene);
+/* Index of a live scene's first body in the pose buffers of avbd_batch_get_all_poses. */
+int32_t avbd_batch_scene_body_offset(const AvbdBatch* b, int32_t scene);
 /* Advances every live scene by `steps` steps (one persistent kernel launch per
  * step, replayed from a CUDA graph). Returns AVBD_STATUS_OK or an error. */
 int32_t avbd_batch_step(AvbdBatch* b, int32_t steps);
+/* Scenes held (live or staged). */
 int32_t avbd_batch_num_scenes(const AvbdBatch* b);
 int32_t avbd_batch_scene_status(AvbdBatch* b, int32_t scene);
 int32_t avbd_batch_scene_bodies(const AvbdBatch* b, int32_t scene);
@@ -197,8 +208,10 @@ int64_t avbd_batch_dynamic_bodies(const AvbdBatch* b);
 /* Poses of one scene into host buffers (pos n*3, quat n*4). */
 int32_t avbd_batch_get_state(AvbdBatch* b, int32_t scene, float* pos, float* quat_wxyz, float* vel,
                              float* omega);
-/* Poses of all live scenes packed in scene order into one host buffer each. */
-int32_t avbd_batch_get_all_poses(AvbdBatch* b, float* pos, float* quat_wxyz, int64_t max_bodies);
+/* Poses of every pool slot (pos and rotation x y z w as float4 per body) into
+ * host buffers of max_bodies float4; a scene's bodies start at
+ * avbd_batch_scene_body_offset(). */
+int32_t avbd_batch_get_all_poses(AvbdBatch* b, float* pos, float* quat_xyzw, int64_t max_bodies);
 /* Device bytes a scene staged in `w` needs inside a batch (admission control). */
 int64_t avbd_scene_footprint_bytes(const AvbdWorld* w);
 /* Per-scene counters after the last step: status, colours, candidate pairs,

@@ -79,6 +79,8 @@ SIGNATURES = [
     ("avbd_batch_create", [C.POINTER(AvbdParams), C.c_int32, C.POINTER(_V)], C.c_int32),
     ("avbd_batch_destroy", [_V], C.c_int32),
     ("avbd_batch_add_scene", [_V, _V], C.c_int32),
+    ("avbd_batch_reserve", [_V, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int32], C.c_int32),
+    ("avbd_batch_scene_body_offset", [_V, C.c_int32], C.c_int32),
     ("avbd_batch_remove_scene", [_V, C.c_int32], C.c_int32),
     ("avbd_batch_step", [_V, C.c_int32], C.c_int32),
     ("avbd_batch_num_scenes", [_V], C.c_int32),

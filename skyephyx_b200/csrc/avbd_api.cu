@@ -6,6 +6,7 @@
 #include <cmath>
 #include <cstdio>
 #include <cstring>
+#include <map>
 #include <memory>
 #include <new>
 #include <vector>
@@ -162,7 +163,7 @@ __global__ void k_remove_oob(World W) {
             p.z > kBoundMax) {
             W.flags[b] = fl | kBodyRemoved;
             atomicAdd(&W.sstate[0].topo, 1);
-            for (int e = W.sinc_off[b]; e < W.sinc_off[b + 1]; ++e) {
+            for (int e = W.sinc_off[b]; e < W.sinc_off[b] + W.sinc_n[b]; ++e) {
                 const uint32_t ent = W.sinc[e];
                 const uint32_t k = ent_kind(ent), idx = ent_index(ent);
                 if (k == kEntForce) atomicOr(&W.ftype[idx], kForceRemoved);
@@ -198,8 +199,10 @@ __global__ void k_collide(World W, int a, int b, uint32_t* ids, float* data, int
 // 1 keeps the step in about 156 registers, 2 in 128, 3 in 80 and 4 in 64 with
 // some spilling, trading spills for resident warps.  The autotuner picks one.
 template <int MINB>
-__global__ void __launch_bounds__(256, MINB) k_batch_step(World W, const int* order, int nlive, int* queue) {
+__global__ void __launch_bounds__(256, MINB) k_batch_step(World W, const int* order, const int* nlive_ptr,
+                                                            int* queue) {
     __shared__ int s_q;
+    const int nlive = *nlive_ptr;   // live scenes, read from device memory so the graph stays replayable
     for (;;) {
         if (threadIdx.x == 0) s_q = atomicAdd(queue, 1);
         __syncthreads();
@@ -275,8 +278,8 @@ struct Pools {
         A(alloc(W.massI, nb)); A(alloc(W.Mw0, nb)); A(alloc(W.Mw1, nb));
         A(alloc(W.flags, nb)); A(alloc(W.friction, nb)); A(alloc(W.colour, nb)); A(alloc(W.local, nb));
         A(alloc(W.reset_flag, nb));
-        A(alloc_c(W.sinc_off, nb + 1)); A(alloc_c(W.sinc_nf, nb)); A(alloc_c(W.sinc, nsinc));
-        A(alloc_c(W.spartner_off, nb + 1)); A(alloc_c(W.spartner, 2 * (size_t)nsp));
+        A(alloc_c(W.sinc_off, nb)); A(alloc_c(W.sinc_n, nb)); A(alloc_c(W.sinc_nf, nb)); A(alloc_c(W.sinc, nsinc));
+        A(alloc_c(W.spartner_off, nb)); A(alloc_c(W.spartner_n, nb)); A(alloc_c(W.spartner, 2 * (size_t)nsp));
         A(alloc(W.inc_off, nb)); A(alloc(W.inc_cnt, nb)); A(alloc(W.cntB, nb)); A(alloc(W.bcur, nb));
         A(alloc(W.cand_cnt, nb)); A(alloc(W.cand_off, nb));
         A(alloc(W.col_list, nb)); A(alloc(W.col_start, (size_t)ns * (kMaxColours + 1)));
@@ -362,91 +365,173 @@ void scene_caps(const HostScene& h, int& candcap, int& kcap) {
 }
 
 template <typename T>
-void put(T* dst, const std::vector<T>& src, size_t at = 0) {
-    if (!src.empty()) cudaMemcpy(dst + at, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice);
+void put(T* dst, const std::vector<T>& src, size_t at, cudaStream_t st) {
+    if (!src.empty()) cudaMemcpyAsync(dst + at, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, st);
 }
 
-// Packs scenes into freshly allocated pools (state of each scene as staged).
-cudaError_t pack_scenes(Pools& P, const std::vector<const HostScene*>& sc, const std::vector<int>& candcaps,
-                        const std::vector<int>& kcaps, const std::vector<int>& groups, std::vector<SceneDesc>& descs) {
-    P.release();
-    P.ns = (int)sc.size();
-    P.nb = P.nf = P.nt = P.nr = P.ncand = P.nk = P.ninc = 0;
-    descs.resize(sc.size());
-    std::vector<int> soff, snf, poff;
-    std::vector<uint32_t> sent;
-    std::vector<int2> partners;
-    for (size_t i = 0; i < sc.size(); ++i) {
-        const HostScene& h = *sc[i];
-        SceneDesc& d = descs[i];
-        d.body0 = P.nb; d.nbody = h.nbody();
-        d.force0 = P.nf; d.nforce = h.nforce();
-        d.tet0 = P.nt; d.ntet = h.ntet();
-        d.tri0 = P.nr; d.ntri = h.ntri();
-        d.cand0 = P.ncand; d.candcap = candcaps[i];
-        d.k0 = P.nk; d.kcap = kcaps[i];
-        d.ndynamic = h.ndynamic();
-        d.group = groups[i];
-        const size_t before = sent.size();
-        h.build_static_incidence(soff, snf, sent, poff, partners, d.body0, d.force0, d.tet0, d.tri0);
-        // static offsets were computed relative to this scene's start of sent
-        for (int b = 0; b < d.nbody; ++b) {
-            soff[d.body0 + b] += 0;   // already global (sent grows monotonically)
+// First-fit allocator of index ranges in one pool, with coalescing frees.
+struct Ranges {
+    int cap = 0;
+    std::map<int, int> free_;   // start -> length
+    void reset(int c) {
+        cap = c;
+        free_.clear();
+        if (c > 0) free_[0] = c;
+    }
+    int alloc(int n) {
+        if (n <= 0) return 0;
+        for (auto it = free_.begin(); it != free_.end(); ++it) {
+            if (it->second >= n) {
+                const int s = it->first, len = it->second;
+                free_.erase(it);
+                if (len > n) free_[s + n] = len - n;
+                return s;
+            }
         }
-        d.inc0 = P.ninc;
-        d.inccap = (int)(sent.size() - before) + 2 * d.candcap;
-        P.nb += d.nbody; P.nf += d.nforce; P.nt += d.ntet; P.nr += d.ntri;
-        P.ncand += d.candcap; P.nk += d.kcap; P.ninc += d.inccap;
+        return -1;
     }
-    soff.push_back((int)sent.size());
-    poff.push_back((int)partners.size());
-    P.nsinc = (int)sent.size();
-    P.nsp = (int)partners.size();
-    cudaError_t e = P.allocate_all();
-    if (e != cudaSuccess) return e;
+    void release(int s, int n) {
+        if (n <= 0) return;
+        auto it = free_.emplace(s, n).first;
+        auto nx = std::next(it);
+        if (nx != free_.end() && it->first + it->second == nx->first) {
+            it->second += nx->second;
+            free_.erase(nx);
+        }
+        if (it != free_.begin()) {
+            auto pv = std::prev(it);
+            if (pv->first + pv->second == it->first) {
+                pv->second += it->second;
+                free_.erase(it);
+            }
+        }
+    }
+};
+
+// Where one scene lives in the pools.
+struct Region {
+    int body0 = 0, nbody = 0, force0 = 0, nforce = 0, tet0 = 0, ntet = 0, tri0 = 0, ntri = 0;
+    int cand0 = 0, ncand = 0, k0 = 0, nk = 0, inc0 = 0, ninc = 0, sinc0 = 0, nsinc = 0, sp0 = 0, nsp = 0;
+};
+
+struct Allocs {
+    Ranges bodies, forces, tets, tris, cand, k, inc, sinc, sp;
+    void reset(const Pools& P) {
+        bodies.reset(P.nb); forces.reset(P.nf); tets.reset(P.nt); tris.reset(P.nr); cand.reset(P.ncand);
+        k.reset(P.nk); inc.reset(P.ninc); sinc.reset(P.nsinc); sp.reset(P.nsp);
+    }
+    void release(const Region& r) {
+        bodies.release(r.body0, r.nbody); forces.release(r.force0, r.nforce); tets.release(r.tet0, r.ntet);
+        tris.release(r.tri0, r.ntri); cand.release(r.cand0, r.ncand); k.release(r.k0, r.nk);
+        inc.release(r.inc0, r.ninc); sinc.release(r.sinc0, r.nsinc); sp.release(r.sp0, r.nsp);
+    }
+};
+
+// Static incidence of a scene, built once per placement.
+struct StaticInc {
+    std::vector<int> off, cnt, nf, poff, pcnt;
+    std::vector<uint32_t> ent;
+    std::vector<int2> partners;
+};
+
+// Reserves pool ranges for a scene; false (and nothing held) if a pool is full.
+bool place_scene(Allocs& A, const HostScene& h, int candcap, int kcap, int nsinc, int nsp, Region& r) {
+    r = Region{};
+    r.nbody = h.nbody(); r.nforce = h.nforce(); r.ntet = h.ntet(); r.ntri = h.ntri();
+    r.ncand = candcap; r.nk = kcap; r.nsinc = nsinc; r.nsp = nsp; r.ninc = nsinc + 2 * candcap;
+    bool ok = true;
+    auto take = [&](Ranges& rg, int n, int& at) {
+        if (!ok) return;
+        at = rg.alloc(n);
+        if (at < 0) { ok = false; at = 0; }
+    };
+    Region got;   // ranges taken so far, for the rollback
+    take(A.bodies, r.nbody, r.body0); if (ok) { got.body0 = r.body0; got.nbody = r.nbody; }
+    take(A.forces, r.nforce, r.force0); if (ok) { got.force0 = r.force0; got.nforce = r.nforce; }
+    take(A.tets, r.ntet, r.tet0); if (ok) { got.tet0 = r.tet0; got.ntet = r.ntet; }
+    take(A.tris, r.ntri, r.tri0); if (ok) { got.tri0 = r.tri0; got.ntri = r.ntri; }
+    take(A.cand, r.ncand, r.cand0); if (ok) { got.cand0 = r.cand0; got.ncand = r.ncand; }
+    take(A.k, r.nk, r.k0); if (ok) { got.k0 = r.k0; got.nk = r.nk; }
+    take(A.inc, r.ninc, r.inc0); if (ok) { got.inc0 = r.inc0; got.ninc = r.ninc; }
+    take(A.sinc, r.nsinc, r.sinc0); if (ok) { got.sinc0 = r.sinc0; got.nsinc = r.nsinc; }
+    take(A.sp, r.nsp, r.sp0); if (ok) { got.sp0 = r.sp0; got.nsp = r.nsp; }
+    if (!ok) A.release(got);
+    return ok;
+}
+
+// Writes a placed scene (as staged) into the pools and its descriptor/state
+// into scene slot `slot`.
+void upload_scene(Pools& P, const HostScene& h, const StaticInc& si, const Region& r, int group, int slot,
+                  SceneDesc& d, cudaStream_t st) {
+    d.body0 = r.body0; d.nbody = r.nbody;
+    d.force0 = r.force0; d.nforce = r.nforce;
+    d.tet0 = r.tet0; d.ntet = r.ntet;
+    d.tri0 = r.tri0; d.ntri = r.ntri;
+    d.cand0 = r.cand0; d.candcap = r.ncand;
+    d.k0 = r.k0; d.kcap = r.nk;
+    d.inc0 = r.inc0; d.inccap = r.ninc;
+    d.ndynamic = h.ndynamic();
+    d.group = group;
     World& W = P.W;
-    std::vector<int> local;
-    for (size_t i = 0; i < sc.size(); ++i) {
-        const HostScene& h = *sc[i];
-        const SceneDesc& d = descs[i];
-        put(W.pos, h.pos, d.body0); put(W.rot, h.rot, d.body0); put(W.scale, h.scale, d.body0);
-        put(W.vel, h.vel, d.body0); put(W.omega, h.omega, d.body0); put(W.massI, h.massI, d.body0);
-        put(W.flags, h.flags, d.body0); put(W.friction, h.friction, d.body0);
-        put(W.lpos, h.pos, d.body0); put(W.lrot, h.rot, d.body0);
-        put(W.ipos, h.pos, d.body0); put(W.irot, h.rot, d.body0);
-        local.resize(d.nbody);
-        for (int b = 0; b < d.nbody; ++b) local[b] = b;
-        put(W.local, local, d.body0);
-        // forces: body ids become global
-        std::vector<int2> fb = h.fbody;
-        for (auto& ab : fb) { if (ab.x >= 0) ab.x += d.body0; ab.y += d.body0; }
-        put(W.ftype, h.ftype, d.force0); put(W.fbody, fb, d.force0); put(W.frA, h.frA, d.force0);
-        put(W.frB, h.frB, d.force0); put(W.fq, h.fq, d.force0); put(W.fparam, h.fparam, d.force0);
-        put(W.fk, h.fk, 6 * (size_t)d.force0); put(W.ffrac, h.ffrac, 6 * (size_t)d.force0);
-        put(W.ffmin, h.ffmin, 6 * (size_t)d.force0); put(W.ffmax, h.ffmax, 6 * (size_t)d.force0);
-        std::vector<int4> ti = h.tidx;
-        for (auto& t : ti) { t.x += d.body0; t.y += d.body0; t.z += d.body0; t.w += d.body0; }
-        put(W.tidx, ti, d.tet0); put(W.tDmInv, h.tDmInv, 9 * (size_t)d.tet0);
-        put(W.tgradN, h.tgradN, 12 * (size_t)d.tet0); put(W.tparam, h.tparam, d.tet0);
-        std::vector<int4> ri = h.ridx;
-        for (auto& t : ri) { t.x += d.body0; t.y += d.body0; t.z += d.body0; }
-        put(W.ridx, ri, d.tri0); put(W.rDmInv, h.rDmInv, d.tri0);
-        put(W.rgradN, h.rgradN, 6 * (size_t)d.tri0); put(W.rparam, h.rparam, d.tri0);
+    put(W.pos, h.pos, d.body0, st); put(W.rot, h.rot, d.body0, st); put(W.scale, h.scale, d.body0, st);
+    put(W.vel, h.vel, d.body0, st); put(W.omega, h.omega, d.body0, st); put(W.massI, h.massI, d.body0, st);
+    put(W.flags, h.flags, d.body0, st); put(W.friction, h.friction, d.body0, st);
+    put(W.lpos, h.pos, d.body0, st); put(W.lrot, h.rot, d.body0, st);
+    put(W.ipos, h.pos, d.body0, st); put(W.irot, h.rot, d.body0, st);
+    if (d.nbody) {
+        cudaMemsetAsync(W.pvel + d.body0, 0, d.nbody * sizeof(float4), st);
+        cudaMemsetAsync(W.reset_flag + d.body0, 0, d.nbody * sizeof(int), st);
     }
-    cudaMemcpy(const_cast<int*>(W.sinc_off), soff.data(), soff.size() * sizeof(int), cudaMemcpyHostToDevice);
-    if (!snf.empty())
-        cudaMemcpy(const_cast<int*>(W.sinc_nf), snf.data(), snf.size() * sizeof(int), cudaMemcpyHostToDevice);
-    if (!sent.empty())
-        cudaMemcpy(const_cast<uint32_t*>(W.sinc), sent.data(), sent.size() * sizeof(uint32_t), cudaMemcpyHostToDevice);
-    cudaMemcpy(const_cast<int*>(W.spartner_off), poff.data(), poff.size() * sizeof(int), cudaMemcpyHostToDevice);
-    if (!partners.empty())
-        cudaMemcpy(const_cast<int*>(W.spartner), partners.data(), partners.size() * sizeof(int2),
-                   cudaMemcpyHostToDevice);
-    cudaMemcpy(P.d_scenes, descs.data(), descs.size() * sizeof(SceneDesc), cudaMemcpyHostToDevice);
-    std::vector<SceneState> st(sc.size());
-    std::memset(st.data(), 0, st.size() * sizeof(SceneState));
-    cudaMemcpy(P.d_sstate, st.data(), st.size() * sizeof(SceneState), cudaMemcpyHostToDevice);
-    return cudaGetLastError();
+    std::vector<int> tmp(d.nbody);
+    for (int b = 0; b < d.nbody; ++b) tmp[b] = b;
+    put(W.local, tmp, d.body0, st);
+    for (int b = 0; b < d.nbody; ++b) tmp[b] = si.off[b] + r.sinc0;
+    put(const_cast<int*>(W.sinc_off), tmp, d.body0, st);
+    put(const_cast<int*>(W.sinc_n), si.cnt, d.body0, st);
+    put(const_cast<int*>(W.sinc_nf), si.nf, d.body0, st);
+    put(const_cast<uint32_t*>(W.sinc), si.ent, r.sinc0, st);
+    for (int b = 0; b < d.nbody; ++b) tmp[b] = si.poff[b] + r.sp0;
+    put(const_cast<int*>(W.spartner_off), tmp, d.body0, st);
+    put(const_cast<int*>(W.spartner_n), si.pcnt, d.body0, st);
+    put(reinterpret_cast<int2*>(const_cast<int*>(W.spartner)), si.partners, r.sp0, st);
+    std::vector<int2> fb = h.fbody;
+    for (auto& ab : fb) { if (ab.x >= 0) ab.x += d.body0; ab.y += d.body0; }
+    put(W.ftype, h.ftype, d.force0, st); put(W.fbody, fb, d.force0, st); put(W.frA, h.frA, d.force0, st);
+    put(W.frB, h.frB, d.force0, st); put(W.fq, h.fq, d.force0, st); put(W.fparam, h.fparam, d.force0, st);
+    put(W.fk, h.fk, 6 * (size_t)d.force0, st); put(W.ffrac, h.ffrac, 6 * (size_t)d.force0, st);
+    put(W.ffmin, h.ffmin, 6 * (size_t)d.force0, st); put(W.ffmax, h.ffmax, 6 * (size_t)d.force0, st);
+    if (d.nforce) {
+        cudaMemsetAsync(W.fpen + 6 * (size_t)d.force0, 0, 6 * (size_t)d.nforce * sizeof(float), st);
+        cudaMemsetAsync(W.flam + 6 * (size_t)d.force0, 0, 6 * (size_t)d.nforce * sizeof(float), st);
+    }
+    std::vector<int4> ti = h.tidx;
+    for (auto& t : ti) { t.x += d.body0; t.y += d.body0; t.z += d.body0; t.w += d.body0; }
+    put(W.tidx, ti, d.tet0, st); put(W.tDmInv, h.tDmInv, 9 * (size_t)d.tet0, st);
+    put(W.tgradN, h.tgradN, 12 * (size_t)d.tet0, st); put(W.tparam, h.tparam, d.tet0, st);
+    std::vector<int4> ri = h.ridx;
+    for (auto& t : ri) { t.x += d.body0; t.y += d.body0; t.z += d.body0; }
+    put(W.ridx, ri, d.tri0, st); put(W.rDmInv, h.rDmInv, d.tri0, st);
+    put(W.rgradN, h.rgradN, 6 * (size_t)d.tri0, st); put(W.rparam, h.rparam, d.tri0, st);
+    cudaMemcpyAsync(P.d_scenes + slot, &d, sizeof(SceneDesc), cudaMemcpyHostToDevice, st);
+    cudaMemsetAsync(P.d_sstate + slot, 0, sizeof(SceneState), st);
+    cudaStreamSynchronize(st);   // the host vectors above are temporaries
+}
+
+// Static incidence entries and joint/spring partner entries a scene needs.
+void static_counts(const HostScene& h, int& nsinc, int& nsp) {
+    nsinc = 4 * h.ntet() + 3 * h.ntri();
+    nsp = 0;
+    for (const int2& ab : h.fbody) {
+        nsinc += ab.x >= 0 ? 2 : 1;
+        nsp += ab.x >= 0 ? 2 : 0;
+    }
+}
+
+StaticInc static_incidence(const HostScene& h, const Region& r) {
+    StaticInc si;
+    h.build_static_incidence(si.off, si.cnt, si.nf, si.ent, si.poff, si.pcnt, si.partners, r.body0, r.force0, r.tet0,
+                             r.tri0);
+    return si;
 }
 
 Params to_params(const AvbdParams& p) {
@@ -512,12 +597,23 @@ int upload(AvbdWorld* w) {
         if (cudaStreamCreateWithFlags(&w->stream, cudaStreamNonBlocking) != cudaSuccess) return AVBD_ERR_CUDA;
         for (auto& e : w->ev) cudaEventCreate(&e);
     }
-    int cc, kc;
+    int cc, kc, nsinc, nsp;
     scene_caps(w->h, cc, kc);
-    std::vector<const HostScene*> sc{&w->h};
+    static_counts(w->h, nsinc, nsp);
     const int g = w->group > 0 ? w->group : scene_group(w->h, 4, 8);
-    if (pack_scenes(w->P, sc, {cc}, {kc}, {g}, w->descs) != cudaSuccess) return AVBD_ERR_NOMEM;
-    w->P.W.P = to_params(w->params);
+    Pools& P = w->P;
+    P.release();
+    P.ns = 1; P.nb = w->h.nbody(); P.nf = w->h.nforce(); P.nt = w->h.ntet(); P.nr = w->h.ntri();
+    P.ncand = cc; P.nk = kc; P.nsinc = nsinc; P.nsp = nsp; P.ninc = nsinc + 2 * cc;
+    if (P.allocate_all() != cudaSuccess) return AVBD_ERR_NOMEM;
+    Allocs A;
+    A.reset(P);
+    Region reg;
+    if (!place_scene(A, w->h, cc, kc, nsinc, nsp, reg)) return AVBD_ERR_NOMEM;
+    w->descs.assign(1, SceneDesc{});
+    upload_scene(P, w->h, static_incidence(w->h, reg), reg, g, 0, w->descs[0], w->stream);
+    if (cudaGetLastError() != cudaSuccess) return AVBD_ERR_CUDA;
+    P.W.P = to_params(w->params);
     w->uploaded = true;
     return 0;
 }
@@ -673,14 +769,21 @@ int world_step(AvbdWorld* w) {
 struct AvbdBatch {
     AvbdParams params{};
     int device = 0;
-    std::vector<HostScene> scenes;   // staged copies, by scene id
-    std::vector<int> live;           // 1 = live
-    bool packed = false;
-    Pools P;
+    // scene slots (scene id = slot); a retired slot is reused by a later scene
+    std::vector<HostScene> scenes;   // staged copies (emptied when a scene retires)
+    std::vector<int> state;          // 0 free, 1 live, 2 staged (not placed yet)
+    std::vector<Region> regions;
     std::vector<SceneDesc> descs;
-    int* d_order = nullptr;
+    std::vector<int> bodies;         // body count of each slot's scene
+    std::vector<int> dynamic;        // dynamic bodies of each slot's scene
+    bool reserved = false;           // pools allocated
+    Pools P;
+    Allocs A;
+    int* d_order = nullptr;          // live slots, largest first
+    int* d_nlive = nullptr;
     int* d_queue = nullptr;
     int nlive = 0;
+    bool order_dirty = true;
     cudaStream_t stream = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
     cudaGraphExec_t graph = nullptr;
@@ -689,7 +792,6 @@ struct AvbdBatch {
     int variant = 1;                     // register budget of the persistent kernel (1..4, see k_batch_step)
     int grid = 0;
     float last_ms = 0.f;
-    std::vector<SceneState> st;
 };
 
 namespace {
@@ -698,7 +800,7 @@ void batch_drop_graph(AvbdBatch* b) {
     if (b->graph) { cudaGraphExecDestroy(b->graph); b->graph = nullptr; }
 }
 
-int batch_pack(AvbdBatch* b) {
+int batch_stream(AvbdBatch* b) {
     int r = device_ready(b->device);
     if (r) return r;
     if (!b->stream) {
@@ -706,35 +808,93 @@ int batch_pack(AvbdBatch* b) {
         cudaEventCreate(&b->e0);
         cudaEventCreate(&b->e1);
     }
-    batch_drop_graph(b);
-    std::vector<const HostScene*> sc;
-    std::vector<int> cc, kc, gr;
-    for (auto& h : b->scenes) {
-        int c, k;
-        scene_caps(h, c, k);
-        sc.push_back(&h);
-        cc.push_back(c);
-        kc.push_back(k);
-        gr.push_back(scene_group(h, b->group_rigid, b->group_fem));
+    return 0;
+}
+
+// Allocates the pools with the given capacities (empty of scenes).
+int batch_reserve(AvbdBatch* b, int64_t bodies, int64_t forces, int64_t tets, int64_t tris, int64_t nscenes,
+                  int64_t nsinc, int64_t nsp) {
+    int r = batch_stream(b);
+    if (r) return r;
+    const int64_t ncand = 16 * bodies + 64 * nscenes, nk = 24 * bodies + 128 * nscenes;
+    const int64_t ninc = nsinc + 2 * ncand;
+    const int64_t lim = 0x07FFFFFF;   // incidence entries index 27 bits
+    if (bodies > lim || forces > lim || tets > lim || tris > lim || ncand > lim || nk > INT32_MAX || ninc > INT32_MAX ||
+        nsinc > INT32_MAX || nscenes > (1 << 20))
+        return AVBD_ERR_INVALID;
+    Pools& P = b->P;
+    P.release();
+    P.ns = (int)nscenes; P.nb = (int)bodies; P.nf = (int)forces; P.nt = (int)tets; P.nr = (int)tris;
+    P.ncand = (int)ncand; P.nk = (int)nk; P.nsinc = (int)nsinc; P.nsp = (int)nsp; P.ninc = (int)ninc;
+    if (P.allocate_all() != cudaSuccess) {
+        P.release();
+        return AVBD_ERR_NOMEM;
     }
-    if (pack_scenes(b->P, sc, cc, kc, gr, b->descs) != cudaSuccess) return AVBD_ERR_NOMEM;
-    b->P.W.P = to_params(b->params);
-    // work queue: live scenes, largest first
-    std::vector<int> order;
-    for (size_t i = 0; i < b->scenes.size(); ++i) if (b->live[i]) order.push_back((int)i);
-    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-        const HostScene& a = b->scenes[x];
-        const HostScene& c = b->scenes[y];
-        return (a.nbody() + a.ntet()) > (c.nbody() + c.ntet());
-    });
+    P.W.P = to_params(b->params);
+    b->A.reset(P);
     if (b->d_order) cudaFree(b->d_order);
+    if (b->d_nlive) cudaFree(b->d_nlive);
     if (b->d_queue) cudaFree(b->d_queue);
-    cudaMalloc(&b->d_order, std::max<size_t>(order.size(), 1) * sizeof(int));
-    cudaMalloc(&b->d_queue, sizeof(int));
-    if (!order.empty())
-        cudaMemcpy(b->d_order, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice);
+    if (cudaMalloc(&b->d_order, std::max<int64_t>(nscenes, 1) * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&b->d_nlive, sizeof(int)) != cudaSuccess || cudaMalloc(&b->d_queue, sizeof(int)) != cudaSuccess)
+        return AVBD_ERR_NOMEM;
+    cudaMemset(b->d_nlive, 0, sizeof(int));
+    b->reserved = true;
+    b->order_dirty = true;
+    batch_drop_graph(b);
+    return 0;
+}
+
+// Places and uploads the staged scene of `slot`; AVBD_ERR_NOMEM if the pools are full.
+int batch_admit(AvbdBatch* b, int slot) {
+    if (slot >= b->P.ns) return AVBD_ERR_NOMEM;
+    HostScene& h = b->scenes[slot];
+    int cc, kc, nsinc, nsp;
+    scene_caps(h, cc, kc);
+    static_counts(h, nsinc, nsp);
+    Region reg;
+    if (!place_scene(b->A, h, cc, kc, nsinc, nsp, reg)) return AVBD_ERR_NOMEM;
+    b->regions[slot] = reg;
+    upload_scene(b->P, h, static_incidence(h, reg), reg, scene_group(h, b->group_rigid, b->group_fem), slot,
+                 b->descs[slot], b->stream);
+    b->state[slot] = 1;
+    b->order_dirty = true;
+    return 0;
+}
+
+// Uploads the live queue (largest scenes first) when it changed.
+void batch_sync_order(AvbdBatch* b) {
+    if (!b->order_dirty) return;
+    std::vector<int> order;
+    for (size_t i = 0; i < b->state.size(); ++i)
+        if (b->state[i] == 1) order.push_back((int)i);
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        const SceneDesc& a = b->descs[x];
+        const SceneDesc& c = b->descs[y];
+        return (a.nbody + a.ntet) > (c.nbody + c.ntet);
+    });
     b->nlive = (int)order.size();
-    b->packed = true;
+    if (!order.empty())
+        cudaMemcpyAsync(b->d_order, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream);
+    cudaMemcpyAsync(b->d_nlive, &b->nlive, sizeof(int), cudaMemcpyHostToDevice, b->stream);
+    cudaStreamSynchronize(b->stream);
+    b->order_dirty = false;
+}
+
+// First step without an explicit reservation: pools sized to the staged scenes.
+int batch_pack(AvbdBatch* b) {
+    int64_t nb = 0, nf = 0, nt = 0, nr = 0, nsinc = 0, nsp = 0;
+    for (size_t i = 0; i < b->scenes.size(); ++i) {
+        if (b->state[i] != 2) continue;
+        const HostScene& h = b->scenes[i];
+        int a, c;
+        static_counts(h, a, c);
+        nb += h.nbody(); nf += h.nforce(); nt += h.ntet(); nr += h.ntri(); nsinc += a; nsp += c;
+    }
+    int r = batch_reserve(b, nb, nf, nt, nr, (int64_t)b->scenes.size(), nsinc, nsp);
+    if (r) return r;
+    for (size_t i = 0; i < b->scenes.size(); ++i)
+        if (b->state[i] == 2 && (r = batch_admit(b, (int)i))) return r;
     return 0;
 }
 
@@ -769,10 +929,10 @@ int batch_build_graph(AvbdBatch* b) {
     cudaMemsetAsync(b->d_queue, 0, sizeof(int), b->stream);
     const size_t smem = kStagedBodies * sizeof(float4);
     switch (b->variant) {
-        case 4: k_batch_step<4><<<b->grid, b->threads, smem, b->stream>>>(b->P.W, b->d_order, b->nlive, b->d_queue); break;
-        case 3: k_batch_step<3><<<b->grid, b->threads, smem, b->stream>>>(b->P.W, b->d_order, b->nlive, b->d_queue); break;
-        case 2: k_batch_step<2><<<b->grid, b->threads, smem, b->stream>>>(b->P.W, b->d_order, b->nlive, b->d_queue); break;
-        default: k_batch_step<1><<<b->grid, b->threads, smem, b->stream>>>(b->P.W, b->d_order, b->nlive, b->d_queue); break;
+        case 4: k_batch_step<4><<<b->grid, b->threads, smem, b->stream>>>(b->P.W, b->d_order, b->d_nlive, b->d_queue); break;
+        case 3: k_batch_step<3><<<b->grid, b->threads, smem, b->stream>>>(b->P.W, b->d_order, b->d_nlive, b->d_queue); break;
+        case 2: k_batch_step<2><<<b->grid, b->threads, smem, b->stream>>>(b->P.W, b->d_order, b->d_nlive, b->d_queue); break;
+        default: k_batch_step<1><<<b->grid, b->threads, smem, b->stream>>>(b->P.W, b->d_order, b->d_nlive, b->d_queue); break;
     }
     if (cudaStreamEndCapture(b->stream, &g) != cudaSuccess) return AVBD_ERR_CUDA;
     cudaError_t e = cudaGraphInstantiate(&b->graph, g, 0);
@@ -1138,6 +1298,7 @@ int32_t avbd_batch_destroy(AvbdBatch* b) {
     if (b->stream) cudaStreamSynchronize(b->stream);
     batch_drop_graph(b);
     if (b->d_order) cudaFree(b->d_order);
+    if (b->d_nlive) cudaFree(b->d_nlive);
     if (b->d_queue) cudaFree(b->d_queue);
     if (b->e0) cudaEventDestroy(b->e0);
     if (b->e1) cudaEventDestroy(b->e1);
@@ -1146,38 +1307,70 @@ int32_t avbd_batch_destroy(AvbdBatch* b) {
     return 0;
 }
 
+int32_t avbd_batch_reserve(AvbdBatch* b, int64_t bodies, int64_t forces, int64_t tets, int64_t tris, int32_t scenes) {
+    if (!b || bodies < 0 || forces < 0 || tets < 0 || tris < 0 || scenes < 1) return AVBD_ERR_INVALID;
+    if (b->reserved) return AVBD_ERR_STATE;
+    int r = batch_reserve(b, bodies, forces, tets, tris, scenes, 2 * forces + 4 * tets + 3 * tris, 2 * forces);
+    if (r) return r;
+    for (size_t i = 0; i < b->scenes.size(); ++i)
+        if (b->state[i] == 2 && (r = batch_admit(b, (int)i))) return r;
+    return 0;
+}
+
 int32_t avbd_batch_add_scene(AvbdBatch* b, const AvbdWorld* w) {
     if (!b || !w) return AVBD_ERR_INVALID;
-    if (b->packed) return AVBD_ERR_STATE;
-    b->scenes.push_back(w->h);
-    b->live.push_back(1);
-    return (int)b->scenes.size() - 1;
+    int slot = -1;
+    for (size_t i = 0; i < b->state.size(); ++i)
+        if (b->state[i] == 0) { slot = (int)i; break; }
+    if (slot < 0) {
+        if (b->reserved && (int)b->state.size() >= b->P.ns) return AVBD_ERR_NOMEM;
+        slot = (int)b->state.size();
+        b->scenes.emplace_back();
+        b->state.push_back(0);
+        b->regions.emplace_back();
+        b->descs.emplace_back();
+        b->bodies.push_back(0);
+        b->dynamic.push_back(0);
+    }
+    b->scenes[slot] = w->h;
+    b->bodies[slot] = w->h.nbody();
+    b->dynamic[slot] = w->h.ndynamic();
+    b->state[slot] = 2;
+    if (b->reserved) {
+        cudaSetDevice(b->device);
+        int r = batch_admit(b, slot);
+        if (r) {   // no room in the pools: nothing was placed
+            b->scenes[slot] = HostScene();
+            b->state[slot] = 0;
+            return r;
+        }
+        b->scenes[slot] = HostScene();   // the device holds it now
+    }
+    return slot;
 }
 
 int32_t avbd_batch_remove_scene(AvbdBatch* b, int32_t scene) {
-    if (!b || scene < 0 || scene >= (int)b->scenes.size()) return AVBD_ERR_INVALID;
-    b->live[scene] = 0;
-    if (b->packed) {
-        // drop it from the work queue; its pool regions stay reserved until the batch is rebuilt
-        std::vector<int> order;
-        for (size_t i = 0; i < b->scenes.size(); ++i) if (b->live[i]) order.push_back((int)i);
-        std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-            return (b->scenes[x].nbody() + b->scenes[x].ntet()) > (b->scenes[y].nbody() + b->scenes[y].ntet());
-        });
-        cudaSetDevice(b->device);
-        if (!order.empty())
-            cudaMemcpy(b->d_order, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice);
-        b->nlive = (int)order.size();
-        batch_drop_graph(b);
+    if (!b || scene < 0 || scene >= (int)b->state.size() || b->state[scene] == 0) return AVBD_ERR_INVALID;
+    if (b->state[scene] == 1) {
+        b->A.release(b->regions[scene]);
+        b->order_dirty = true;
     }
+    b->state[scene] = 0;
+    b->scenes[scene] = HostScene();
+    b->bodies[scene] = 0;
+    b->dynamic[scene] = 0;
     return 0;
 }
 
 int32_t avbd_batch_step(AvbdBatch* b, int32_t steps) {
     if (!b || steps < 0) return AVBD_ERR_INVALID;
     int r;
-    if (!b->packed && (r = batch_pack(b))) return r;
+    if (!b->reserved) {
+        if ((r = batch_pack(b))) return r;
+        for (auto& h : b->scenes) h = HostScene();
+    }
     cudaSetDevice(b->device);
+    batch_sync_order(b);
     if (!b->grid) batch_launch_shape(b);
     b->P.W.P = to_params(b->params);
     if (!b->graph && (r = batch_build_graph(b))) return r;
@@ -1190,11 +1383,20 @@ int32_t avbd_batch_step(AvbdBatch* b, int32_t steps) {
     return cudaGetLastError() == cudaSuccess ? AVBD_STATUS_OK : AVBD_ERR_CUDA;
 }
 
-int32_t avbd_batch_num_scenes(const AvbdBatch* b) { return b ? (int)b->scenes.size() : AVBD_ERR_INVALID; }
+int32_t avbd_batch_num_scenes(const AvbdBatch* b) {
+    if (!b) return AVBD_ERR_INVALID;
+    int n = 0;
+    for (int s : b->state) n += s != 0;
+    return n;
+}
+
+static bool live_slot(const AvbdBatch* b, int scene) {
+    return b && scene >= 0 && scene < (int)b->state.size() && b->state[scene] == 1;
+}
 
 int32_t avbd_batch_scene_status(AvbdBatch* b, int32_t scene) {
-    if (!b || scene < 0 || scene >= (int)b->scenes.size()) return AVBD_ERR_INVALID;
-    if (!b->packed) return AVBD_STATUS_OK;
+    if (!b || scene < 0 || scene >= (int)b->state.size() || b->state[scene] == 0) return AVBD_ERR_INVALID;
+    if (b->state[scene] == 2) return AVBD_STATUS_OK;
     cudaSetDevice(b->device);
     SceneState st;
     if (cudaMemcpy(&st, b->P.d_sstate + scene, sizeof(SceneState), cudaMemcpyDeviceToHost) != cudaSuccess)
@@ -1203,8 +1405,8 @@ int32_t avbd_batch_scene_status(AvbdBatch* b, int32_t scene) {
 }
 
 int32_t avbd_batch_scene_info(AvbdBatch* b, int32_t scene, int32_t out[6]) {
-    if (!b || !out || scene < 0 || scene >= (int)b->scenes.size()) return AVBD_ERR_INVALID;
-    if (!b->packed) { for (int i = 0; i < 6; ++i) out[i] = 0; return 0; }
+    if (!b || !out || scene < 0 || scene >= (int)b->state.size() || b->state[scene] == 0) return AVBD_ERR_INVALID;
+    if (b->state[scene] == 2) { for (int i = 0; i < 6; ++i) out[i] = 0; return 0; }
     cudaSetDevice(b->device);
     SceneState st;
     if (cudaMemcpy(&st, b->P.d_sstate + scene, sizeof(SceneState), cudaMemcpyDeviceToHost) != cudaSuccess)
@@ -1215,29 +1417,27 @@ int32_t avbd_batch_scene_info(AvbdBatch* b, int32_t scene, int32_t out[6]) {
 }
 
 int32_t avbd_batch_scene_bodies(const AvbdBatch* b, int32_t scene) {
-    if (!b || scene < 0 || scene >= (int)b->scenes.size()) return AVBD_ERR_INVALID;
-    return b->scenes[scene].nbody();
+    if (!b || scene < 0 || scene >= (int)b->state.size() || b->state[scene] == 0) return AVBD_ERR_INVALID;
+    return b->bodies[scene];
 }
 
 int64_t avbd_batch_dynamic_bodies(const AvbdBatch* b) {
     if (!b) return AVBD_ERR_INVALID;
     int64_t n = 0;
-    for (size_t i = 0; i < b->scenes.size(); ++i)
-        if (b->live[i]) n += b->scenes[i].ndynamic();
+    for (size_t i = 0; i < b->state.size(); ++i)
+        if (b->state[i] != 0) n += b->dynamic[i];
     return n;
 }
 
 int32_t avbd_batch_get_state(AvbdBatch* b, int32_t scene, float* pos, float* quat, float* vel, float* omega) {
-    if (!b || scene < 0 || scene >= (int)b->scenes.size()) return AVBD_ERR_INVALID;
-    const HostScene& h = b->scenes[scene];
-    const int n = h.nbody();
-    if (!b->packed) return 0;
+    if (!live_slot(b, scene)) return AVBD_ERR_INVALID;
+    const int n = b->bodies[scene];
     cudaSetDevice(b->device);
     const int b0 = b->descs[scene].body0;
     std::vector<float4> buf(n);
     const World& W = b->P.W;
     auto fetch = [&](const float4* src, float* dst, bool q) {
-        if (!dst) return;
+        if (!dst || n == 0) return;
         cudaMemcpy(buf.data(), src + b0, n * sizeof(float4), cudaMemcpyDeviceToHost);
         for (int i = 0; i < n; ++i) {
             const float4 x = buf[i];
@@ -1253,7 +1453,7 @@ int32_t avbd_batch_get_state(AvbdBatch* b, int32_t scene, float* pos, float* qua
 }
 
 int32_t avbd_batch_get_all_poses(AvbdBatch* b, float* pos, float* quat, int64_t max_bodies) {
-    if (!b || !b->packed) return AVBD_ERR_STATE;
+    if (!b || !b->reserved) return AVBD_ERR_STATE;
     cudaSetDevice(b->device);
     const int n = b->P.nb;
     if (n > max_bodies) return AVBD_ERR_INVALID;
@@ -1266,16 +1466,29 @@ int32_t avbd_batch_get_all_poses(AvbdBatch* b, float* pos, float* quat, int64_t 
     return n;
 }
 
+int32_t avbd_batch_scene_body_offset(const AvbdBatch* b, int32_t scene) {
+    if (!live_slot(b, scene)) return AVBD_ERR_INVALID;
+    return b->descs[scene].body0;
+}
+
+// Device bytes per unit of each pool (allocate_all / alloc_tables).
+constexpr int64_t kBytesPerBody = 15 * 16 + 17 * 4;        // float4 state + per-body ints
+constexpr int64_t kBytesPerCand = 2 * (8 + 4 + 4 + 4 + 4);  // two manifold tables
+constexpr int64_t kBytesPerContact = 2 * (4 + 9 * 16);      // two contact pools
+constexpr int64_t kBytesPerForce = 4 + 8 + 6 * 16 + 6 * 6 * 4;
+constexpr int64_t kBytesPerTet = 16 + 36 + 48 + 16;
+constexpr int64_t kBytesPerTri = 16 + 16 + 24 + 16;
+
 int64_t avbd_scene_footprint_bytes(const AvbdWorld* w) {
     if (!w) return AVBD_ERR_INVALID;
-    int cc, kc;
+    int cc, kc, nsinc, nsp;
     scene_caps(w->h, cc, kc);
-    const int64_t nb = w->h.nbody();
-    int64_t bytes = nb * (16 * 15 + 4 * 16);
-    bytes += (int64_t)w->h.nforce() * (16 * 8 + 4 * 36 + 8);
-    bytes += (int64_t)w->h.ntet() * (16 + 36 + 48 + 16) + (int64_t)w->h.ntri() * (16 + 16 + 24 + 16);
-    bytes += 2 * (int64_t)cc * (8 + 4 + 4 + 4) + 2 * (int64_t)kc * (4 + 16 * 9);
-    bytes += 4 * (int64_t)(2 * cc + 8 * nb);
+    static_counts(w->h, nsinc, nsp);
+    int64_t bytes = (int64_t)w->h.nbody() * kBytesPerBody + (int64_t)w->h.nforce() * kBytesPerForce +
+                    (int64_t)w->h.ntet() * kBytesPerTet + (int64_t)w->h.ntri() * kBytesPerTri;
+    bytes += (int64_t)cc * kBytesPerCand + (int64_t)kc * kBytesPerContact;
+    bytes += 4 * ((int64_t)nsinc + 2 * cc) + 4 * (int64_t)nsinc + 8 * (int64_t)nsp;
+    bytes += sizeof(SceneDesc) + sizeof(SceneState) + 4 * (kMaxColours + 1);
     return bytes;
 }
 
@@ -1309,7 +1522,7 @@ static bool valid_group(int g) { return g == 1 || g == 2 || g == 4 || g == 8 || 
 
 int32_t avbd_batch_set_groups(AvbdBatch* b, int32_t rigid_group, int32_t fem_group) {
     if (!b || !valid_group(rigid_group) || !valid_group(fem_group)) return AVBD_ERR_INVALID;
-    if (b->packed) return AVBD_ERR_STATE;
+    if (b->reserved) return AVBD_ERR_STATE;
     b->group_rigid = rigid_group;
     b->group_fem = fem_group;
     return 0;

@@ -156,10 +156,12 @@ struct World {
     int* reset_flag;    // set by a fracturing force for the manifold reset pass
 
     // ---- static incidence (forces + energies), per body, built at upload ----
-    const int* sinc_off;     // global offsets into sinc (nbody_total + 1 entries)
+    const int* sinc_off;     // per body: first entry in sinc
+    const int* sinc_n;       // per body: number of entries
     const int* sinc_nf;      // per body: leading force entries (energy entries follow)
     const uint32_t* sinc;    // entries
-    const int* spartner_off; // joint/spring partners for the broadphase filter (nbody_total + 1)
+    const int* spartner_off; // per body: first joint/spring partner (broadphase filter)
+    const int* spartner_n;   // per body: number of partners
     const int* spartner;     // (partner body, force) pairs, as int2
 
     // ---- per-step incidence (CSR) ----

@@ -267,9 +267,10 @@ int HostScene::make_tet_volume(float ox, float oy, float oz, int nx, int ny, int
     return first;
 }
 
-void HostScene::build_static_incidence(std::vector<int>& off, std::vector<int>& nf, std::vector<uint32_t>& ent,
-                                       std::vector<int>& poff, std::vector<int2>& partners, int body_base,
-                                       int force_base, int tet_base, int tri_base) const {
+void HostScene::build_static_incidence(std::vector<int>& off, std::vector<int>& cnt, std::vector<int>& nf,
+                                       std::vector<uint32_t>& ent, std::vector<int>& poff, std::vector<int>& pcnt,
+                                       std::vector<int2>& partners, int body_base, int force_base, int tet_base,
+                                       int tri_base) const {
     const int n = nbody();
     std::vector<std::vector<uint32_t>> fe(n), ee(n);
     std::vector<std::vector<int2>> pp(n);
@@ -290,13 +291,16 @@ void HostScene::build_static_incidence(std::vector<int>& off, std::vector<int>& 
         const int v[3] = {ridx[t].x, ridx[t].y, ridx[t].z};
         for (int r = 0; r < 3; ++r) ee[v[r]].push_back(ent_make(kEntTri, (uint32_t)r, (uint32_t)(tri_base + t)));
     }
+    off.clear(); cnt.clear(); nf.clear(); ent.clear(); poff.clear(); pcnt.clear(); partners.clear();
     for (int b = 0; b < n; ++b) {
         off.push_back((int)ent.size());
         nf.push_back((int)fe[b].size());
         ent.insert(ent.end(), fe[b].begin(), fe[b].end());
         ent.insert(ent.end(), ee[b].begin(), ee[b].end());
+        cnt.push_back((int)ent.size() - off.back());
         poff.push_back((int)partners.size());
         partners.insert(partners.end(), pp[b].begin(), pp[b].end());
+        pcnt.push_back((int)partners.size() - poff.back());
     }
 }
 

@@ -57,10 +57,13 @@ struct HostScene {
     int make_tet_volume(float ox, float oy, float oz, int nx, int ny, int nz, float cell, float E, float nu,
                         float particle_mass, float friction_, bool pin_min_x);
 
-    // static incidence (forces then energies per body) and joint/spring partner lists
-    void build_static_incidence(std::vector<int>& off, std::vector<int>& nf, std::vector<uint32_t>& ent,
-                                std::vector<int>& poff, std::vector<int2>& partners, int body_base, int force_base,
-                                int tet_base, int tri_base) const;
+    // Static incidence (forces then energies per body) and joint/spring partner
+    // lists.  Offsets are relative to the scene's own entry / partner arrays;
+    // entry indices and partner bodies are global (shifted by the bases).
+    void build_static_incidence(std::vector<int>& off, std::vector<int>& cnt, std::vector<int>& nf,
+                                std::vector<uint32_t>& ent, std::vector<int>& poff, std::vector<int>& pcnt,
+                                std::vector<int2>& partners, int body_base, int force_base, int tet_base,
+                                int tri_base) const;
 };
 
 }  // namespace avbd

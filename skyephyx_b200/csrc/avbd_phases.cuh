@@ -103,7 +103,7 @@ AVBD_HD void predict_body(const World& W, int b) {
 // ===========================================================================
 AVBD_HD bool pair_constrained(const World& W, int sc_sinc_base, int i, int j) {
     // static partner list of i: (partner body, force) pairs
-    const int b0 = W.spartner_off[i], b1 = W.spartner_off[i + 1];
+    const int b0 = W.spartner_off[i], b1 = b0 + W.spartner_n[i];
     for (int k = b0; k < b1; ++k) {
         int2 pf = reinterpret_cast<const int2*>(W.spartner)[k];
         if (pf.x == j && !(W.ftype[pf.y] & kForceRemoved)) return true;

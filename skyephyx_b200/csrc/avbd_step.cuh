@@ -111,7 +111,7 @@ __device__ __noinline__ bool build_incidence(const World& W, const SceneDesc& sc
         if (W.cn[cur][c] > 0) atomicAdd(&W.cntB[W.cpair[cur][c].y], 1);
     __syncthreads();
     for (int b = b0 + tid; b < b1; b += nt) {
-        const int ns = W.sinc_off[b + 1] - W.sinc_off[b];
+        const int ns = W.sinc_n[b];
         W.inc_cnt[b] = ns + W.cntB[b] + owned_live(W, cur, b, sc.cand0);
     }
     __syncthreads();
@@ -123,7 +123,7 @@ __device__ __noinline__ bool build_incidence(const World& W, const SceneDesc& sc
     for (int b = b0 + tid; b < b1; b += nt) {
         const int off = sc.inc0 + W.inc_off[b];
         W.inc_off[b] = off;
-        const int s0 = W.sinc_off[b], nf = W.sinc_nf[b], ns = W.sinc_off[b + 1] - s0;
+        const int s0 = W.sinc_off[b], nf = W.sinc_nf[b], ns = W.sinc_n[b];
         int k = off;
         for (int e = 0; e < nf; ++e) W.inc[k++] = W.sinc[s0 + e];
         k += W.cntB[b];
@@ -145,7 +145,7 @@ __device__ __noinline__ bool build_incidence(const World& W, const SceneDesc& sc
     // then by pair (creation order within a broadphase pass)
     for (int b = b0 + tid; b < b1; b += nt) {
         uint32_t* seg = W.inc + W.inc_off[b] + W.sinc_nf[b];
-        const int n = W.inc_cnt[b] - (W.sinc_off[b + 1] - W.sinc_off[b]);
+        const int n = W.inc_cnt[b] - W.sinc_n[b];
         sort_manifold_entries(W, cur, seg, n);
     }
     if (tid == 0) st->ninc = total;
@@ -485,7 +485,7 @@ __device__ void scene_step(const World& W, int scene) {
                 p.z > kBoundMax) {
                 W.flags[b] = fl | kBodyRemoved;
                 atomicAdd(&st->topo, 1);
-                for (int e = W.sinc_off[b]; e < W.sinc_off[b + 1]; ++e) {
+                for (int e = W.sinc_off[b]; e < W.sinc_off[b] + W.sinc_n[b]; ++e) {
                     const uint32_t ent = W.sinc[e];
                     const uint32_t k = ent_kind(ent), idx = ent_index(ent);
                     if (k == kEntForce) atomicOr(&W.ftype[idx], kForceRemoved);

@@ -267,9 +267,24 @@ class Batch:
         except Exception:
             pass
 
+    def reserve(self, bodies, forces, tets, tris, scenes):
+        """Allocates the device pools (bodies, joints+springs, tets, triangles, scene slots)."""
+        check(self._lib.avbd_batch_reserve(self._h, int(bodies), int(forces), int(tets), int(tris), int(scenes)),
+              "batch_reserve")
+
     def add_scene(self, solver: Solver) -> int:
-        """Copies a staged (never stepped) Solver scene into the batch."""
+        """Copies a staged (never stepped) Solver scene into the batch; returns its scene id."""
         return check(self._lib.avbd_batch_add_scene(self._h, solver.handle), "batch_add_scene")
+
+    def try_add_scene(self, solver: Solver):
+        """Like add_scene, but returns None when the scene does not fit in the free pool space."""
+        r = self._lib.avbd_batch_add_scene(self._h, solver.handle)
+        if r == -3:   # AVBD_ERR_NOMEM
+            return None
+        return check(r, "batch_add_scene")
+
+    def body_offset(self, scene: int) -> int:
+        return check(self._lib.avbd_batch_scene_body_offset(self._h, int(scene)), "scene_body_offset")
 
     def remove_scene(self, scene: int):
         check(self._lib.avbd_batch_remove_scene(self._h, int(scene)), "batch_remove_scene")
