@@ -225,7 +225,11 @@ int32_t avbd_batch_get_launch(const AvbdBatch* b, int32_t* threads_per_cta, int3
  * thread) .. 4 (64, some spilling); trades spills for resident warps. */
 int32_t avbd_batch_set_kernel(AvbdBatch* b, int32_t register_variant);
 /* Lanes that share one body's primal update (1, 2, 4, 8, 16 or 32), for rigid
- * scenes and for FEM scenes; before the first step (autotuner knob). */
+ * scenes and for FEM scenes; before the first step (autotuner knob).
+ * fem_group may also be AVBD_GROUP_FLAT: every (particle, tet) term of a colour
+ * is evaluated by its own lane and each particle then sums its terms in
+ * incidence order (scenes with StVK triangles use 4 lanes instead). */
+#define AVBD_GROUP_FLAT 64
 int32_t avbd_batch_set_groups(AvbdBatch* b, int32_t rigid_group, int32_t fem_group);
 /* Same knob for a single world (0 = by scene kind); before the first step. */
 int32_t avbd_set_group(AvbdWorld* w, int32_t group);

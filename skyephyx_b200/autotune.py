@@ -28,7 +28,7 @@ SPACE = {
     "variant": (1, 2, 3, 4),
     "threads": (64, 128, 256),
     "rigid_group": (1, 2),
-    "fem_group": (2, 4, 8),
+    "fem_group": (2, 4, 8, 64),   # 64: term-per-lane flat sweep
 }
 
 

@@ -108,23 +108,23 @@ void launch_primal(int group, const World& W, int cur, int first, int count, flo
     }
 }
 
-__global__ void k_dual(World W, int cur, int ncand, float alpha) {
+__global__ void k_dual(World W, int cur, int nlive, float alpha, int last) {
     const SceneDesc sc = W.scenes[0];
-    const int n = sc.nforce + ncand;
+    const int n = sc.nforce + nlive;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         if (i < sc.nforce) {
             if (dual_force(W, sc.force0 + i, alpha)) atomicOr(&W.sstate[0].flags, 8);
         } else {
-            dual_manifold(W, cur, sc.cand0 + i - sc.nforce, alpha);
+            dual_manifold(W, cur, W.live[cur][sc.cand0 + i - sc.nforce], alpha, last != 0);
         }
     }
 }
 
-__global__ void k_fracture_reset(World W, int cur, int ncand) {
+__global__ void k_fracture_reset(World W, int cur, int nlive) {
     if (!(W.sstate[0].flags & 8)) return;
     const SceneDesc sc = W.scenes[0];
-    for (int c = sc.cand0 + blockIdx.x * blockDim.x + threadIdx.x; c < sc.cand0 + ncand; c += gridDim.x * blockDim.x)
-        fracture_reset_slot(W, cur, c);
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nlive; i += gridDim.x * blockDim.x)
+        fracture_reset_slot(W, cur, W.live[cur][sc.cand0 + i]);
 }
 
 __global__ void k_fracture_clear(World W) {
@@ -282,7 +282,7 @@ struct Pools {
         A(alloc_c(W.spartner_off, nb)); A(alloc_c(W.spartner_n, nb)); A(alloc_c(W.spartner, 2 * (size_t)nsp));
         A(alloc(W.inc_off, nb)); A(alloc(W.inc_cnt, nb)); A(alloc(W.cntB, nb)); A(alloc(W.bcur, nb));
         A(alloc(W.cand_cnt, nb)); A(alloc(W.cand_off, nb));
-        A(alloc(W.col_list, nb)); A(alloc(W.col_start, (size_t)ns * (kMaxColours + 1)));
+        A(alloc(W.col_list, nb)); A(alloc(W.col_tinc, nb)); A(alloc(W.col_start, (size_t)ns * (kMaxColours + 1)));
         A(alloc(W.ftype, nf)); A(alloc(W.fbody, nf)); A(alloc(W.frA, nf)); A(alloc(W.frB, nf));
         A(alloc(W.fq, nf)); A(alloc(W.fparam, nf)); A(alloc(W.fC0p, nf)); A(alloc(W.fC0a, nf));
         A(alloc(W.fk, 6 * (size_t)nf)); A(alloc(W.ffrac, 6 * (size_t)nf)); A(alloc(W.ffmin, 6 * (size_t)nf));
@@ -300,7 +300,7 @@ struct Pools {
         cudaError_t e = cudaSuccess;
 #define A(expr) if ((e = (expr)) != cudaSuccess) return e
         A(alloc(W.cpair[t], nc)); A(alloc(W.cn[t], nc)); A(alloc(W.cfric[t], nc)); A(alloc(W.kbase[t], nc));
-        A(alloc(W.cbirth[t], nc));
+        A(alloc(W.cbirth[t], nc)); A(alloc(W.live[t], nc));
         A(alloc(W.kid[t], k)); A(alloc(W.krA[t], k)); A(alloc(W.krB[t], k)); A(alloc(W.kn[t], k));
         A(alloc(W.kt1[t], k)); A(alloc(W.kt2[t], k)); A(alloc(W.krAw[t], k)); A(alloc(W.krBw[t], k));
         A(alloc(W.kpen[t], k)); A(alloc(W.klam[t], k));
@@ -331,6 +331,7 @@ struct Pools {
                 if ((e = grow(W.cfric[t], ncand, nc, kc)) != cudaSuccess) return e;
                 if ((e = grow(W.kbase[t], ncand, nc, kc)) != cudaSuccess) return e;
                 if ((e = grow(W.cbirth[t], ncand, nc, kc)) != cudaSuccess) return e;
+                if ((e = grow(W.live[t], ncand, nc, kc)) != cudaSuccess) return e;
             }
             if (k > nk) {
                 if ((e = grow(W.kid[t], nk, k, kk)) != cudaSuccess) return e;
@@ -354,7 +355,9 @@ struct Pools {
 // Lanes per body in the primal sweep: FEM vertices gather about 20 tets each,
 // rigid bodies a handful of manifolds.
 int scene_group(const HostScene& h, int rigid_group, int fem_group) {
-    return (h.ntet() > 0 || h.ntri() > 0) ? fem_group : rigid_group;
+    if (h.ntet() == 0 && h.ntri() == 0) return rigid_group;
+    if (fem_group == kGroupFlat && h.ntri() > 0) return 4;   // the flat sweep takes tet energies only
+    return fem_group;
 }
 
 // Capacity policy of one scene.
@@ -683,6 +686,8 @@ int world_step(AvbdWorld* w) {
         SceneState fix = w->st;
         fix.kused[cur] = 0;
         fix.need_k = 0;
+        fix.nlive[cur] = 0;
+        fix.nmatched = 0;
         cudaMemcpy(P.d_sstate, &fix, sizeof(SceneState), cudaMemcpyHostToDevice);
     }
     if (w->st.need_k) return AVBD_STATUS_CAPACITY;
@@ -701,6 +706,7 @@ int world_step(AvbdWorld* w) {
     if ((r = sync_state(w))) return r;
     if (w->st.status != kStatusOk) return w->st.status == kStatusTimeout ? AVBD_STATUS_TIMEOUT : AVBD_STATUS_CAPACITY;
     const int ncol = w->st.ncolours;
+    const int nlive = w->st.nlive[cur];
     w->ncolours = ncol;
     w->col_start.resize(ncol + 1);
     cudaMemcpyAsync(w->col_start.data(), P.W.col_start, (ncol + 1) * sizeof(int), cudaMemcpyDeviceToHost, s);
@@ -717,9 +723,11 @@ int world_step(AvbdWorld* w) {
             const int n = w->col_start[c + 1] - w->col_start[c];
             if (n > 0) launch_primal(d.group, P.W, cur, w->col_start[c], n, alpha, 0, s);
         }
-        if (d.nforce + ncand > 0) k_dual<<<blocks_for(d.nforce + ncand), kThreads, 0, s>>>(P.W, cur, ncand, alpha);
+        const int last = it == w->params.num_iterations - 1;
+        if (d.nforce + nlive > 0)
+            k_dual<<<blocks_for(d.nforce + nlive), kThreads, 0, s>>>(P.W, cur, nlive, alpha, last);
         if (has_fracture) {
-            k_fracture_reset<<<blocks_for(ncand), kThreads, 0, s>>>(P.W, cur, ncand);
+            k_fracture_reset<<<blocks_for(nlive), kThreads, 0, s>>>(P.W, cur, nlive);
             k_fracture_clear<<<blocks_for(d.nbody), kThreads, 0, s>>>(P.W);
             k_flags_clear<<<1, 32, 0, s>>>(P.W, 8);
         }
@@ -1472,8 +1480,8 @@ int32_t avbd_batch_scene_body_offset(const AvbdBatch* b, int32_t scene) {
 }
 
 // Device bytes per unit of each pool (allocate_all / alloc_tables).
-constexpr int64_t kBytesPerBody = 15 * 16 + 17 * 4;        // float4 state + per-body ints
-constexpr int64_t kBytesPerCand = 2 * (8 + 4 + 4 + 4 + 4);  // two manifold tables
+constexpr int64_t kBytesPerBody = 15 * 16 + 18 * 4;        // float4 state + per-body ints
+constexpr int64_t kBytesPerCand = 2 * (8 + 4 + 4 + 4 + 4 + 4);  // two manifold tables
 constexpr int64_t kBytesPerContact = 2 * (4 + 9 * 16);      // two contact pools
 constexpr int64_t kBytesPerForce = 4 + 8 + 6 * 16 + 6 * 6 * 4;
 constexpr int64_t kBytesPerTet = 16 + 36 + 48 + 16;
@@ -1518,10 +1526,12 @@ int32_t avbd_batch_get_launch(const AvbdBatch* b, int32_t* threads, int32_t* cta
 
 float avbd_batch_last_ms(const AvbdBatch* b) { return b ? b->last_ms : -1.f; }
 
+static_assert(kGroupFlat == AVBD_GROUP_FLAT, "flat sweep selector");
 static bool valid_group(int g) { return g == 1 || g == 2 || g == 4 || g == 8 || g == 16 || g == 32; }
 
 int32_t avbd_batch_set_groups(AvbdBatch* b, int32_t rigid_group, int32_t fem_group) {
-    if (!b || !valid_group(rigid_group) || !valid_group(fem_group)) return AVBD_ERR_INVALID;
+    if (!b || !valid_group(rigid_group) || !(valid_group(fem_group) || fem_group == kGroupFlat))
+        return AVBD_ERR_INVALID;
     if (b->reserved) return AVBD_ERR_STATE;
     b->group_rigid = rigid_group;
     b->group_fem = fem_group;

@@ -15,9 +15,13 @@
 #if defined(__CUDACC__)
 #define AVBD_HD __host__ __device__ __forceinline__
 #define AVBD_D __device__ __forceinline__
+// one compiled body shared by every caller (same instruction selection, so the
+// same rounding, wherever it is called from)
+#define AVBD_HD_OUTLINE static __host__ __device__ __noinline__
 #else
 #define AVBD_HD inline
 #define AVBD_D inline
+#define AVBD_HD_OUTLINE inline
 #endif
 
 #if defined(__CUDA_ARCH__)
@@ -50,6 +54,8 @@ constexpr float kNewContactPenaltyMax = 100000.0f;   // manifold.cpp:186
 
 constexpr int kMaxContacts = 8;       // Manifold::contactPoints[8] (force.hpp:172)
 constexpr int kMaxColours = 1024;     // colour slots per scene
+constexpr int kColourWorkBuckets = 16; // work classes used to order bodies within a colour
+constexpr int kGroupFlat = 64;         // SceneDesc::group of scenes swept term-per-lane (AVBD_GROUP_FLAT)
 
 // body flags
 constexpr int kBodyStatic = 1;
@@ -103,7 +109,7 @@ struct SceneDesc {
     int k0, kcap;            // contact slots (bump-allocated per step)
     int inc0, inccap;        // incidence (CSR) entries
     int ndynamic;
-    int group;               // lanes per body in the primal sweep (1, 2, 4, 8, 16, 32)
+    int group;               // lanes per body in the primal sweep (1, 2, 4, 8, 16, 32) or kGroupFlat
 };
 
 // Per-scene mutable counters (device).
@@ -179,6 +185,7 @@ struct World {
     float* cfric[2];    // friction per slot
     int* kbase[2];      // first contact slot of each candidate slot
     int* cbirth[2];     // step at which the slot's manifold was created (Mesh::forces order)
+    int* live[2];       // live manifold slots of each table, nlive[t] of them from the scene's cand0
     // contact slots: slot * kMaxContacts + k
     uint32_t* kid[2];
     float4* krA[2];     // local rA (xyz), w = penetration
@@ -221,6 +228,7 @@ struct World {
 
     // ---- colouring ----
     int* col_list;      // per scene region [body0, body0+nbody): bodies grouped by colour
+    int* col_tinc;      // flat-sweep scenes: inclusive prefix of tet terms over the scene's col_list
     int* col_start;     // per scene kMaxColours+1 offsets (scene * (kMaxColours+1))
 
     Params P;

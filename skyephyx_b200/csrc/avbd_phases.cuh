@@ -188,7 +188,8 @@ AVBD_HD void narrowphase_slot(const World& W, const SceneDesc& sc, SceneState* s
     const int base = sc.k0 + kofs;
     W.kbase[cur][slot] = base;
     W.cn[cur][slot] = col.n;
-    AVBD_ATOMIC_ADD(&st->nlive[cur], 1);
+    const int li = AVBD_ATOMIC_ADD(&st->nlive[cur], 1);
+    if (li < sc.candcap) W.live[cur][sc.cand0 + li] = slot;
     const float fr = XSQRT(XMUL(W.friction[A], W.friction[B]));
     W.cfric[cur][slot] = fr;
     // previous contacts of the same pair
@@ -641,11 +642,38 @@ AVBD_HD void sys_zero(Sys6& s) {
     }
 }
 
-// Adds the rows of incidence entries first, first + stride, ... of body b
-// (solver.cpp:399-435): forces (manifolds, joints, springs) then energies.
-AVBD_HD void primal_entries(const World& W, int cur, int b, float alpha, bool write_stick, int first, int stride,
-                            Sys6& s) {
-    const int e0 = W.inc_off[b], e1 = e0 + W.inc_cnt[b];
+// Gradient and projected Hessian of tet `idx` for its vertex `role`
+// (NeoHookeanFEM::ComputeEnergyTerms, neohookeanfem.cpp:40-90); false for a
+// removed tet.  Out of line, so every sweep variant gets bitwise the same term.
+AVBD_HD_OUTLINE bool tet_term(const World& W, int idx, int role, V3& g, S3& H) {
+    const int4 v = W.tidx[idx];
+    const float4 tp = W.tparam[idx];
+    if (tp.w != 0.f) return false;   // removed energy
+    const float* gn = W.tgradN + (size_t)idx * 12 + role * 3;
+    neohookean_terms(v3(W.pos[v.x]), v3(W.pos[v.y]), v3(W.pos[v.z]), v3(W.pos[v.w]), W.tDmInv + (size_t)idx * 9,
+                     v3(gn[0], gn[1], gn[2]), tp.x, tp.y, tp.z, W.P.projection_mode, W.P.trust_region_rho, g, H);
+    return true;
+}
+
+// Rounded adds: the term is rounded before it is accumulated, whether it was
+// just computed (inlined) or read back from shared memory, so every sweep
+// variant sums the same values.
+AVBD_HD void sys_add_energy(Sys6& s, float gx, float gy, float gz, float hxx, float hyy, float hzz, float hxy,
+                            float hxz, float hyz) {
+    s.r[0] = XADD(s.r[0], gx); s.r[1] = XADD(s.r[1], gy); s.r[2] = XADD(s.r[2], gz);
+    s.a[0][0] = XADD(s.a[0][0], hxx); s.a[1][1] = XADD(s.a[1][1], hyy); s.a[2][2] = XADD(s.a[2][2], hzz);
+    s.a[1][0] = XADD(s.a[1][0], hxy); s.a[2][0] = XADD(s.a[2][0], hxz); s.a[2][1] = XADD(s.a[2][1], hyz);
+}
+
+AVBD_HD void sys_add_energy(Sys6& s, const V3& g, const S3& H) {
+    sys_add_energy(s, g.x, g.y, g.z, H.xx, H.yy, H.zz, H.xy, H.xz, H.yz);
+}
+
+// Adds the rows of incidence entries e0 + first, e0 + first + stride, ... < e1
+// of body b (solver.cpp:399-435): forces (manifolds, joints, springs) then
+// energies.
+AVBD_HD void primal_entry_range(const World& W, int cur, int b, float alpha, bool write_stick, int e0, int e1,
+                                int first, int stride, Sys6& s) {
     for (int e = e0 + first; e < e1; e += stride) {
         const uint32_t ent = W.inc[e];
         const uint32_t kind = ent_kind(ent), idx = ent_index(ent);
@@ -657,19 +685,9 @@ AVBD_HD void primal_entries(const World& W, int cur, int b, float alpha, bool wr
             if ((t & 15) == kForceJoint) primal_joint(W, (int)idx, b, alpha, s);
             else primal_spring(W, (int)idx, b, s);
         } else if (kind == kEntTet) {
-            const int4 v = W.tidx[idx];
-            const float4 tp = W.tparam[idx];
-            if (tp.w != 0.f) continue;   // removed energy
-            const int role = (int)ent_role(ent);
-            const float* gn = W.tgradN + (size_t)idx * 12 + role * 3;
             V3 g;
             S3 H;
-            neohookean_terms(v3(W.pos[v.x]), v3(W.pos[v.y]), v3(W.pos[v.z]), v3(W.pos[v.w]),
-                             W.tDmInv + (size_t)idx * 9, v3(gn[0], gn[1], gn[2]), tp.x, tp.y, tp.z,
-                             W.P.projection_mode, W.P.trust_region_rho, g, H);
-            s.r[0] += g.x; s.r[1] += g.y; s.r[2] += g.z;
-            s.a[0][0] += H.xx; s.a[1][1] += H.yy; s.a[2][2] += H.zz;
-            s.a[1][0] += H.xy; s.a[2][0] += H.xz; s.a[2][1] += H.yz;
+            if (tet_term(W, (int)idx, (int)ent_role(ent), g, H)) sys_add_energy(s, g, H);
         } else {
             const int4 v = W.ridx[idx];
             const float4 rp = W.rparam[idx];
@@ -680,11 +698,15 @@ AVBD_HD void primal_entries(const World& W, int cur, int b, float alpha, bool wr
             S3 H;
             stvk_terms(v3(W.pos[v.x]), v3(W.pos[v.y]), v3(W.pos[v.z]), W.rDmInv[idx], gn[0], gn[1], rp.x, rp.y,
                        rp.z, W.P.projection_mode, W.P.trust_region_rho, g, H);
-            s.r[0] += g.x; s.r[1] += g.y; s.r[2] += g.z;
-            s.a[0][0] += H.xx; s.a[1][1] += H.yy; s.a[2][2] += H.zz;
-            s.a[1][0] += H.xy; s.a[2][0] += H.xz; s.a[2][1] += H.yz;
+            sys_add_energy(s, g, H);
         }
     }
+}
+
+AVBD_HD void primal_entries(const World& W, int cur, int b, float alpha, bool write_stick, int first, int stride,
+                            Sys6& s) {
+    const int e0 = W.inc_off[b];
+    primal_entry_range(W, cur, b, alpha, write_stick, e0, e0 + W.inc_cnt[b], first, stride, s);
 }
 
 // LDLT solve and pose update (solver.cpp:437-448).
@@ -726,7 +748,9 @@ AVBD_HD bool dual_row(float C, float k, float fmin, float fmax, float frac, floa
     return false;
 }
 
-AVBD_HD void dual_manifold(const World& W, int cur, int slot, float alpha) {
+// write_stick: the last ComputeConstraints call of the step decides the stick
+// flag, so only the final dual sweep needs to store it.
+AVBD_HD void dual_manifold(const World& W, int cur, int slot, float alpha, bool write_stick = true) {
     const int nc = W.cn[cur][slot];
     if (nc == 0) return;
     const int2 ab = W.cpair[cur][slot];
@@ -759,8 +783,10 @@ AVBD_HD void dual_manifold(const World& W, int cur, int slot, float alpha) {
         const float bound = fabsf(lam.x) * fr;
         const float tl = sqrtf(lam.y * lam.y + lam.z * lam.z);
         const float tc = sqrtf(t14.w * t14.w + t24.w * t24.w);
-        rA4.w = (tl < bound && tc < kStickThreshold) ? 1.f : 0.f;
-        W.krAw[cur][o] = rA4;
+        if (write_stick) {
+            rA4.w = (tl < bound && tc < kStickThreshold) ? 1.f : 0.f;
+            W.krAw[cur][o] = rA4;
+        }
         dual_row(C[0], INFINITY, -INFINITY, 0.f, INFINITY, beta, pen.x, lam.x);
         dual_row(C[1], INFINITY, -bound, bound, INFINITY, beta, pen.y, lam.y);
         dual_row(C[2], INFINITY, -bound, bound, INFINITY, beta, pen.z, lam.z);

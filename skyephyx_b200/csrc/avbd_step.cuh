@@ -249,6 +249,95 @@ __device__ __noinline__ void primal_sweep_cta_dispatch(const World& W, int cur, 
     }
 }
 
+// ---------------------------------------------------------------------------
+// Term-per-lane primal sweep of one colour, for scenes whose energies are all
+// tetrahedra.  Up to kFlatSlots (particle, tet) terms of the colour are
+// evaluated at once, one per lane, into shared memory; then one lane per
+// particle adds its inertia, its force and manifold rows and its tet terms in
+// incidence order (the reference's order) and solves.  Lanes stay busy
+// whatever the particles' degrees.  tinc (the scene's col_tinc) holds the
+// inclusive prefix of tet terms over the colour list; the colour occupies
+// list positions [c0, c1).  sm: 10 * kFlatSlots words of shared memory.
+// ---------------------------------------------------------------------------
+constexpr int kFlatSlots = 1024;
+static_assert(10 * kFlatSlots * sizeof(float) <= kStagedBodies * sizeof(float4),
+              "the flat sweep reuses the broadphase's dynamic shared memory");
+
+__device__ __forceinline__ int tet_terms(const World& W, int b) { return W.sinc_n[b] - W.sinc_nf[b]; }
+
+__device__ __noinline__ void primal_sweep_flat(const World& W, int cur, const int* list, const int* tinc, int c0,
+                                               int c1, float alpha, bool write_stick, float* sm) {
+    int* smap = reinterpret_cast<int*>(sm + 9 * kFlatSlots);
+    const int tid = threadIdx.x, nt = blockDim.x;
+    for (int v = c0; v < c1;) {
+        const int base = v == 0 ? 0 : tinc[v - 1];
+        // the longest run of particles [v, vend) whose terms fit the slots (at least one)
+        int lo = v + 1, hi = c1;
+        while (lo < hi) {
+            const int mid = (lo + hi + 1) >> 1;
+            if (tinc[mid - 1] - base <= kFlatSlots) lo = mid;
+            else hi = mid - 1;
+        }
+        const int vend = lo;
+        const int total = tinc[vend - 1] - base;
+        const bool flat = total <= kFlatSlots;
+        if (flat) {
+            for (int j = v + tid; j < vend; j += nt)
+                for (int q = (j == 0 ? 0 : tinc[j - 1]) - base; q < tinc[j] - base; ++q) smap[q] = j;
+            __syncthreads();
+            for (int q = tid; q < total; q += nt) {
+                const int j = smap[q];
+                const int b = list[j];
+                const int k = q - ((j == 0 ? 0 : tinc[j - 1]) - base);
+                const uint32_t ent = W.inc[W.inc_off[b] + W.inc_cnt[b] - tet_terms(W, b) + k];
+                V3 g = v3(0.f, 0.f, 0.f);
+                S3 H;
+                s3_zero(H);
+                if (!(W.flags[b] & kBodyRemoved)) tet_term(W, (int)ent_index(ent), (int)ent_role(ent), g, H);
+                sm[0 * kFlatSlots + q] = g.x; sm[1 * kFlatSlots + q] = g.y; sm[2 * kFlatSlots + q] = g.z;
+                sm[3 * kFlatSlots + q] = H.xx; sm[4 * kFlatSlots + q] = H.yy; sm[5 * kFlatSlots + q] = H.zz;
+                sm[6 * kFlatSlots + q] = H.xy; sm[7 * kFlatSlots + q] = H.xz; sm[8 * kFlatSlots + q] = H.yz;
+            }
+            __syncthreads();
+        }
+        for (int j = v + tid; j < vend; j += nt) {
+            const int b = list[j];
+            if (W.flags[b] & kBodyRemoved) continue;
+            Sys6 s;
+            sys_zero(s);
+            primal_init_mass(W, b, s);
+            const int e0 = W.inc_off[b], e1 = e0 + W.inc_cnt[b];
+            if (!flat) {
+                primal_entry_range(W, cur, b, alpha, write_stick, e0, e1, 0, 1, s);
+            } else {
+                const int nterm = tet_terms(W, b);
+                primal_entry_range(W, cur, b, alpha, write_stick, e0, e1 - nterm, 0, 1, s);
+                const int q0 = (j == 0 ? 0 : tinc[j - 1]) - base;
+                for (int q = q0; q < q0 + nterm; ++q) {
+                    // a removed tet left zeros: adding them changes no value
+                    sys_add_energy(s, sm[0 * kFlatSlots + q], sm[1 * kFlatSlots + q], sm[2 * kFlatSlots + q],
+                                   sm[3 * kFlatSlots + q], sm[4 * kFlatSlots + q], sm[5 * kFlatSlots + q],
+                                   sm[6 * kFlatSlots + q], sm[7 * kFlatSlots + q], sm[8 * kFlatSlots + q]);
+                }
+            }
+            primal_finish(W, b, s);
+        }
+        __syncthreads();
+        v = vend;
+    }
+}
+
+// One colour of a scene's primal sweep, by the scene's lane grouping.
+__device__ __forceinline__ void primal_colour(const World& W, const SceneDesc& sc, int cur, const int* cs, int c,
+                                              float alpha, bool write_stick, float* sm) {
+    if (sc.group == kGroupFlat)
+        primal_sweep_flat(W, cur, W.col_list + sc.body0, W.col_tinc + sc.body0, cs[c], cs[c + 1], alpha, write_stick,
+                          sm);
+    else
+        primal_sweep_cta_dispatch(W, cur, W.col_list + sc.body0 + cs[c], cs[c + 1] - cs[c], alpha, write_stick,
+                                  sc.group);
+}
+
 __device__ __noinline__ bool colour_scene(const World& W, const SceneDesc& sc, SceneState* st, int scene, int cur);
 
 // Keeps the previous step's colouring when the contact graph is unchanged:
@@ -345,11 +434,30 @@ __device__ __noinline__ bool colour_scene(const World& W, const SceneDesc& sc, S
         st->ncolours = ncol;
     }
     __syncthreads();
-    for (int b = b0 + tid; b < b1; b += nt) {
-        const int c = col[b];
-        if (c >= 0) W.col_list[b0 + atomicAdd(&s_count[c], 1)] = b;
+    // Within a colour, bodies are ordered by decreasing work (incidence entries
+    // per lane of a body group), so the bodies sharing a warp take similar
+    // time.  Bodies of one colour share no constraint, so their order within
+    // the colour does not change any result.
+    const int g = (sc.group > 0 && sc.group <= 32) ? sc.group : 1;
+    for (int key = kColourWorkBuckets - 1; key >= 0; --key) {
+        for (int b = b0 + tid; b < b1; b += nt) {
+            const int c = col[b];
+            if (c < 0) continue;
+            const int k = min(kColourWorkBuckets - 1, (W.inc_cnt[b] + g - 1) / g);
+            if (k == key) W.col_list[b0 + atomicAdd(&s_count[c], 1)] = b;
+        }
+        __syncthreads();
     }
-    __syncthreads();
+    if (sc.group == kGroupFlat) {
+        // inclusive prefix of tet terms over the list
+        const int n = cs[ncol];
+        int* tinc = W.col_tinc + b0;
+        for (int i = tid; i < n; i += nt) tinc[i] = tet_terms(W, W.col_list[b0 + i]);
+        __syncthreads();
+        block_exclusive_scan(tinc, tinc, n);
+        for (int i = tid; i < n; i += nt) tinc[i] += tet_terms(W, W.col_list[b0 + i]);
+        __syncthreads();
+    }
     return st->status == kStatusOk;
 }
 
@@ -361,12 +469,14 @@ __device__ __noinline__ void narrowphase_cta(const World& W, const SceneDesc& sc
         narrowphase_slot(W, sc, st, c, cur, old_count);
 }
 
-// Returns true if this thread saw a force fracture.
-__device__ __noinline__ bool dual_cta(const World& W, const SceneDesc& sc, int cur, int ncand) {
+// Returns true if this thread saw a force fracture.  Manifolds come from the
+// step's live list (each manifold's dual is independent of the others).
+__device__ __noinline__ bool dual_cta(const World& W, const SceneDesc& sc, int cur, int nlive, bool last) {
     bool broke = false;
     for (int f = sc.force0 + threadIdx.x; f < sc.force0 + sc.nforce; f += blockDim.x)
         if (dual_force(W, f, W.P.alpha)) broke = true;
-    for (int c = sc.cand0 + threadIdx.x; c < sc.cand0 + ncand; c += blockDim.x) dual_manifold(W, cur, c, W.P.alpha);
+    const int* live = W.live[cur] + sc.cand0;
+    for (int i = threadIdx.x; i < nlive; i += blockDim.x) dual_manifold(W, cur, live[i], W.P.alpha, last);
     return broke;
 }
 
@@ -441,22 +551,23 @@ __device__ void scene_step(const World& W, int scene) {
     __syncthreads();
     AVBD_PHASE(4);
     const int ncol = st->ncolours;
+    const int nlive = st->nlive[cur];
     const int* cs = W.col_start + (size_t)scene * (kMaxColours + 1);
     // 5. iterations
     for (int it = 0; it < W.P.num_iterations; ++it) {
         for (int c = 0; c < ncol; ++c) {
-            primal_sweep_cta_dispatch(W, cur, W.col_list + b0 + cs[c], cs[c + 1] - cs[c], W.P.alpha, false, sc.group);
+            primal_colour(W, sc, cur, cs, c, W.P.alpha, false, reinterpret_cast<float*>(s_bodies));
             __syncthreads();
         }
         AVBD_PHASE(5);
         if (tid == 0) s_flags = 0;
         __syncthreads();
-        if (dual_cta(W, sc, cur, ncand)) s_flags = 1;
+        if (dual_cta(W, sc, cur, nlive, it == W.P.num_iterations - 1)) s_flags = 1;
         __syncthreads();
         const int fractured = s_flags;
         __syncthreads();
         if (fractured) {
-            for (int c = sc.cand0 + tid; c < sc.cand0 + ncand; c += nt) fracture_reset_slot(W, cur, c);
+            for (int i = tid; i < nlive; i += nt) fracture_reset_slot(W, cur, W.live[cur][sc.cand0 + i]);
             __syncthreads();
             for (int b = b0 + tid; b < b1; b += nt) W.reset_flag[b] = 0;
             __syncthreads();
@@ -501,7 +612,7 @@ __device__ void scene_step(const World& W, int scene) {
     // 7. post-stabilisation
     if (W.P.post_stabilization) {
         for (int c = 0; c < ncol; ++c) {
-            primal_sweep_cta_dispatch(W, cur, W.col_list + b0 + cs[c], cs[c + 1] - cs[c], 0.f, true, sc.group);
+            primal_colour(W, sc, cur, cs, c, 0.f, true, reinterpret_cast<float*>(s_bodies));
             __syncthreads();
         }
     }

@@ -16,6 +16,7 @@ import numpy as np
 from ._lib import AvbdError, AvbdParams, AvbdTimings, STATUS, check, default_params, load
 
 INF = float("inf")
+GROUP_FLAT = 64   # AVBD_GROUP_FLAT: one lane per (particle, tet) term in FEM scenes
 
 
 _FLOAT_ARRAYS = {n: C.c_float * n for n in (3, 4, 6)}
@@ -322,7 +323,8 @@ class Batch:
         return pos, quat, vel, omega
 
     def set_groups(self, rigid_group=4, fem_group=8):
-        """Lanes per body in the primal sweep for rigid and FEM scenes (before the first step)."""
+        """Lanes per body in the primal sweep for rigid and FEM scenes (before the
+        first step); fem_group may be GROUP_FLAT (one lane per particle-tet term)."""
         check(self._lib.avbd_batch_set_groups(self._h, int(rigid_group), int(fem_group)), "set_groups")
 
     def set_launch(self, threads_per_cta=0, ctas_per_sm=0):

@@ -72,3 +72,52 @@ def test_batch_matches_oracle(oracle_mod):
         po = o.get_state()[0]
         pb = batch.get_state(i)[0]
         assert np.abs(po - pb).max(initial=0.0) <= 1e-4, f"scene {i}"
+
+
+def fem_on_ground(s):
+    """A free tet block whose bottom particles touch a static ground box
+    (particle-box manifolds beside the tet terms)."""
+    s.add_body(scenes.CUBE, 1.0, 0.5, scenes.v3(0, -0.5, 0), scenes.v3(10, 1, 10), is_static=True)
+    s.make_tet_volume(-0.9, 0.04, -0.45, 7, 3, 4, 0.3, 2e4, 0.3, 1.0, 0.5, False)
+
+
+FEM_BUILDERS = [
+    lambda s: scenes.fem_scene(s, 700, scenes.rng_for(4, 1)),
+    lambda s: scenes.fem_scene(s, 1500, scenes.rng_for(4, 4)),
+    fem_on_ground,
+    scenes.level_soft_beam,
+]
+
+
+def run_groups(builders, fem_group, steps):
+    from skyephyx_b200 import Batch
+    b = Batch()
+    b.set_groups(1, fem_group)
+    keep = [staged(f) for f in builders]
+    for w in keep:
+        b.add_scene(w)
+    assert b.step(steps) == "ok"
+    for i in range(len(builders)):
+        assert b.scene_status(i) == "ok", f"scene {i}"
+    return [b.get_state(i)[:2] for i in range(len(builders))]
+
+
+def test_flat_sweep_equals_one_lane_per_particle():
+    """The term-per-lane sweep sums each particle's terms in incidence order,
+    exactly like one lane per particle: results are bitwise equal."""
+    from skyephyx_b200 import GROUP_FLAT
+    one = run_groups(FEM_BUILDERS, 1, 4)
+    flat = run_groups(FEM_BUILDERS, GROUP_FLAT, 4)
+    for i, ((p1, q1), (pf, qf)) in enumerate(zip(one, flat)):
+        assert np.array_equal(p1.view(np.uint32), pf.view(np.uint32)), f"scene {i}"
+        assert np.array_equal(q1.view(np.uint32), qf.view(np.uint32)), f"scene {i}"
+
+
+def test_flat_sweep_matches_oracle(oracle_mod):
+    from skyephyx_b200 import GROUP_FLAT
+    flat = run_groups(FEM_BUILDERS, GROUP_FLAT, 1)
+    for i, f in enumerate(FEM_BUILDERS):
+        o = oracle_mod.OracleSolver()
+        f(o)
+        assert o.step_coloured() == 0
+        assert np.abs(o.get_state()[0] - flat[i][0]).max(initial=0.0) <= 1e-4, f"scene {i}"
