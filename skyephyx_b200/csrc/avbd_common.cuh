@@ -15,13 +15,9 @@
 #if defined(__CUDACC__)
 #define AVBD_HD __host__ __device__ __forceinline__
 #define AVBD_D __device__ __forceinline__
-// one compiled body shared by every caller (same instruction selection, so the
-// same rounding, wherever it is called from)
-#define AVBD_HD_OUTLINE static __host__ __device__ __noinline__
 #else
 #define AVBD_HD inline
 #define AVBD_D inline
-#define AVBD_HD_OUTLINE inline
 #endif
 
 #if defined(__CUDA_ARCH__)

@@ -359,83 +359,91 @@ AVBD_HD void sys_add_row(Sys6& s, const float J[6], float pen, float f) {
     }
 }
 
-template <int K, int Q>
+// The factorisation runs on the leading N x N block (N = 6, or 3 when rows
+// and columns 3..5 and r[3..5] are exactly zero, as for a particle with only
+// energy terms: the zero rows never win a pivot, every product they enter is
+// an exact zero, and their unknowns come out 0 either way, so N = 3 performs
+// the N = 6 arithmetic on the translational block minus those exact zeros).
+template <int N, int K, int Q>
 AVBD_HD void sym_swap(float (&a)[6][6]) {
 #pragma unroll
-    for (int j = 0; j < 6; ++j) swapf(a[K][j], a[Q][j]);
+    for (int j = 0; j < N; ++j) swapf(a[K][j], a[Q][j]);
 #pragma unroll
-    for (int i = 0; i < 6; ++i) swapf(a[i][K], a[i][Q]);
+    for (int i = 0; i < N; ++i) swapf(a[i][K], a[i][Q]);
 }
 
-template <int K>
+template <int N, int K>
 AVBD_HD void ldlt_pivot(float (&a)[6][6], int p) {
-    if (K < 1 && p == 1) sym_swap<K, 1>(a);
-    if (K < 2 && p == 2) sym_swap<K, 2>(a);
-    if (K < 3 && p == 3) sym_swap<K, 3>(a);
-    if (K < 4 && p == 4) sym_swap<K, 4>(a);
-    if (K < 5 && p == 5) sym_swap<K, 5>(a);
+    if (K < 1 && 1 < N && p == 1) sym_swap<N, K, 1>(a);
+    if (K < 2 && 2 < N && p == 2) sym_swap<N, K, 2>(a);
+    if (K < 3 && 3 < N && p == 3) sym_swap<N, K, 3>(a);
+    if (K < 4 && 4 < N && p == 4) sym_swap<N, K, 4>(a);
+    if (K < 5 && 5 < N && p == 5) sym_swap<N, K, 5>(a);
 }
 
-template <int K>
+template <int N, int K>
 AVBD_HD void ldlt_step(float (&a)[6][6], float (&d)[6], int (&t)[6]) {
     int p = K;
     float best = fabsf(a[K][K]);
 #pragma unroll
-    for (int i = K + 1; i < 6; ++i)
+    for (int i = K + 1; i < N; ++i)
         if (fabsf(a[i][i]) > best) { best = fabsf(a[i][i]); p = i; }
     t[K] = p;
-    ldlt_pivot<K>(a, p);
+    ldlt_pivot<N, K>(a, p);
     const float dk = a[K][K];
     d[K] = dk;
     if (dk != 0.f) {
 #pragma unroll
-        for (int i = K + 1; i < 6; ++i) {
+        for (int i = K + 1; i < N; ++i) {
             const float lik = a[i][K] / dk;
 #pragma unroll
             for (int j = K + 1; j <= i; ++j) a[i][j] = a[i][j] - lik * a[j][K];
         }
 #pragma unroll
-        for (int i = K + 1; i < 6; ++i) a[i][K] = a[i][K] / dk;
+        for (int i = K + 1; i < N; ++i) a[i][K] = a[i][K] / dk;
 #pragma unroll
-        for (int i = K + 1; i < 6; ++i)
+        for (int i = K + 1; i < N; ++i)
 #pragma unroll
-            for (int j = i + 1; j < 6; ++j) a[i][j] = a[j][i];
+            for (int j = i + 1; j < N; ++j) a[i][j] = a[j][i];
     } else {
 #pragma unroll
-        for (int i = K + 1; i < 6; ++i) a[i][K] = 0.f;
+        for (int i = K + 1; i < N; ++i) a[i][K] = 0.f;
     }
 }
 
-template <int K>
+template <int N, int K>
 AVBD_HD void perm_apply(float (&x)[6], int p) {
 #pragma unroll
-    for (int q = K + 1; q < 6; ++q)
+    for (int q = K + 1; q < N; ++q)
         if (p == q) swapf(x[K], x[q]);
 }
 
-AVBD_HD void ldlt_solve6(Sys6& s, float (&x)[6]) {
+template <int N>
+AVBD_HD void ldlt_solve(Sys6& s, float (&x)[6]) {
     float (&a)[6][6] = s.a;
 #pragma unroll
-    for (int i = 0; i < 6; ++i)
+    for (int i = 0; i < N; ++i)
 #pragma unroll
-        for (int j = i + 1; j < 6; ++j) a[i][j] = a[j][i];
+        for (int j = i + 1; j < N; ++j) a[i][j] = a[j][i];
     float d[6];
-    int t[6];
-    ldlt_step<0>(a, d, t);
-    ldlt_step<1>(a, d, t);
-    ldlt_step<2>(a, d, t);
-    ldlt_step<3>(a, d, t);
-    ldlt_step<4>(a, d, t);
-    ldlt_step<5>(a, d, t);
+    int t[6] = {0, 1, 2, 3, 4, 5};
+    ldlt_step<N, 0>(a, d, t);
+    ldlt_step<N, 1>(a, d, t);
+    ldlt_step<N, 2>(a, d, t);
+    if (N > 3) {
+        ldlt_step<N, 3>(a, d, t);
+        ldlt_step<N, 4>(a, d, t);
+        ldlt_step<N, 5>(a, d, t);
+    }
 #pragma unroll
-    for (int i = 0; i < 6; ++i) x[i] = s.r[i];
-    perm_apply<0>(x, t[0]);
-    perm_apply<1>(x, t[1]);
-    perm_apply<2>(x, t[2]);
-    perm_apply<3>(x, t[3]);
-    perm_apply<4>(x, t[4]);
+    for (int i = 0; i < 6; ++i) x[i] = i < N ? s.r[i] : 0.f;
+    perm_apply<N, 0>(x, t[0]);
+    perm_apply<N, 1>(x, t[1]);
+    perm_apply<N, 2>(x, t[2]);
+    perm_apply<N, 3>(x, t[3]);
+    perm_apply<N, 4>(x, t[4]);
 #pragma unroll
-    for (int i = 0; i < 6; ++i) {
+    for (int i = 0; i < N; ++i) {
         float v = x[i];
 #pragma unroll
         for (int j = 0; j < i; ++j) v = v - a[i][j] * x[j];
@@ -443,19 +451,34 @@ AVBD_HD void ldlt_solve6(Sys6& s, float (&x)[6]) {
     }
     const float tiny = 1.17549435e-38f;
 #pragma unroll
-    for (int i = 0; i < 6; ++i) x[i] = (fabsf(d[i]) > tiny) ? x[i] / d[i] : 0.f;
+    for (int i = 0; i < N; ++i) x[i] = (fabsf(d[i]) > tiny) ? x[i] / d[i] : 0.f;
 #pragma unroll
-    for (int i = 5; i >= 0; --i) {
+    for (int i = N - 1; i >= 0; --i) {
         float v = x[i];
 #pragma unroll
-        for (int j = i + 1; j < 6; ++j) v = v - a[j][i] * x[j];
+        for (int j = i + 1; j < N; ++j) v = v - a[j][i] * x[j];
         x[i] = v;
     }
-    perm_apply<4>(x, t[4]);
-    perm_apply<3>(x, t[3]);
-    perm_apply<2>(x, t[2]);
-    perm_apply<1>(x, t[1]);
-    perm_apply<0>(x, t[0]);
+    perm_apply<N, 4>(x, t[4]);
+    perm_apply<N, 3>(x, t[3]);
+    perm_apply<N, 2>(x, t[2]);
+    perm_apply<N, 1>(x, t[1]);
+    perm_apply<N, 0>(x, t[0]);
+}
+
+// True when rows 3..5 of the lower triangle and r[3..5] are all zero.
+AVBD_HD bool sys_rotation_free(const Sys6& s) {
+    bool z = s.r[3] == 0.f && s.r[4] == 0.f && s.r[5] == 0.f;
+#pragma unroll
+    for (int i = 3; i < 6; ++i)
+#pragma unroll
+        for (int j = 0; j <= i; ++j) z = z && s.a[i][j] == 0.f;
+    return z;
+}
+
+AVBD_HD void ldlt_solve6(Sys6& s, float (&x)[6]) {
+    if (sys_rotation_free(s)) ldlt_solve<3>(s, x);
+    else ldlt_solve<6>(s, x);
 }
 
 // ===========================================================================
@@ -644,8 +667,8 @@ AVBD_HD void sys_zero(Sys6& s) {
 
 // Gradient and projected Hessian of tet `idx` for its vertex `role`
 // (NeoHookeanFEM::ComputeEnergyTerms, neohookeanfem.cpp:40-90); false for a
-// removed tet.  Out of line, so every sweep variant gets bitwise the same term.
-AVBD_HD_OUTLINE bool tet_term(const World& W, int idx, int role, V3& g, S3& H) {
+// removed tet.
+AVBD_HD bool tet_term(const World& W, int idx, int role, V3& g, S3& H) {
     const int4 v = W.tidx[idx];
     const float4 tp = W.tparam[idx];
     if (tp.w != 0.f) return false;   // removed energy
@@ -716,8 +739,10 @@ AVBD_HD void primal_finish(const World& W, int b, Sys6& s) {
     const V3 pos = v3(W.pos[b]);
     const Q4 rot = q4(W.rot[b]);
     const V3 npos = pos - v3(x[0], x[1], x[2]);
-    const Q4 dq = quaternion_from_difference(v3(x[3], x[4], x[5]), -1.f);
-    const Q4 nrot = qnormalize(qmul(dq, rot));
+    // a zero rotation step gives dq = (1, 0, 0, 0) and qmul(dq, rot) = rot
+    // exactly (up to the sign of zero components), so it is skipped
+    const bool turn = x[3] != 0.f || x[4] != 0.f || x[5] != 0.f;
+    const Q4 nrot = qnormalize(turn ? qmul(quaternion_from_difference(v3(x[3], x[4], x[5]), -1.f), rot) : rot);
     W.pos[b] = f4(npos);
     W.rot[b] = f4(nrot);
     W.dlin[b] = f4(npos - v3(W.lpos[b]));
