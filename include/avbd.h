@@ -217,12 +217,20 @@ int64_t avbd_scene_footprint_bytes(const AvbdWorld* w);
 /* Per-scene counters after the last step: status, colours, candidate pairs,
  * contact points, incidence entries, steps taken (6 values). */
 int32_t avbd_batch_scene_info(AvbdBatch* b, int32_t scene, int32_t out[6]);
-/* Launch shape of the persistent kernel: threads per CTA (32..256) and CTAs
- * per SM (0 = as many as fit). */
+/* Launch shape of the persistent kernel: threads per CTA (32..1024, 0 = the
+ * most the kernel build serves; clamped to it) and CTAs per SM (0 = as many
+ * as fit). */
 int32_t avbd_batch_set_launch(AvbdBatch* b, int32_t threads_per_cta, int32_t ctas_per_sm);
 int32_t avbd_batch_get_launch(const AvbdBatch* b, int32_t* threads_per_cta, int32_t* ctas_per_sm);
-/* Register budget of the persistent kernel build: 1 (about 156 registers per
- * thread) .. 4 (64, some spilling); trades spills for resident warps. */
+/* Small scenes share a CTA: a scene with at most units_per_lane (bodies +
+ * tets) per lane of half a team is run by half of it while the other half
+ * takes the next scene, down to a warp (or an eighth of a larger CTA).
+ * 0 (the default) keeps one scene per CTA.  Autotuner knob. */
+int32_t avbd_batch_set_team_work(AvbdBatch* b, int32_t units_per_lane);
+/* Build of the persistent kernel: 1..4 serve CTAs of up to 256 threads with
+ * about 156, 128, 80 or 64 registers per thread (spills traded for resident
+ * warps); 5 and 6 serve 512 threads (128 or 64 registers), 7 serves 1024
+ * threads (64 registers), giving each scene more lanes. */
 int32_t avbd_batch_set_kernel(AvbdBatch* b, int32_t register_variant);
 /* Lanes that share one body's primal update (1, 2, 4, 8, 16 or 32), for rigid
  * scenes and for FEM scenes; before the first step (autotuner knob).

@@ -3,9 +3,13 @@
 Knobs (all exact: they change only which lanes do which work, never the
 arithmetic of a scene, so every candidate gives bitwise-identical results
 for a given lanes-per-body choice):
-  * register budget of the kernel build (156, 128, 80 or 64 registers per thread);
+  * kernel build: CTA size bound and register budget (156, 128, 80 or 64
+    registers per thread at 256 threads; 512- and 1024-thread builds);
   * threads per CTA;
-  * lanes sharing one body's primal update, for rigid and for FEM scenes.
+  * lanes sharing one body's primal update, for rigid and for FEM scenes
+    (64: the term-per-lane flat sweep of FEM scenes);
+  * scene work per lane below which a CTA splits into teams running one
+    scene each.
 
 ``tune(staged_solvers)`` times every candidate on the given staged scenes
 (device time of a few steps after a warm-up) and returns the fastest;
@@ -22,13 +26,17 @@ import time
 HERE = os.path.dirname(os.path.abspath(__file__))
 TABLE = os.path.join(HERE, "autotune_table.json")
 
-DEFAULT = {"variant": 1, "threads": 128, "rigid_group": 1, "fem_group": 4}
+DEFAULT = {"variant": 4, "threads": 256, "rigid_group": 1, "fem_group": 64}
+
+# largest CTA each kernel build serves (avbd_batch_set_kernel)
+VARIANT_MAX_THREADS = {1: 256, 2: 256, 3: 256, 4: 256, 5: 512, 6: 512, 7: 1024}
 
 SPACE = {
-    "variant": (1, 2, 3, 4),
-    "threads": (64, 128, 256),
+    "variant": (1, 2, 3, 4, 5, 6, 7),
+    "threads": (128, 256, 512, 1024),
     "rigid_group": (1, 2),
     "fem_group": (2, 4, 8, 64),   # 64: term-per-lane flat sweep
+    "team_work": (0, 2, 4, 8),    # scene work per lane below which CTAs split into teams
 }
 
 
@@ -69,12 +77,16 @@ def apply(batch, cfg: dict) -> None:
     batch.set_groups(cfg["rigid_group"], cfg["fem_group"])
     batch.set_kernel(cfg["variant"])
     batch.set_launch(cfg["threads"], 0)
+    batch.set_team_work(cfg.get("team_work", 0))
 
 
 def candidates(space=SPACE):
+    """Every combination whose CTA size the kernel build serves."""
     keys = list(space)
     for vals in itertools.product(*(space[k] for k in keys)):
-        yield dict(zip(keys, vals))
+        cfg = dict(zip(keys, vals))
+        if cfg["threads"] <= VARIANT_MAX_THREADS.get(cfg["variant"], 256):
+            yield cfg
 
 
 def time_config(staged, cfg, steps=3, warmup=2, iterations=10):
@@ -90,18 +102,38 @@ def time_config(staged, cfg, steps=3, warmup=2, iterations=10):
     return ms
 
 
-def tune(staged, space=SPACE, steps=3, warmup=2, log=None):
-    """Times each candidate; returns (best_cfg, best_ms, results)."""
+def tune(staged, space=SPACE, steps=3, warmup=2, log=None, start=None, rounds=2):
+    """Coordinate descent from `start` (default DEFAULT): each knob in turn
+    takes its fastest value with the others fixed, for up to `rounds` passes
+    or until nothing changes.  Returns (best_cfg, best_ms, results)."""
     results = []
-    best, best_ms = None, float("inf")
     t0 = time.perf_counter()
-    for cfg in candidates(space):
-        ms = time_config(staged, cfg, steps, warmup)
-        results.append((cfg, ms))
-        if log:
-            log(f"{cfg} {ms:.3f} ms/step")
-        if ms < best_ms:
-            best, best_ms = cfg, ms
+    cache = {}
+
+    def measure(cfg):
+        key = tuple(sorted(cfg.items()))
+        if key not in cache:
+            if cfg["threads"] > VARIANT_MAX_THREADS.get(cfg["variant"], 256):
+                cache[key] = float("inf")
+            else:
+                cache[key] = time_config(staged, cfg, steps, warmup)
+                results.append((dict(cfg), cache[key]))
+                if log:
+                    log(f"{cfg} {cache[key]:.3f} ms/step")
+        return cache[key]
+
+    best = dict(start or DEFAULT)
+    best_ms = measure(best)
+    for _ in range(rounds):
+        changed = False
+        for knob, values in space.items():
+            for v in values:
+                cfg = dict(best, **{knob: v})
+                ms = measure(cfg)
+                if ms < best_ms:
+                    best, best_ms, changed = cfg, ms, True
+        if not changed:
+            break
     if log:
         log(f"tuned {len(results)} candidates in {time.perf_counter() - t0:.1f} s: {best} {best_ms:.3f} ms")
     return best, best_ms, results

@@ -32,8 +32,10 @@ __global__ void k_bp_count(World W) {
 }
 
 __global__ void k_scan_cand(World W) {
+    __shared__ TeamShared s_team;
+    const Team T = Team::cta(&s_team, nullptr, 0);
     const SceneDesc sc = W.scenes[0];
-    const int total = block_exclusive_scan(W.cand_cnt + sc.body0, W.cand_off + sc.body0, sc.nbody);
+    const int total = block_exclusive_scan(T, W.cand_cnt + sc.body0, W.cand_off + sc.body0, sc.nbody);
     if (threadIdx.x == 0) W.sstate[0].need_cand = total;
 }
 
@@ -65,13 +67,16 @@ __global__ void k_force_init(World W) {
 }
 
 __global__ void k_incidence_colour(World W, int cur) {
+    __shared__ TeamShared s_team;
+    __shared__ float4 s_count[(kMaxColours + 1 + 3) / 4];   // colour counts
+    const Team T = Team::cta(&s_team, s_count, (kMaxColours + 1 + 3) / 4);
     const SceneDesc sc = W.scenes[0];
     SceneState* st = W.sstate;
-    if (!build_incidence(W, sc, st, cur)) {
+    if (!build_incidence(T, W, sc, st, cur)) {
         if (threadIdx.x == 0) st->status = kStatusCapacity;
         return;
     }
-    colour_scene_cached(W, sc, st, 0, cur);
+    colour_scene_cached(T, W, sc, st, 0, cur);
 }
 
 __global__ void k_predict(World W) {
@@ -195,24 +200,65 @@ __global__ void k_collide(World W, int a, int b, uint32_t* ids, float* data, int
 // Batched path: one persistent kernel per step; each CTA pulls scenes from a
 // size-ordered queue and runs a scene's whole step.
 // ===========================================================================
-// MINB sets the register budget (about 65536 / (256 * MINB) per thread):
-// 1 keeps the step in about 156 registers, 2 in 128, 3 in 80 and 4 in 64 with
-// some spilling, trading spills for resident warps.  The autotuner picks one.
-template <int MINB>
-__global__ void __launch_bounds__(256, MINB) k_batch_step(World W, const int* order, const int* nlive_ptr,
-                                                            int* queue) {
-    __shared__ int s_q;
+// MAXT is the largest CTA the build serves and MINB sets its register budget
+// (about 65536 / (MAXT * MINB) per thread).  The 256-thread builds keep a
+// step in about 156 (MINB 1), 128, 80 or 64 registers; the 512- and
+// 1024-thread builds give a large scene more lanes.  The autotuner picks one.
+//
+// A CTA starts as one team pulling scenes from the queue (largest first).  A
+// scene whose work (bodies + tets) is at most team_work per lane of half the
+// team is run by the lower half while the upper half, now a team of its own,
+// pulls the next scene; teams keep splitting this way down to
+// Team::min_size(), so small scenes run several to a CTA without waiting on
+// each other's barriers.
+__device__ __forceinline__ bool scene_fits_half(const World& W, int scene, int team_size) {
+    if (W.team_work <= 0 || team_size / 2 < Team::min_size()) return false;
+    const SceneDesc& d = W.scenes[scene];
+    return (long long)(d.nbody + d.ntet) <= (long long)W.team_work * (team_size / 2);
+}
+
+template <int MAXT, int MINB>
+__global__ void __launch_bounds__(MAXT, MINB) k_batch_step(World W, const int* order, const int* nlive_ptr,
+                                                             int* queue) {
+    __shared__ TeamShared s_team[kMaxTeams];
+    extern __shared__ float4 s_stage[];
     const int nlive = *nlive_ptr;   // live scenes, read from device memory so the graph stays replayable
+    Team T = Team::cta(s_team, s_stage, W.stage_bodies);
+    int scene = -1;
     for (;;) {
-        if (threadIdx.x == 0) s_q = atomicAdd(queue, 1);
-        __syncthreads();
-        const int q = s_q;
-        __syncthreads();
-        if (q >= nlive) break;
-        scene_step(W, order[q]);
-        __syncthreads();
+        if (scene < 0) {
+            if (T.rank == 0) T.sh->q = atomicAdd(queue, 1);
+            T.sync();
+            const int q = T.sh->q;
+            T.sync();
+            if (q >= nlive) break;
+            scene = order[q];
+        }
+        if (scene_fits_half(W, scene, T.size)) {
+            const bool lower = T.rank < T.size / 2;
+            T = T.half(lower, s_team);
+            if (!lower) scene = -1;
+            continue;
+        }
+        scene_step(W, scene, T);
+        T.sync();
+        scene = -1;
     }
 }
+
+using BatchKernel = void (*)(World, const int*, const int*, int*);
+struct BatchVariant {
+    BatchKernel fn;
+    int max_threads;
+};
+// Index = register variant of avbd_batch_set_kernel.
+const BatchVariant kBatchVariants[] = {
+    {nullptr, 0},
+    {k_batch_step<256, 1>, 256}, {k_batch_step<256, 2>, 256}, {k_batch_step<256, 3>, 256},
+    {k_batch_step<256, 4>, 256}, {k_batch_step<512, 1>, 512}, {k_batch_step<512, 2>, 512},
+    {k_batch_step<1024, 1>, 1024},
+};
+constexpr int kNumBatchVariants = 7;
 
 int blocks_for(int n, int threads = kThreads) {
     int b = (n + threads - 1) / threads;
@@ -288,7 +334,7 @@ struct Pools {
         A(alloc(W.fk, 6 * (size_t)nf)); A(alloc(W.ffrac, 6 * (size_t)nf)); A(alloc(W.ffmin, 6 * (size_t)nf));
         A(alloc(W.ffmax, 6 * (size_t)nf)); A(alloc(W.fpen, 6 * (size_t)nf)); A(alloc(W.flam, 6 * (size_t)nf));
         A(alloc(W.tidx, nt)); A(alloc(W.tDmInv, 9 * (size_t)nt)); A(alloc(W.tgradN, 12 * (size_t)nt));
-        A(alloc(W.tparam, nt));
+        A(alloc(W.tparam, nt)); A(alloc(W.fterm, 4 * (size_t)nt));
         A(alloc(W.ridx, nr)); A(alloc(W.rDmInv, nr)); A(alloc(W.rgradN, 6 * (size_t)nr)); A(alloc(W.rparam, nr));
         A(alloc(W.inc, ninc));
         for (int t = 0; t < 2; ++t) A(alloc_tables(t, ncand, nk));
@@ -797,8 +843,10 @@ struct AvbdBatch {
     cudaGraphExec_t graph = nullptr;
     int threads = 0, ctas_per_sm = 0;   // 0 = automatic
     int group_rigid = 4, group_fem = 8;  // lanes per body in the primal sweep
-    int variant = 1;                     // register budget of the persistent kernel (1..4, see k_batch_step)
+    int variant = 1;                     // build of the persistent kernel (1..7, see kBatchVariants)
     int grid = 0;
+    int stage = 0;   // float4 slots of dynamic shared memory per CTA
+    int team_work = 0;   // bodies + tets per lane below which a CTA team splits (0 = never)
     float last_ms = 0.f;
 };
 
@@ -907,24 +955,19 @@ int batch_pack(AvbdBatch* b) {
 }
 
 int batch_launch_shape(AvbdBatch* b) {
-    int threads = b->threads > 0 ? b->threads : 128;
+    const BatchVariant& kv = kBatchVariants[b->variant];
+    int threads = b->threads > 0 ? std::min(b->threads, kv.max_threads) : kv.max_threads;
     int sms = 148;
     cudaDeviceGetAttribute(&sms, cudaDevAttrMultiProcessorCount, b->device);
     int per_sm = 0;
-    const size_t smem = kStagedBodies * sizeof(float4);
-    cudaFuncSetAttribute(k_batch_step<1>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(k_batch_step<2>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(k_batch_step<3>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    cudaFuncSetAttribute(k_batch_step<4>, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
-    switch (b->variant) {
-        case 4: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_step<4>, threads, smem); break;
-        case 3: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_step<3>, threads, smem); break;
-        case 2: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_step<2>, threads, smem); break;
-        default: cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, k_batch_step<1>, threads, smem); break;
-    }
+    const int stage = std::max(256, kStagedBodies * threads / 256);
+    const size_t smem = stage * sizeof(float4);
+    cudaFuncSetAttribute(kv.fn, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)smem);
+    cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kv.fn, threads, smem);
     if (per_sm < 1) per_sm = 1;
     if (b->ctas_per_sm > 0) per_sm = std::min(per_sm, b->ctas_per_sm);
     b->threads = threads;
+    b->stage = stage;
     b->ctas_per_sm = per_sm;
     b->grid = sms * per_sm;
     return 0;
@@ -935,12 +978,16 @@ int batch_build_graph(AvbdBatch* b) {
     cudaGraph_t g;
     if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return AVBD_ERR_CUDA;
     cudaMemsetAsync(b->d_queue, 0, sizeof(int), b->stream);
-    const size_t smem = kStagedBodies * sizeof(float4);
-    switch (b->variant) {
-        case 4: k_batch_step<4><<<b->grid, b->threads, smem, b->stream>>>(b->P.W, b->d_order, b->d_nlive, b->d_queue); break;
-        case 3: k_batch_step<3><<<b->grid, b->threads, smem, b->stream>>>(b->P.W, b->d_order, b->d_nlive, b->d_queue); break;
-        case 2: k_batch_step<2><<<b->grid, b->threads, smem, b->stream>>>(b->P.W, b->d_order, b->d_nlive, b->d_queue); break;
-        default: k_batch_step<1><<<b->grid, b->threads, smem, b->stream>>>(b->P.W, b->d_order, b->d_nlive, b->d_queue); break;
+    b->P.W.stage_bodies = b->stage;
+    b->P.W.team_work = b->team_work;
+    const size_t smem = (size_t)b->stage * sizeof(float4);
+    {
+        const int* order = b->d_order;
+        const int* nlive = b->d_nlive;
+        int* queue = b->d_queue;
+        void* args[] = {&b->P.W, &order, &nlive, &queue};
+        cudaLaunchKernel((const void*)kBatchVariants[b->variant].fn, dim3(b->grid), dim3(b->threads), args, smem,
+                         b->stream);
     }
     if (cudaStreamEndCapture(b->stream, &g) != cudaSuccess) return AVBD_ERR_CUDA;
     cudaError_t e = cudaGraphInstantiate(&b->graph, g, 0);
@@ -1484,7 +1531,7 @@ constexpr int64_t kBytesPerBody = 15 * 16 + 18 * 4;        // float4 state + per
 constexpr int64_t kBytesPerCand = 2 * (8 + 4 + 4 + 4 + 4 + 4);  // two manifold tables
 constexpr int64_t kBytesPerContact = 2 * (4 + 9 * 16);      // two contact pools
 constexpr int64_t kBytesPerForce = 4 + 8 + 6 * 16 + 6 * 6 * 4;
-constexpr int64_t kBytesPerTet = 16 + 36 + 48 + 16;
+constexpr int64_t kBytesPerTet = 16 + 36 + 48 + 16 + 16;
 constexpr int64_t kBytesPerTri = 16 + 16 + 24 + 16;
 
 int64_t avbd_scene_footprint_bytes(const AvbdWorld* w) {
@@ -1501,7 +1548,7 @@ int64_t avbd_scene_footprint_bytes(const AvbdWorld* w) {
 }
 
 int32_t avbd_batch_set_launch(AvbdBatch* b, int32_t threads, int32_t ctas_per_sm) {
-    if (!b || threads < 0 || ctas_per_sm < 0 || (threads && (threads % 32 || threads > 256))) return AVBD_ERR_INVALID;
+    if (!b || threads < 0 || ctas_per_sm < 0 || (threads && (threads % 32 || threads > 1024))) return AVBD_ERR_INVALID;
     b->threads = threads;
     b->ctas_per_sm = ctas_per_sm;
     b->grid = 0;
@@ -1510,9 +1557,16 @@ int32_t avbd_batch_set_launch(AvbdBatch* b, int32_t threads, int32_t ctas_per_sm
 }
 
 int32_t avbd_batch_set_kernel(AvbdBatch* b, int32_t register_variant) {
-    if (!b || register_variant < 1 || register_variant > 4) return AVBD_ERR_INVALID;
+    if (!b || register_variant < 1 || register_variant > kNumBatchVariants) return AVBD_ERR_INVALID;
     b->variant = register_variant;
     b->grid = 0;
+    batch_drop_graph(b);
+    return 0;
+}
+
+int32_t avbd_batch_set_team_work(AvbdBatch* b, int32_t units_per_lane) {
+    if (!b || units_per_lane < 0) return AVBD_ERR_INVALID;
+    b->team_work = units_per_lane;
     batch_drop_graph(b);
     return 0;
 }

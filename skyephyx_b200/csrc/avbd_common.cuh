@@ -132,6 +132,8 @@ struct SceneState {
 // Structure-of-arrays device world.  One instance is passed by value to kernels.
 struct World {
     int nscenes;
+    int stage_bodies;   // batched kernel: float4 slots of dynamic shared memory per CTA
+    int team_work;      // batched kernel: bodies + tets per lane below which a team splits (0 = never)
     const SceneDesc* scenes;
     SceneState* sstate;
 
@@ -225,6 +227,7 @@ struct World {
     // ---- colouring ----
     int* col_list;      // per scene region [body0, body0+nbody): bodies grouped by colour
     int* col_tinc;      // flat-sweep scenes: inclusive prefix of tet terms over the scene's col_list
+    uint32_t* fterm;    // flat-sweep scenes: tet-term entries in colour-list order, 4 slots per tet from 4 * tet0
     int* col_start;     // per scene kMaxColours+1 offsets (scene * (kMaxColours+1))
 
     Params P;
@@ -369,6 +372,17 @@ AVBD_HD V3 quaternion_to_rotvec(Q4 q) {
 }
 
 AVBD_HD float clampf(float v, float lo, float hi) { return v < lo ? lo : (hi < v ? hi : v); }
+
+// Fast reciprocal and reciprocal square root (a couple of ulp on the device,
+// where they replace IEEE divide / square-root sequences on latency-critical
+// chains; plain on the host).
+#if defined(__CUDA_ARCH__)
+AVBD_HD float fast_rcp(float x) { return __fdividef(1.f, x); }
+AVBD_HD float fast_rsqrt(float x) { return rsqrtf(x); }
+#else
+AVBD_HD float fast_rcp(float x) { return 1.f / x; }
+AVBD_HD float fast_rsqrt(float x) { return 1.f / sqrtf(x); }
+#endif
 
 AVBD_HD uint32_t colour_priority(uint32_t x) {
     // integer mixer (Wellons "lowbias32"); the CPU colouring twin uses the same function

@@ -21,9 +21,12 @@ AVBD_HD float det3(const M3& m) {
 }
 
 AVBD_HD void jacobi_cs(float app, float aqq, float apq, float& c, float& s) {
-    float tau = (aqq - app) / (2.f * apq);
-    float t = (tau >= 0.f ? 1.f : -1.f) / (fabsf(tau) + sqrtf(1.f + tau * tau));
-    c = 1.f / sqrtf(1.f + t * t);
+    const float tau = (aqq - app) * fast_rcp(2.f * apq);
+    const float at = fabsf(tau);
+    const float r = 1.f + tau * tau;
+    const float root = r < 1e30f ? r * fast_rsqrt(r) : at;   // sqrt(1 + tau^2), no overflow
+    const float t = (tau >= 0.f ? 1.f : -1.f) * fast_rcp(at + root);
+    c = fast_rsqrt(1.f + t * t);
     s = t * c;
 }
 
@@ -42,13 +45,13 @@ AVBD_HD void swapf(float& a, float& b) { float t = a; a = b; b = t; }
 AVBD_HD void svd3(const M3& F, M3& U, V3& S, M3& V) {
     V3 a0 = F.c[0], a1 = F.c[1], a2 = F.c[2];
     V3 v0 = v3(1, 0, 0), v1 = v3(0, 1, 0), v2 = v3(0, 0, 1);
-    const float eps = 1.1920929e-07f;
+    const float eps2 = 1.1920929e-07f * 1.1920929e-07f;   // |a_p . a_q| <= eps |a_p| |a_q|, squared
     for (int sweep = 0; sweep < 64; ++sweep) {
         bool rotated = false;
 #define AVBD_SVD_PAIR(ap, aq, vp, vq)                                           \
         {                                                                       \
             float al = sqnorm(ap), be = sqnorm(aq), ga = dot(ap, aq);           \
-            if (!(ga == 0.f || fabsf(ga) <= eps * sqrtf(al * be))) {            \
+            if (!(ga == 0.f || ga * ga <= eps2 * (al * be))) {                  \
                 float c, s;                                                     \
                 jacobi_cs(al, be, ga, c, s);                                    \
                 rot_cols(ap, aq, c, s);                                         \
@@ -68,9 +71,9 @@ AVBD_HD void svd3(const M3& F, M3& U, V3& S, M3& V) {
     if (s1 < s2) { swapf(s1, s2); swap3(a1, a2); swap3(v1, v2); }
     if (s0 < s1) { swapf(s0, s1); swap3(a0, a1); swap3(v0, v1); }
     const float tiny = 1.17549435e-38f;
-    V3 u0 = s0 > tiny ? a0 / s0 : v3(1, 0, 0);
-    V3 u1 = s1 > tiny ? a1 / s1 : v3(0, 1, 0);
-    V3 u2 = s2 > tiny ? a2 / s2 : cross(u0, u1);
+    V3 u0 = s0 > tiny ? a0 * fast_rcp(s0) : v3(1, 0, 0);
+    V3 u1 = s1 > tiny ? a1 * fast_rcp(s1) : v3(0, 1, 0);
+    V3 u2 = s2 > tiny ? a2 * fast_rcp(s2) : cross(u0, u1);
     U.c[0] = u0; U.c[1] = u1; U.c[2] = u2;
     V.c[0] = v0; V.c[1] = v1; V.c[2] = v2;
     S = v3(s0, s1, s2);

@@ -364,32 +364,32 @@ AVBD_HD void sys_add_row(Sys6& s, const float J[6], float pen, float f) {
 // energy terms: the zero rows never win a pivot, every product they enter is
 // an exact zero, and their unknowns come out 0 either way, so N = 3 performs
 // the N = 6 arithmetic on the translational block minus those exact zeros).
-template <int N, int K, int Q>
-AVBD_HD void sym_swap(float (&a)[6][6]) {
+template <int M, int N, int K, int Q>
+AVBD_HD void sym_swap(float (&a)[M][M]) {
 #pragma unroll
     for (int j = 0; j < N; ++j) swapf(a[K][j], a[Q][j]);
 #pragma unroll
     for (int i = 0; i < N; ++i) swapf(a[i][K], a[i][Q]);
 }
 
-template <int N, int K>
-AVBD_HD void ldlt_pivot(float (&a)[6][6], int p) {
-    if (K < 1 && 1 < N && p == 1) sym_swap<N, K, 1>(a);
-    if (K < 2 && 2 < N && p == 2) sym_swap<N, K, 2>(a);
-    if (K < 3 && 3 < N && p == 3) sym_swap<N, K, 3>(a);
-    if (K < 4 && 4 < N && p == 4) sym_swap<N, K, 4>(a);
-    if (K < 5 && 5 < N && p == 5) sym_swap<N, K, 5>(a);
+template <int M, int N, int K>
+AVBD_HD void ldlt_pivot(float (&a)[M][M], int p) {
+    if (K < 1 && 1 < N && p == 1) sym_swap<M, N, K, (1 < N ? 1 : 0)>(a);
+    if (K < 2 && 2 < N && p == 2) sym_swap<M, N, K, (2 < N ? 2 : 0)>(a);
+    if (K < 3 && 3 < N && p == 3) sym_swap<M, N, K, (3 < N ? 3 : 0)>(a);
+    if (K < 4 && 4 < N && p == 4) sym_swap<M, N, K, (4 < N ? 4 : 0)>(a);
+    if (K < 5 && 5 < N && p == 5) sym_swap<M, N, K, (5 < N ? 5 : 0)>(a);
 }
 
-template <int N, int K>
-AVBD_HD void ldlt_step(float (&a)[6][6], float (&d)[6], int (&t)[6]) {
+template <int M, int N, int K>
+AVBD_HD void ldlt_step(float (&a)[M][M], float (&d)[M], int (&t)[M]) {
     int p = K;
     float best = fabsf(a[K][K]);
 #pragma unroll
     for (int i = K + 1; i < N; ++i)
         if (fabsf(a[i][i]) > best) { best = fabsf(a[i][i]); p = i; }
     t[K] = p;
-    ldlt_pivot<N, K>(a, p);
+    ldlt_pivot<M, N, K>(a, p);
     const float dk = a[K][K];
     d[K] = dk;
     if (dk != 0.f) {
@@ -411,37 +411,33 @@ AVBD_HD void ldlt_step(float (&a)[6][6], float (&d)[6], int (&t)[6]) {
     }
 }
 
-template <int N, int K>
-AVBD_HD void perm_apply(float (&x)[6], int p) {
-#pragma unroll
-    for (int q = K + 1; q < N; ++q)
-        if (p == q) swapf(x[K], x[q]);
-}
-
-template <int N>
-AVBD_HD void ldlt_solve(Sys6& s, float (&x)[6]) {
-    float (&a)[6][6] = s.a;
+// Solves the leading N x N block of a (lower triangle given) for r; x[N..M) = 0.
+template <int M, int N>
+AVBD_HD void ldlt_solve(float (&a)[M][M], const float (&r)[M], float (&x)[M]) {
 #pragma unroll
     for (int i = 0; i < N; ++i)
 #pragma unroll
         for (int j = i + 1; j < N; ++j) a[i][j] = a[j][i];
-    float d[6];
-    int t[6] = {0, 1, 2, 3, 4, 5};
-    ldlt_step<N, 0>(a, d, t);
-    ldlt_step<N, 1>(a, d, t);
-    ldlt_step<N, 2>(a, d, t);
-    if (N > 3) {
-        ldlt_step<N, 3>(a, d, t);
-        ldlt_step<N, 4>(a, d, t);
-        ldlt_step<N, 5>(a, d, t);
+    float d[M];
+    int t[M];
+#pragma unroll
+    for (int i = 0; i < M; ++i) t[i] = i;
+    ldlt_step<M, N, 0>(a, d, t);
+    ldlt_step<M, N, 1>(a, d, t);
+    ldlt_step<M, N, 2>(a, d, t);
+    if constexpr (N > 3) {
+        ldlt_step<M, N, 3>(a, d, t);
+        ldlt_step<M, N, 4>(a, d, t);
+        ldlt_step<M, N, 5>(a, d, t);
     }
 #pragma unroll
-    for (int i = 0; i < 6; ++i) x[i] = i < N ? s.r[i] : 0.f;
-    perm_apply<N, 0>(x, t[0]);
-    perm_apply<N, 1>(x, t[1]);
-    perm_apply<N, 2>(x, t[2]);
-    perm_apply<N, 3>(x, t[3]);
-    perm_apply<N, 4>(x, t[4]);
+    for (int i = 0; i < M; ++i) x[i] = i < N ? r[i] : 0.f;
+#pragma unroll
+    for (int k = 0; k + 1 < N; ++k) {
+#pragma unroll
+        for (int q = k + 1; q < N; ++q)
+            if (t[k] == q) swapf(x[k], x[q]);
+    }
 #pragma unroll
     for (int i = 0; i < N; ++i) {
         float v = x[i];
@@ -459,11 +455,67 @@ AVBD_HD void ldlt_solve(Sys6& s, float (&x)[6]) {
         for (int j = i + 1; j < N; ++j) v = v - a[j][i] * x[j];
         x[i] = v;
     }
-    perm_apply<N, 4>(x, t[4]);
-    perm_apply<N, 3>(x, t[3]);
-    perm_apply<N, 2>(x, t[2]);
-    perm_apply<N, 1>(x, t[1]);
-    perm_apply<N, 0>(x, t[0]);
+#pragma unroll
+    for (int k = N - 2; k >= 0; --k) {
+#pragma unroll
+        for (int q = k + 1; q < N; ++q)
+            if (t[k] == q) swapf(x[k], x[q]);
+    }
+}
+
+// LDL^T of the leading N x N block without pivoting, one reciprocal per
+// pivot.  The primal systems are symmetric positive definite whenever every
+// diagonal block carries mass (inertial term plus positive semidefinite force
+// and energy rows), and for those pivoting only changes rounding; the pivot
+// search and the symmetric swaps are most of the pivoted solver's latency.
+// Returns false, leaving x untouched, when a pivot is not clearly positive
+// (e.g. a rotational block made of contact rows alone): the caller then uses
+// the pivoted solver, which handles semidefinite systems.
+template <int M, int N>
+AVBD_HD bool ldlt_solve_spd(const float (&a)[M][M], const float (&r)[M], float (&x)[M]) {
+    float l[N][N];
+#pragma unroll
+    for (int i = 0; i < N; ++i)
+#pragma unroll
+        for (int j = 0; j <= i; ++j) l[i][j] = a[i][j];
+    float dinv[N];
+    bool ok = true;
+#pragma unroll
+    for (int k = 0; k < N; ++k) {
+        const float dk = l[k][k];
+        ok = ok && dk > 1e-6f * a[k][k];   // false for NaN too
+        const float inv = fast_rcp(dk);
+        dinv[k] = inv;
+#pragma unroll
+        for (int i = k + 1; i < N; ++i) {
+            const float lik = l[i][k] * inv;
+#pragma unroll
+            for (int j = k + 1; j <= i; ++j) l[i][j] = l[i][j] - lik * l[j][k];
+        }
+#pragma unroll
+        for (int i = k + 1; i < N; ++i) l[i][k] = l[i][k] * inv;
+    }
+    if (!ok) return false;
+    float y[N];
+#pragma unroll
+    for (int i = 0; i < N; ++i) {
+        float v = r[i];
+#pragma unroll
+        for (int j = 0; j < i; ++j) v = v - l[i][j] * y[j];
+        y[i] = v;
+    }
+#pragma unroll
+    for (int i = 0; i < N; ++i) y[i] = y[i] * dinv[i];
+#pragma unroll
+    for (int i = N - 1; i >= 0; --i) {
+        float v = y[i];
+#pragma unroll
+        for (int j = i + 1; j < N; ++j) v = v - l[j][i] * y[j];
+        y[i] = v;
+    }
+#pragma unroll
+    for (int i = 0; i < M; ++i) x[i] = i < N ? y[i] : 0.f;
+    return true;
 }
 
 // True when rows 3..5 of the lower triangle and r[3..5] are all zero.
@@ -477,8 +529,11 @@ AVBD_HD bool sys_rotation_free(const Sys6& s) {
 }
 
 AVBD_HD void ldlt_solve6(Sys6& s, float (&x)[6]) {
-    if (sys_rotation_free(s)) ldlt_solve<3>(s, x);
-    else ldlt_solve<6>(s, x);
+    if (sys_rotation_free(s)) {
+        if (!ldlt_solve_spd<6, 3>(s.a, s.r, x)) ldlt_solve<6, 3>(s.a, s.r, x);
+    } else {
+        if (!ldlt_solve_spd<6, 6>(s.a, s.r, x)) ldlt_solve<6, 6>(s.a, s.r, x);
+    }
 }
 
 // ===========================================================================
@@ -733,9 +788,7 @@ AVBD_HD void primal_entries(const World& W, int cur, int b, float alpha, bool wr
 }
 
 // LDLT solve and pose update (solver.cpp:437-448).
-AVBD_HD void primal_finish(const World& W, int b, Sys6& s) {
-    float x[6];
-    ldlt_solve6(s, x);
+AVBD_HD void primal_apply(const World& W, int b, const float (&x)[6]) {
     const V3 pos = v3(W.pos[b]);
     const Q4 rot = q4(W.rot[b]);
     const V3 npos = pos - v3(x[0], x[1], x[2]);
@@ -747,6 +800,52 @@ AVBD_HD void primal_finish(const World& W, int b, Sys6& s) {
     W.rot[b] = f4(nrot);
     W.dlin[b] = f4(npos - v3(W.lpos[b]));
     W.dang[b] = f4(rotation_difference(nrot, q4(W.lrot[b])));
+}
+
+AVBD_HD void primal_finish(const World& W, int b, Sys6& s) {
+    float x[6];
+    ldlt_solve6(s, x);
+    primal_apply(W, b, x);
+}
+
+// A particle whose incidence holds only energy terms has exactly zero
+// rotational rows (no inertia, no force rows): its translational 3x3 system
+// alone performs the same arithmetic as primal_init_mass + ldlt_solve<6, 3>.
+struct Sys3 {
+    float a[3][3];
+    float r[3];
+};
+
+AVBD_HD bool energy_only_particle(const World& W, int b) {
+    if (!(W.flags[b] & kBodyParticle)) return false;
+    const float4 M0 = W.Mw0[b], M1 = W.Mw1[b];
+    return M0.y == 0.f && M0.z == 0.f && M0.w == 0.f && M1.x == 0.f && M1.y == 0.f && M1.z == 0.f;
+}
+
+AVBD_HD void particle_init_mass(const World& W, int b, Sys3& s) {
+    const float dt = W.P.dt;
+    const float dt2 = dt * dt;
+    const float m = W.Mw0[b].x / dt2;
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) s.a[i][j] = i == j ? m : 0.f;
+    const V3 dl = v3(W.pos[b]) - v3(W.ipos[b]);
+    s.r[0] = m * dl.x; s.r[1] = m * dl.y; s.r[2] = m * dl.z;
+}
+
+AVBD_HD void particle_add_energy(Sys3& s, float gx, float gy, float gz, float hxx, float hyy, float hzz, float hxy,
+                                 float hxz, float hyz) {
+    s.r[0] = XADD(s.r[0], gx); s.r[1] = XADD(s.r[1], gy); s.r[2] = XADD(s.r[2], gz);
+    s.a[0][0] = XADD(s.a[0][0], hxx); s.a[1][1] = XADD(s.a[1][1], hyy); s.a[2][2] = XADD(s.a[2][2], hzz);
+    s.a[1][0] = XADD(s.a[1][0], hxy); s.a[2][0] = XADD(s.a[2][0], hxz); s.a[2][1] = XADD(s.a[2][1], hyz);
+}
+
+AVBD_HD void particle_finish(const World& W, int b, Sys3& s) {
+    float x3[3];
+    if (!ldlt_solve_spd<3, 3>(s.a, s.r, x3)) ldlt_solve<3, 3>(s.a, s.r, x3);
+    const float x[6] = {x3[0], x3[1], x3[2], 0.f, 0.f, 0.f};
+    primal_apply(W, b, x);
 }
 
 // One body by one thread, in the reference's summation order.

@@ -12,14 +12,15 @@
 __device__ unsigned long long g_phase_cycles[2 * 16];
 __device__ unsigned long long g_scene_cycles[1 << 16];
 #define AVBD_PHASE_BEGIN(kind) long long _avbd_t0 = clock64(), _avbd_s0 = _avbd_t0; const int _avbd_kind = (kind);
+// (team time is counted in 256-thread CTA equivalents: cycles x team size / 256)
 #define AVBD_PHASE(k)                                                                               \
-    if (threadIdx.x == 0) {                                                                         \
+    if (T.rank == 0) {                                                                              \
         long long _t = clock64();                                                                   \
-        atomicAdd(&g_phase_cycles[_avbd_kind * 16 + (k)], (unsigned long long)(_t - _avbd_t0));     \
+        atomicAdd(&g_phase_cycles[_avbd_kind * 16 + (k)], (unsigned long long)((_t - _avbd_t0) * T.size / 256)); \
         _avbd_t0 = _t;                                                                              \
     }
 #define AVBD_PHASE_END(scene) \
-    if (threadIdx.x == 0 && (scene) < (1 << 16)) g_scene_cycles[(scene)] = (unsigned long long)(clock64() - _avbd_s0);
+    if (T.rank == 0 && (scene) < (1 << 16)) g_scene_cycles[(scene)] = (unsigned long long)((clock64() - _avbd_s0) * T.size / 256);
 #else
 #define AVBD_PHASE_BEGIN(kind)
 #define AVBD_PHASE(k)
@@ -29,18 +30,71 @@ __device__ unsigned long long g_scene_cycles[1 << 16];
 namespace avbd {
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kStagedBodies = 2560;   // bodies whose pose fits the broadphase's shared-memory stage (40 KB)
+constexpr int kStagedBodies = 2560;   // stage of a 256-thread CTA (40 KB); smaller CTAs get proportionally less
+constexpr int kMaxTeams = 8;          // teams a CTA may split into
 
-// Exclusive scan of in[0, n) into out[0, n) by one CTA; returns the total.
+// Scalars a team shares through shared memory.
+struct TeamShared {
+    int q, flags, remaining, progress, maxc, carry;
+    int warp_tot[32];
+};
+
+// Consecutive whole warps of a CTA that run one scene together: the whole CTA
+// (barrier 0, i.e. __syncthreads) or a power-of-two part of it with its own
+// named barrier (a single warp uses __syncwarp).  Teams only split, so the
+// teams alive at one time partition the CTA's warps; a team's barrier id and
+// shared slot follow from its first warp, which no other live team shares.
+struct Team {
+    int rank;          // thread index within the team
+    int size;          // threads (a multiple of 32)
+    int first_warp;    // first warp of the team within the CTA
+    int bar;           // named barrier id (0 for the whole CTA)
+    TeamShared* sh;    // the team's shared scalars
+    float4* stage;     // the team's slice of the dynamic shared memory
+    int stage_cap;     // float4 slots in that slice
+
+    __device__ __forceinline__ void sync() const {
+        if (bar == 0) __syncthreads();
+        else if (size == 32) __syncwarp();
+        else asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(size) : "memory");
+    }
+    // Smallest team a CTA splits into: a warp, or an eighth of a larger CTA.
+    __device__ __forceinline__ static int min_size() { return max(32, (int)(blockDim.x / kMaxTeams)); }
+    __device__ __forceinline__ static Team cta(TeamShared* shared, float4* stage, int stage_cap) {
+        Team t;
+        t.rank = threadIdx.x;
+        t.size = blockDim.x;
+        t.first_warp = 0;
+        t.bar = 0;
+        t.sh = shared;
+        t.stage = stage;
+        t.stage_cap = stage_cap;
+        return t;
+    }
+    // The lower or upper half of this team, as a team of its own.
+    __device__ __forceinline__ Team half(bool lower, TeamShared* shared) const {
+        Team t;
+        const int h = size / 2;
+        t.size = h;
+        t.rank = lower ? rank : rank - h;
+        t.first_warp = first_warp + (lower ? 0 : h / 32);
+        const int slot = t.first_warp / (min_size() / 32);
+        t.bar = h == 32 ? -1 : 1 + slot;
+        t.sh = shared + slot;
+        t.stage_cap = stage_cap / 2;
+        t.stage = stage + (lower ? 0 : t.stage_cap);
+        return t;
+    }
+};
+
+// Exclusive scan of in[0, n) into out[0, n) by one team; returns the total.
 // in and out may alias.
-__device__ int block_exclusive_scan(const int* in, int* out, int n) {
-    __shared__ int warp_tot[32];
-    __shared__ int carry;
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = (blockDim.x + 31) >> 5;
-    if (threadIdx.x == 0) carry = 0;
-    __syncthreads();
-    for (int base = 0; base < n; base += blockDim.x) {
-        const int i = base + threadIdx.x;
+__device__ int block_exclusive_scan(const Team& T, const int* in, int* out, int n) {
+    const int lane = T.rank & 31, warp = T.rank >> 5, nwarps = T.size >> 5;
+    if (T.rank == 0) T.sh->carry = 0;
+    T.sync();
+    for (int base = 0; base < n; base += T.size) {
+        const int i = base + T.rank;
         const int v = i < n ? in[i] : 0;
         int x = v;
 #pragma unroll
@@ -48,26 +102,26 @@ __device__ int block_exclusive_scan(const int* in, int* out, int n) {
             int y = __shfl_up_sync(kFull, x, o);
             if (lane >= o) x += y;
         }
-        if (lane == 31) warp_tot[warp] = x;
-        __syncthreads();
+        if (lane == 31) T.sh->warp_tot[warp] = x;
+        T.sync();
         if (warp == 0) {
-            int w = lane < nwarps ? warp_tot[lane] : 0;
+            int w = lane < nwarps ? T.sh->warp_tot[lane] : 0;
 #pragma unroll
             for (int o = 1; o < 32; o <<= 1) {
                 int y = __shfl_up_sync(kFull, w, o);
                 if (lane >= o) w += y;
             }
-            warp_tot[lane] = w;
+            T.sh->warp_tot[lane] = w;
         }
-        __syncthreads();
-        const int prefix = carry + (warp > 0 ? warp_tot[warp - 1] : 0);
+        T.sync();
+        const int prefix = T.sh->carry + (warp > 0 ? T.sh->warp_tot[warp - 1] : 0);
         if (i < n) out[i] = prefix + x - v;
-        __syncthreads();
-        if (threadIdx.x == blockDim.x - 1) carry = prefix + x;
-        __syncthreads();
+        T.sync();
+        if (T.rank == T.size - 1) T.sh->carry = prefix + x;
+        T.sync();
     }
-    const int total = carry;
-    __syncthreads();
+    const int total = T.sh->carry;
+    T.sync();
     return total;
 }
 
@@ -101,21 +155,22 @@ __device__ __forceinline__ void sort_manifold_entries(const World& W, int cur, u
 }
 
 // Returns false (and sets need_inc) when the scene's incidence region is too small.
-__device__ __noinline__ bool build_incidence(const World& W, const SceneDesc& sc, SceneState* st, int cur) {
-    const int tid = threadIdx.x, nt = blockDim.x;
+__device__ __noinline__ bool build_incidence(const Team& T, const World& W, const SceneDesc& sc, SceneState* st,
+                                             int cur) {
+    const int tid = T.rank, nt = T.size;
     const int b0 = sc.body0, b1 = sc.body0 + sc.nbody;
     const int ncand = st->ncand[cur];
     for (int b = b0 + tid; b < b1; b += nt) W.cntB[b] = 0;
-    __syncthreads();
+    T.sync();
     for (int c = sc.cand0 + tid; c < sc.cand0 + ncand; c += nt)
         if (W.cn[cur][c] > 0) atomicAdd(&W.cntB[W.cpair[cur][c].y], 1);
-    __syncthreads();
+    T.sync();
     for (int b = b0 + tid; b < b1; b += nt) {
         const int ns = W.sinc_n[b];
         W.inc_cnt[b] = ns + W.cntB[b] + owned_live(W, cur, b, sc.cand0);
     }
-    __syncthreads();
-    const int total = block_exclusive_scan(W.inc_cnt + b0, W.inc_off + b0, sc.nbody);
+    T.sync();
+    const int total = block_exclusive_scan(T, W.inc_cnt + b0, W.inc_off + b0, sc.nbody);
     if (total > sc.inccap) {
         if (tid == 0) { st->need_inc = total; }
         return false;
@@ -133,14 +188,14 @@ __device__ __noinline__ bool build_incidence(const World& W, const SceneDesc& sc
         for (int e = nf; e < ns; ++e) W.inc[k++] = W.sinc[s0 + e];
         W.bcur[b] = 0;
     }
-    __syncthreads();
+    T.sync();
     for (int c = sc.cand0 + tid; c < sc.cand0 + ncand; c += nt) {
         if (W.cn[cur][c] == 0) continue;
         const int B = W.cpair[cur][c].y;
         const int p = atomicAdd(&W.bcur[B], 1);
         W.inc[W.inc_off[B] + W.sinc_nf[B] + p] = ent_make(kEntManifold, 1, (uint32_t)c);
     }
-    __syncthreads();
+    T.sync();
     // order each body's manifolds as Mesh::forces holds them: by creation step,
     // then by pair (creation order within a broadphase pass)
     for (int b = b0 + tid; b < b1; b += nt) {
@@ -149,7 +204,7 @@ __device__ __noinline__ bool build_incidence(const World& W, const SceneDesc& sc
         sort_manifold_entries(W, cur, seg, n);
     }
     if (tid == 0) st->ninc = total;
-    __syncthreads();
+    T.sync();
     return true;
 }
 
@@ -225,10 +280,11 @@ __device__ __forceinline__ void primal_group(const World& W, int cur, int b, flo
     if (b >= 0 && lane == 0) primal_finish(W, b, s);
 }
 
-// Sweeps the bodies list[0, n) with groups of G lanes of the calling CTA.
+// Sweeps the bodies list[0, n) with groups of G lanes of the calling team.
 template <int G>
-__device__ void primal_sweep_cta(const World& W, int cur, const int* list, int n, float alpha, bool write_stick) {
-    const int lane = threadIdx.x % G, gid = threadIdx.x / G, ngroups = blockDim.x / G;
+__device__ void primal_sweep_cta(const Team& T, const World& W, int cur, const int* list, int n, float alpha,
+                                 bool write_stick) {
+    const int lane = T.rank % G, gid = T.rank / G, ngroups = T.size / G;
     for (int base = 0; base < n; base += ngroups) {
         const int i = base + gid;
         int b = i < n ? list[i] : -1;
@@ -237,143 +293,165 @@ __device__ void primal_sweep_cta(const World& W, int cur, const int* list, int n
     }
 }
 
-__device__ __noinline__ void primal_sweep_cta_dispatch(const World& W, int cur, const int* list, int n, float alpha,
-                                                          bool write_stick, int group) {
+__device__ __noinline__ void primal_sweep_cta_dispatch(const Team& T, const World& W, int cur, const int* list, int n,
+                                                          float alpha, bool write_stick, int group) {
     switch (group) {
-        case 32: primal_sweep_cta<32>(W, cur, list, n, alpha, write_stick); break;
-        case 16: primal_sweep_cta<16>(W, cur, list, n, alpha, write_stick); break;
-        case 8: primal_sweep_cta<8>(W, cur, list, n, alpha, write_stick); break;
-        case 4: primal_sweep_cta<4>(W, cur, list, n, alpha, write_stick); break;
-        case 2: primal_sweep_cta<2>(W, cur, list, n, alpha, write_stick); break;
-        default: primal_sweep_cta<1>(W, cur, list, n, alpha, write_stick); break;
+        case 32: primal_sweep_cta<32>(T, W, cur, list, n, alpha, write_stick); break;
+        case 16: primal_sweep_cta<16>(T, W, cur, list, n, alpha, write_stick); break;
+        case 8: primal_sweep_cta<8>(T, W, cur, list, n, alpha, write_stick); break;
+        case 4: primal_sweep_cta<4>(T, W, cur, list, n, alpha, write_stick); break;
+        case 2: primal_sweep_cta<2>(T, W, cur, list, n, alpha, write_stick); break;
+        default: primal_sweep_cta<1>(T, W, cur, list, n, alpha, write_stick); break;
     }
 }
 
 // ---------------------------------------------------------------------------
 // Term-per-lane primal sweep of one colour, for scenes whose energies are all
-// tetrahedra.  Up to kFlatSlots (particle, tet) terms of the colour are
+// tetrahedra.  Up to nslots (particle, tet) terms of the colour are
 // evaluated at once, one per lane, into shared memory; then one lane per
 // particle adds its inertia, its force and manifold rows and its tet terms in
 // incidence order (the reference's order) and solves.  Lanes stay busy
 // whatever the particles' degrees.  tinc (the scene's col_tinc) holds the
-// inclusive prefix of tet terms over the colour list; the colour occupies
-// list positions [c0, c1).  sm: 10 * kFlatSlots words of shared memory.
+// inclusive prefix of tet terms over the colour list and fterm the terms'
+// incidence entries in that order (both made with the colouring); the colour
+// occupies list positions [c0, c1).  sm: 9 * nslots words of shared memory (the
+// broadphase's stage, reused).
 // ---------------------------------------------------------------------------
-constexpr int kFlatSlots = 1024;
-static_assert(10 * kFlatSlots * sizeof(float) <= kStagedBodies * sizeof(float4),
-              "the flat sweep reuses the broadphase's dynamic shared memory");
 
 __device__ __forceinline__ int tet_terms(const World& W, int b) { return W.sinc_n[b] - W.sinc_nf[b]; }
 
-__device__ __noinline__ void primal_sweep_flat(const World& W, int cur, const int* list, const int* tinc, int c0,
-                                               int c1, float alpha, bool write_stick, float* sm) {
-    int* smap = reinterpret_cast<int*>(sm + 9 * kFlatSlots);
-    const int tid = threadIdx.x, nt = blockDim.x;
+// Any body of a flat-swept colour: inertia, force and manifold rows, then its
+// tet terms from slot q0 on (q0 < 0: terms evaluated here, the slots did not
+// hold them).  Out of line: the 6x6 system stays out of the sweep's registers.
+__device__ __noinline__ void flat_finish_body(const World& W, int cur, int b, int e0, int e1, int q0, float alpha,
+                                              bool write_stick, const float* sm, int nslots) {
+    Sys6 s;
+    sys_zero(s);
+    primal_init_mass(W, b, s);
+    if (q0 < 0) {
+        primal_entry_range(W, cur, b, alpha, write_stick, e0, e1, 0, 1, s);
+    } else {
+        const int nterm = tet_terms(W, b);
+        primal_entry_range(W, cur, b, alpha, write_stick, e0, e1 - nterm, 0, 1, s);
+        for (int q = q0; q < q0 + nterm; ++q) {
+            // a removed tet left zeros: adding them changes no value
+            sys_add_energy(s, sm[0 * nslots + q], sm[1 * nslots + q], sm[2 * nslots + q],
+                           sm[3 * nslots + q], sm[4 * nslots + q], sm[5 * nslots + q],
+                           sm[6 * nslots + q], sm[7 * nslots + q], sm[8 * nslots + q]);
+        }
+    }
+    primal_finish(W, b, s);
+}
+
+__device__ __noinline__ void primal_sweep_flat(const Team& T, const World& W, int cur, const int* list,
+                                               const int* tinc, const uint32_t* fterm, int c0, int c1, float alpha,
+                                               bool write_stick) {
+    float* sm = reinterpret_cast<float*>(T.stage);
+    const int nslots = T.stage_cap * 4 / 9;
+    const int tid = T.rank, nt = T.size;
     for (int v = c0; v < c1;) {
         const int base = v == 0 ? 0 : tinc[v - 1];
         // the longest run of particles [v, vend) whose terms fit the slots (at least one)
-        int lo = v + 1, hi = c1;
-        while (lo < hi) {
-            const int mid = (lo + hi + 1) >> 1;
-            if (tinc[mid - 1] - base <= kFlatSlots) lo = mid;
-            else hi = mid - 1;
+        int vend = c1;
+        if (tinc[c1 - 1] - base > nslots) {
+            int lo = v + 1, hi = c1;
+            while (lo < hi) {
+                const int mid = (lo + hi + 1) >> 1;
+                if (tinc[mid - 1] - base <= nslots) lo = mid;
+                else hi = mid - 1;
+            }
+            vend = lo;
         }
-        const int vend = lo;
         const int total = tinc[vend - 1] - base;
-        const bool flat = total <= kFlatSlots;
+        const bool flat = total <= nslots;
         if (flat) {
-            for (int j = v + tid; j < vend; j += nt)
-                for (int q = (j == 0 ? 0 : tinc[j - 1]) - base; q < tinc[j] - base; ++q) smap[q] = j;
-            __syncthreads();
             for (int q = tid; q < total; q += nt) {
-                const int j = smap[q];
-                const int b = list[j];
-                const int k = q - ((j == 0 ? 0 : tinc[j - 1]) - base);
-                const uint32_t ent = W.inc[W.inc_off[b] + W.inc_cnt[b] - tet_terms(W, b) + k];
+                const uint32_t ent = fterm[base + q];
                 V3 g = v3(0.f, 0.f, 0.f);
                 S3 H;
                 s3_zero(H);
-                if (!(W.flags[b] & kBodyRemoved)) tet_term(W, (int)ent_index(ent), (int)ent_role(ent), g, H);
-                sm[0 * kFlatSlots + q] = g.x; sm[1 * kFlatSlots + q] = g.y; sm[2 * kFlatSlots + q] = g.z;
-                sm[3 * kFlatSlots + q] = H.xx; sm[4 * kFlatSlots + q] = H.yy; sm[5 * kFlatSlots + q] = H.zz;
-                sm[6 * kFlatSlots + q] = H.xy; sm[7 * kFlatSlots + q] = H.xz; sm[8 * kFlatSlots + q] = H.yz;
+                tet_term(W, (int)ent_index(ent), (int)ent_role(ent), g, H);   // removed tets stay zero
+                sm[0 * nslots + q] = g.x; sm[1 * nslots + q] = g.y; sm[2 * nslots + q] = g.z;
+                sm[3 * nslots + q] = H.xx; sm[4 * nslots + q] = H.yy; sm[5 * nslots + q] = H.zz;
+                sm[6 * nslots + q] = H.xy; sm[7 * nslots + q] = H.xz; sm[8 * nslots + q] = H.yz;
             }
-            __syncthreads();
+            T.sync();
         }
         for (int j = v + tid; j < vend; j += nt) {
             const int b = list[j];
             if (W.flags[b] & kBodyRemoved) continue;
-            Sys6 s;
-            sys_zero(s);
-            primal_init_mass(W, b, s);
             const int e0 = W.inc_off[b], e1 = e0 + W.inc_cnt[b];
-            if (!flat) {
-                primal_entry_range(W, cur, b, alpha, write_stick, e0, e1, 0, 1, s);
-            } else {
-                const int nterm = tet_terms(W, b);
-                primal_entry_range(W, cur, b, alpha, write_stick, e0, e1 - nterm, 0, 1, s);
-                const int q0 = (j == 0 ? 0 : tinc[j - 1]) - base;
-                for (int q = q0; q < q0 + nterm; ++q) {
-                    // a removed tet left zeros: adding them changes no value
-                    sys_add_energy(s, sm[0 * kFlatSlots + q], sm[1 * kFlatSlots + q], sm[2 * kFlatSlots + q],
-                                   sm[3 * kFlatSlots + q], sm[4 * kFlatSlots + q], sm[5 * kFlatSlots + q],
-                                   sm[6 * kFlatSlots + q], sm[7 * kFlatSlots + q], sm[8 * kFlatSlots + q]);
-                }
+            const int q0 = (j == 0 ? 0 : tinc[j - 1]) - base;
+            if (flat && e1 - e0 == tinc[j] - base - q0 && energy_only_particle(W, b)) {
+                Sys3 s;
+                particle_init_mass(W, b, s);
+                for (int q = q0; q < q0 + e1 - e0; ++q)
+                    particle_add_energy(s, sm[0 * nslots + q], sm[1 * nslots + q], sm[2 * nslots + q],
+                                        sm[3 * nslots + q], sm[4 * nslots + q], sm[5 * nslots + q],
+                                        sm[6 * nslots + q], sm[7 * nslots + q], sm[8 * nslots + q]);
+                particle_finish(W, b, s);
+                continue;
             }
-            primal_finish(W, b, s);
+            flat_finish_body(W, cur, b, e0, e1, flat ? q0 : -1, alpha, write_stick, sm, nslots);
         }
-        __syncthreads();
+        T.sync();
         v = vend;
     }
 }
 
 // One colour of a scene's primal sweep, by the scene's lane grouping.
-__device__ __forceinline__ void primal_colour(const World& W, const SceneDesc& sc, int cur, const int* cs, int c,
-                                              float alpha, bool write_stick, float* sm) {
+__device__ __forceinline__ void primal_colour(const Team& T, const World& W, const SceneDesc& sc, int cur,
+                                              const int* cs, int c, float alpha, bool write_stick) {
     if (sc.group == kGroupFlat)
-        primal_sweep_flat(W, cur, W.col_list + sc.body0, W.col_tinc + sc.body0, cs[c], cs[c + 1], alpha, write_stick,
-                          sm);
+        primal_sweep_flat(T, W, cur, W.col_list + sc.body0, W.col_tinc + sc.body0, W.fterm + 4 * (size_t)sc.tet0,
+                          cs[c], cs[c + 1], alpha, write_stick);
     else
-        primal_sweep_cta_dispatch(W, cur, W.col_list + sc.body0 + cs[c], cs[c + 1] - cs[c], alpha, write_stick,
+        primal_sweep_cta_dispatch(T, W, cur, W.col_list + sc.body0 + cs[c], cs[c + 1] - cs[c], alpha, write_stick,
                                   sc.group);
 }
 
-__device__ __noinline__ bool colour_scene(const World& W, const SceneDesc& sc, SceneState* st, int scene, int cur);
+__device__ __noinline__ bool colour_scene(const Team& T, const World& W, const SceneDesc& sc, SceneState* st,
+                                          int scene, int cur);
 
 // Keeps the previous step's colouring when the contact graph is unchanged:
 // the same number of live manifolds in both tables, every live one already
 // live last step, and no force or body removed since the colouring was made.
 // The colouring is a deterministic function of that graph, so reusing it is
 // exact.
-__device__ bool colour_scene_cached(const World& W, const SceneDesc& sc, SceneState* st, int scene, int cur) {
+__device__ bool colour_scene_cached(const Team& T, const World& W, const SceneDesc& sc, SceneState* st, int scene,
+                                    int cur) {
     const int old = cur ^ 1;
     const bool reuse = st->colours_valid && st->nlive[cur] == st->nlive[old] && st->nmatched == st->nlive[cur] &&
                        st->topo == st->coloured_topo;
-    __syncthreads();
+    T.sync();
     if (reuse) return true;
-    const bool ok = colour_scene(W, sc, st, scene, cur);
-    if (threadIdx.x == 0) {
+    const bool ok = colour_scene(T, W, sc, st, scene, cur);
+    if (T.rank == 0) {
         st->colours_valid = ok ? 1 : 0;
         st->coloured_topo = st->topo;
     }
-    __syncthreads();
+    T.sync();
     return ok;
 }
 
 // Returns false (status TIMEOUT or CAPACITY set) if colouring could not finish.
-__device__ __noinline__ bool colour_scene(const World& W, const SceneDesc& sc, SceneState* st, int scene, int cur) {
-    __shared__ int s_remaining, s_progress, s_maxc;
-    __shared__ int s_count[kMaxColours + 1];
-    const int tid = threadIdx.x, nt = blockDim.x;
+// The colour counts live in the team's stage (at least kMaxColours + 1 ints).
+__device__ __noinline__ bool colour_scene(const Team& T, const World& W, const SceneDesc& sc, SceneState* st,
+                                          int scene, int cur) {
+    int& s_remaining = T.sh->remaining;
+    int& s_progress = T.sh->progress;
+    int& s_maxc = T.sh->maxc;
+    int* s_count = reinterpret_cast<int*>(T.stage);
+    const int tid = T.rank, nt = T.size;
     const int b0 = sc.body0, b1 = sc.body0 + sc.nbody;
     volatile int* col = W.colour;
     for (int b = b0 + tid; b < b1; b += nt) col[b] = (W.flags[b] & (kBodyStatic | kBodyRemoved)) ? -2 : -1;
     if (tid == 0) s_maxc = 0;
-    __syncthreads();
+    T.sync();
     const int max_rounds = sc.nbody + 2;
     for (int round = 0;; ++round) {
         if (tid == 0) { s_remaining = 0; s_progress = 0; }
-        __syncthreads();
+        T.sync();
         for (int b = b0 + tid; b < b1; b += nt) {
             if (col[b] != -1) continue;
             const int lb = W.local[b];
@@ -406,26 +484,26 @@ __device__ __noinline__ bool colour_scene(const World& W, const SceneDesc& sc, S
             atomicMax(&s_maxc, chosen + 1);
             s_progress = 1;
         }
-        __syncthreads();
+        T.sync();
         const int remaining = s_remaining, progress = s_progress;
-        __syncthreads();   // every thread has read the flags before thread 0 resets them
+        T.sync();   // every thread has read the flags before thread 0 resets them
         if (!remaining) break;
         if (!progress || round > max_rounds) {
             if (tid == 0) st->status = kStatusTimeout;
-            __syncthreads();
+            T.sync();
             return false;
         }
     }
     const int ncol = s_maxc;
-    __syncthreads();
+    T.sync();
     // colour lists: counting sort of the dynamic bodies by colour
     for (int c = tid; c <= ncol; c += nt) s_count[c] = 0;
-    __syncthreads();
+    T.sync();
     for (int b = b0 + tid; b < b1; b += nt) {
         const int c = col[b];
         if (c >= 0) atomicAdd(&s_count[c], 1);
     }
-    __syncthreads();
+    T.sync();
     int* cs = W.col_start + (size_t)scene * (kMaxColours + 1);
     if (tid == 0) {
         int acc = 0;
@@ -433,7 +511,7 @@ __device__ __noinline__ bool colour_scene(const World& W, const SceneDesc& sc, S
         cs[ncol] = acc;
         st->ncolours = ncol;
     }
-    __syncthreads();
+    T.sync();
     // Within a colour, bodies are ordered by decreasing work (incidence entries
     // per lane of a body group), so the bodies sharing a warp take similar
     // time.  Bodies of one colour share no constraint, so their order within
@@ -446,71 +524,81 @@ __device__ __noinline__ bool colour_scene(const World& W, const SceneDesc& sc, S
             const int k = min(kColourWorkBuckets - 1, (W.inc_cnt[b] + g - 1) / g);
             if (k == key) W.col_list[b0 + atomicAdd(&s_count[c], 1)] = b;
         }
-        __syncthreads();
+        T.sync();
     }
     if (sc.group == kGroupFlat) {
         // inclusive prefix of tet terms over the list
         const int n = cs[ncol];
         int* tinc = W.col_tinc + b0;
         for (int i = tid; i < n; i += nt) tinc[i] = tet_terms(W, W.col_list[b0 + i]);
-        __syncthreads();
-        block_exclusive_scan(tinc, tinc, n);
-        for (int i = tid; i < n; i += nt) tinc[i] += tet_terms(W, W.col_list[b0 + i]);
-        __syncthreads();
+        T.sync();
+        block_exclusive_scan(T, tinc, tinc, n);
+        // the tet-term entries of every listed particle, in list order
+        uint32_t* fterm = W.fterm + 4 * (size_t)sc.tet0;
+        for (int i = tid; i < n; i += nt) {
+            const int b = W.col_list[b0 + i];
+            const int k = tet_terms(W, b);
+            const uint32_t* ent = W.inc + W.inc_off[b] + W.inc_cnt[b] - k;
+            const int q0 = tinc[i];
+            for (int e = 0; e < k; ++e) fterm[q0 + e] = ent[e];
+            tinc[i] = q0 + k;
+        }
+        T.sync();
     }
     return st->status == kStatusOk;
 }
 
 // Phase loops of one scene kept out of line, so each gets its own register
 // allocation instead of the union of every inlined phase.
-__device__ __noinline__ void narrowphase_cta(const World& W, const SceneDesc& sc, SceneState* st, int cur, int ncand,
-                                             int old_count) {
-    for (int c = sc.cand0 + threadIdx.x; c < sc.cand0 + ncand; c += blockDim.x)
+__device__ __noinline__ void narrowphase_cta(const Team& T, const World& W, const SceneDesc& sc, SceneState* st,
+                                             int cur, int ncand, int old_count) {
+    for (int c = sc.cand0 + T.rank; c < sc.cand0 + ncand; c += T.size)
         narrowphase_slot(W, sc, st, c, cur, old_count);
 }
 
 // Returns true if this thread saw a force fracture.  Manifolds come from the
 // step's live list (each manifold's dual is independent of the others).
-__device__ __noinline__ bool dual_cta(const World& W, const SceneDesc& sc, int cur, int nlive, bool last) {
+__device__ __noinline__ bool dual_cta(const Team& T, const World& W, const SceneDesc& sc, int cur, int nlive,
+                                      bool last) {
     bool broke = false;
-    for (int f = sc.force0 + threadIdx.x; f < sc.force0 + sc.nforce; f += blockDim.x)
+    for (int f = sc.force0 + T.rank; f < sc.force0 + sc.nforce; f += T.size)
         if (dual_force(W, f, W.P.alpha)) broke = true;
     const int* live = W.live[cur] + sc.cand0;
-    for (int i = threadIdx.x; i < nlive; i += blockDim.x) dual_manifold(W, cur, live[i], W.P.alpha, last);
+    for (int i = T.rank; i < nlive; i += T.size) dual_manifold(W, cur, live[i], W.P.alpha, last);
     return broke;
 }
 
 // ---------------------------------------------------------------------------
-// Whole step of one scene on one CTA (batched path).
+// Whole step of one scene by one team (batched path).
 // ---------------------------------------------------------------------------
-__device__ void scene_step(const World& W, int scene) {
+__device__ void scene_step(const World& W, int scene, const Team& T) {
     const SceneDesc sc = W.scenes[scene];
     SceneState* st = W.sstate + scene;
-    const int tid = threadIdx.x, nt = blockDim.x;
-    __shared__ int s_flags;
+    const int tid = T.rank, nt = T.size;
+    int& s_flags = T.sh->flags;
     if (st->status != kStatusOk && st->status != kStatusCapacity && st->status != kStatusTimeout) return;
-    __syncthreads();
+    T.sync();
     if (tid == 0) { st->status = kStatusOk; st->need_cand = 0; st->need_k = 0; st->need_inc = 0; }
     AVBD_PHASE_BEGIN(sc.ntet > 0 ? 1 : 0);
     const int old = st->cur, cur = old ^ 1;
     const int b0 = sc.body0, b1 = sc.body0 + sc.nbody;
     // 1. broadphase: count, scan, capacity check, write; positions and radii
     //    staged in shared memory when the scene fits
-    extern __shared__ float4 s_bodies[];
-    const bool staged = sc.nbody <= kStagedBodies;
+    float4* s_bodies = T.stage;
+    const bool staged = sc.nbody <= T.stage_cap;
     if (staged) {
         for (int b = b0 + tid; b < b1; b += nt) {
             float4 p = W.pos[b];
             p.w = (W.flags[b] & kBodyRemoved) ? -INFINITY : W.scale[b].w;
             s_bodies[b - b0] = p;
         }
-        __syncthreads();
+        T.sync();
     }
     for (int b = b0 + tid; b < b1; b += nt)
         W.cand_cnt[b] = staged ? broadphase_body_staged(W, sc, b, s_bodies, nullptr, 0)
                                : broadphase_body(W, sc, b, nullptr, 0);
-    __syncthreads();
-    const int ncand = block_exclusive_scan(W.cand_cnt + b0, W.cand_off + b0, sc.nbody);
+    T.sync();
+    const int ncand = block_exclusive_scan(T, W.cand_cnt + b0, W.cand_off + b0, sc.nbody);
     if (ncand > sc.candcap) {
         if (tid == 0) { st->status = kStatusCapacity; st->need_cand = ncand; }
         return;
@@ -521,12 +609,12 @@ __device__ void scene_step(const World& W, int scene) {
         else broadphase_body(W, sc, b, out, W.cand_cnt[b]);
     }
     if (tid == 0) { st->kused[cur] = 0; st->nlive[cur] = 0; st->nmatched = 0; }
-    __syncthreads();
+    T.sync();
     AVBD_PHASE(0);
     // 2. narrowphase + manifold warm start into the other table
     const int old_count = st->ncand[old];
-    narrowphase_cta(W, sc, st, cur, ncand, old_count);
-    __syncthreads();
+    narrowphase_cta(T, W, sc, st, cur, ncand, old_count);
+    T.sync();
     if (st->need_k) {
         if (tid == 0) { st->status = kStatusCapacity; st->need_k = st->kused[cur]; }
         return;
@@ -536,19 +624,19 @@ __device__ void scene_step(const World& W, int scene) {
     // 2b. joints / springs warm start
     for (int f = sc.force0 + tid; f < sc.force0 + sc.nforce; f += nt)
         if (force_init(W, f)) atomicAdd(&st->topo, 1);
-    __syncthreads();
+    T.sync();
     // incidence
-    if (!build_incidence(W, sc, st, cur)) {
+    if (!build_incidence(T, W, sc, st, cur)) {
         if (tid == 0) st->status = kStatusCapacity;
         return;
     }
     AVBD_PHASE(2);
     // colouring
-    if (!colour_scene_cached(W, sc, st, scene, cur)) return;
+    if (!colour_scene_cached(T, W, sc, st, scene, cur)) return;
     AVBD_PHASE(3);
     // 4. prediction
     for (int b = b0 + tid; b < b1; b += nt) predict_body(W, b);
-    __syncthreads();
+    T.sync();
     AVBD_PHASE(4);
     const int ncol = st->ncolours;
     const int nlive = st->nlive[cur];
@@ -556,34 +644,34 @@ __device__ void scene_step(const World& W, int scene) {
     // 5. iterations
     for (int it = 0; it < W.P.num_iterations; ++it) {
         for (int c = 0; c < ncol; ++c) {
-            primal_colour(W, sc, cur, cs, c, W.P.alpha, false, reinterpret_cast<float*>(s_bodies));
-            __syncthreads();
+            primal_colour(T, W, sc, cur, cs, c, W.P.alpha, false);
+            T.sync();
         }
         AVBD_PHASE(5);
         if (tid == 0) s_flags = 0;
-        __syncthreads();
-        if (dual_cta(W, sc, cur, nlive, it == W.P.num_iterations - 1)) s_flags = 1;
-        __syncthreads();
+        T.sync();
+        if (dual_cta(T, W, sc, cur, nlive, it == W.P.num_iterations - 1)) s_flags = 1;
+        T.sync();
         const int fractured = s_flags;
-        __syncthreads();
+        T.sync();
         if (fractured) {
             for (int i = tid; i < nlive; i += nt) fracture_reset_slot(W, cur, W.live[cur][sc.cand0 + i]);
-            __syncthreads();
+            T.sync();
             for (int b = b0 + tid; b < b1; b += nt) W.reset_flag[b] = 0;
-            __syncthreads();
+            T.sync();
         }
         AVBD_PHASE(6);
     }
     // 6. velocities, explosion, out of bounds
     if (tid == 0) s_flags = 0;
-    __syncthreads();
+    T.sync();
     for (int b = b0 + tid; b < b1; b += nt) {
         const int r = velocity_body(W, b);
         if (r) atomicOr(&s_flags, r);
     }
-    __syncthreads();
+    T.sync();
     const int vf = s_flags;
-    __syncthreads();
+    T.sync();
     if (vf & 1) { if (tid == 0) st->status = kStatusExploded; return; }
     if (vf & 2) { if (tid == 0) st->status = kStatusNan; return; }
     if (vf & 4) {
@@ -605,15 +693,15 @@ __device__ void scene_step(const World& W, int scene) {
                 }
             }
         }
-        __syncthreads();
+        T.sync();
     }
     if (tid == 0) st->step += 1;
     AVBD_PHASE(7);
     // 7. post-stabilisation
     if (W.P.post_stabilization) {
         for (int c = 0; c < ncol; ++c) {
-            primal_colour(W, sc, cur, cs, c, 0.f, true, reinterpret_cast<float*>(s_bodies));
-            __syncthreads();
+            primal_colour(T, W, sc, cur, cs, c, 0.f, true);
+            T.sync();
         }
     }
     AVBD_PHASE(8);

@@ -330,8 +330,14 @@ class Batch:
     def set_launch(self, threads_per_cta=0, ctas_per_sm=0):
         check(self._lib.avbd_batch_set_launch(self._h, int(threads_per_cta), int(ctas_per_sm)), "set_launch")
 
+    def set_team_work(self, units_per_lane=0):
+        """Scenes with at most this many (bodies + tets) per lane of half a team
+        share a CTA with others (0: one scene per CTA); before stepping."""
+        check(self._lib.avbd_batch_set_team_work(self._h, int(units_per_lane)), "set_team_work")
+
     def set_kernel(self, register_variant=1):
-        """Register budget of the persistent kernel build (1..4)."""
+        """Build of the persistent kernel: 1..4 for CTAs of up to 256 threads
+        (156, 128, 80 or 64 registers), 5/6 for 512 threads, 7 for 1024."""
         check(self._lib.avbd_batch_set_kernel(self._h, int(register_variant)), "set_kernel")
 
     def launch(self):

@@ -122,3 +122,22 @@ def test_flat_sweep_matches_oracle(oracle_mod):
         f(o)
         assert o.step_coloured() == 0
         assert np.abs(o.get_state()[0] - flat[i][0]).max(initial=0.0) <= 1e-4, f"scene {i}"
+
+
+def test_team_split_changes_nothing():
+    """Small scenes run by half- or quarter-CTA teams give bitwise the results
+    of one scene per CTA (no per-body arithmetic depends on the team size)."""
+    from skyephyx_b200 import Batch
+    builders = mix_builders()
+    results = []
+    for team_work in (0, 64):
+        b = Batch()
+        b.set_team_work(team_work)
+        keep = [staged(f) for f in builders]
+        for w in keep:
+            b.add_scene(w)
+        assert b.step(3) == "ok"
+        results.append([b.get_state(i)[:2] for i in range(len(builders))])
+    for i, ((p0, q0), (p1, q1)) in enumerate(zip(*results)):
+        assert np.array_equal(p0.view(np.uint32), p1.view(np.uint32)), f"scene {i}"
+        assert np.array_equal(q0.view(np.uint32), q1.view(np.uint32)), f"scene {i}"
