@@ -53,8 +53,11 @@ uint32_t colour_hash(uint32_t x) {
 }
 
 // CPU twin of the device colouring: greedy first-fit in priority order, where
-// priority is (hash(local index), local index) ascending.  Edges join dynamic
-// bodies that share a force (manifold, joint, spring) or an energy.
+// priority is (degree descending, hash(local index), local index), degree
+// being the number of forces and energies a body takes part in; then one
+// iterated-greedy pass (priority: first-pass colour descending, then as
+// before).  Edges join dynamic bodies that share a force (manifold, joint,
+// spring) or an energy.
 void colour_bodies(Orc& o) {
     Solver& s = o.solver;
     const int n = (int)s.bodyPtrs.size();
@@ -70,23 +73,42 @@ void colour_bodies(Orc& o) {
     };
     for (Force* f : s.forcePtrs) link(f->linkedBodies);
     for (Energy* e : s.energyPtrs) link(e->linkedBodies);
+    // priority: more forces and energies first (largest degree first), then hash, then index
+    std::vector<int> deg(n, 0);
+    for (Force* f : s.forcePtrs)
+        for (Mesh* m : f->linkedBodies) ++deg[m->solverIndex];
+    for (Energy* e : s.energyPtrs)
+        for (Mesh* m : e->linkedBodies) ++deg[m->solverIndex];
     std::vector<int> order(n);
     for (int i = 0; i < n; ++i) order[i] = i;
-    std::sort(order.begin(), order.end(), [](int a, int b) {
+    std::sort(order.begin(), order.end(), [&](int a, int b) {
+        if (deg[a] != deg[b]) return deg[a] > deg[b];
         uint32_t ha = colour_hash((uint32_t)a), hb = colour_hash((uint32_t)b);
         return ha != hb ? ha < hb : a < b;
     });
-    std::vector<int> col(n, -1);
-    int ncol = 0;
-    std::vector<char> used;
-    for (int v : order) {
-        if (s.bodyPtrs[v]->isStatic) continue;
-        used.assign(ncol + 1, 0);
-        for (int u : adj[v]) if (col[u] >= 0) used[col[u]] = 1;
-        int c = 0;
-        while (used[c]) ++c;
-        col[v] = c;
-        if (c + 1 > ncol) ncol = c + 1;
+    auto greedy = [&](const std::vector<int>& ord, std::vector<int>& col) {
+        col.assign(n, -1);
+        int ncol = 0;
+        std::vector<char> used;
+        for (int v : ord) {
+            if (s.bodyPtrs[v]->isStatic) continue;
+            used.assign(ncol + 1, 0);
+            for (int u : adj[v]) if (col[u] >= 0) used[col[u]] = 1;
+            int c = 0;
+            while (used[c]) ++c;
+            col[v] = c;
+            if (c + 1 > ncol) ncol = c + 1;
+        }
+        return ncol;
+    };
+    std::vector<int> col;
+    int ncol = greedy(order, col);
+    {
+        // one iterated-greedy pass (never more colours): the classes in reverse
+        // order, each class in the first pass's priority order
+        std::vector<int> prev = col;
+        std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return prev[a] > prev[b]; });
+        ncol = greedy(order, col);
     }
     o.colour = col;
     o.num_colours = ncol;

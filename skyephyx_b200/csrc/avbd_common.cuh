@@ -237,6 +237,17 @@ struct World {
 // Vector helpers
 // ---------------------------------------------------------------------------
 struct V3 { float x, y, z; };
+// Fast reciprocal and reciprocal square root (a couple of ulp on the device,
+// where they replace IEEE divide / square-root sequences on latency-critical
+// chains; plain on the host).
+#if defined(__CUDA_ARCH__)
+AVBD_HD float fast_rcp(float x) { return __fdividef(1.f, x); }
+AVBD_HD float fast_rsqrt(float x) { return rsqrtf(x); }
+#else
+AVBD_HD float fast_rcp(float x) { return 1.f / x; }
+AVBD_HD float fast_rsqrt(float x) { return 1.f / sqrtf(x); }
+#endif
+
 struct Q4 { float x, y, z, w; };   // quaternion, Eigen coefficient order
 
 AVBD_HD V3 v3(float x, float y, float z) { V3 r; r.x = x; r.y = y; r.z = z; return r; }
@@ -320,8 +331,8 @@ AVBD_HD V3 qvec(Q4 a) { return v3(a.x, a.y, a.z); }
 AVBD_HD Q4 qnormalize(Q4 q) {
     float n2 = ((q.x * q.x + q.y * q.y) + q.z * q.z) + q.w * q.w;
     if (n2 > 0.f) {
-        float n = sqrtf(n2);
-        q.x /= n; q.y /= n; q.z /= n; q.w /= n;
+        const float inv = fast_rsqrt(n2);
+        q.x *= inv; q.y *= inv; q.z *= inv; q.w *= inv;
     }
     return q;
 }
@@ -341,7 +352,7 @@ AVBD_HD V3 rotation_difference(Q4 q, Q4 p) {
     float sin_half = norm(v);
     if (sin_half < 1e-6f) return 2.f * v;
     float half = atan2f(sin_half, dq.w);
-    return (2.f * half / sin_half) * v;
+    return (2.f * half * fast_rcp(sin_half)) * v;
 }
 // QuaternionFromDifference (math.hpp:31-48)
 AVBD_HD Q4 quaternion_from_difference(V3 v, float sign) {
@@ -356,7 +367,7 @@ AVBD_HD Q4 quaternion_from_difference(V3 v, float sign) {
         float s, c;
         sincosf(ha, &s, &c);
         q.w = c;
-        V3 h = (sign * s) * (v / angle);
+        V3 h = (sign * s * fast_rcp(angle)) * v;
         q.x = h.x; q.y = h.y; q.z = h.z;
     }
     return qnormalize(q);
@@ -373,16 +384,6 @@ AVBD_HD V3 quaternion_to_rotvec(Q4 q) {
 
 AVBD_HD float clampf(float v, float lo, float hi) { return v < lo ? lo : (hi < v ? hi : v); }
 
-// Fast reciprocal and reciprocal square root (a couple of ulp on the device,
-// where they replace IEEE divide / square-root sequences on latency-critical
-// chains; plain on the host).
-#if defined(__CUDA_ARCH__)
-AVBD_HD float fast_rcp(float x) { return __fdividef(1.f, x); }
-AVBD_HD float fast_rsqrt(float x) { return rsqrtf(x); }
-#else
-AVBD_HD float fast_rcp(float x) { return 1.f / x; }
-AVBD_HD float fast_rsqrt(float x) { return 1.f / sqrtf(x); }
-#endif
 
 AVBD_HD uint32_t colour_priority(uint32_t x) {
     // integer mixer (Wellons "lowbias32"); the CPU colouring twin uses the same function

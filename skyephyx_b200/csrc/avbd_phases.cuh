@@ -117,6 +117,21 @@ AVBD_HD bool sphere_overlap(float4 pi, float4 pj, float ri, float rj) {
     return dist < XADD(ri, rj);
 }
 
+// The same decision as sphere_overlap, settled by a squared-distance test
+// wherever the two sides are further apart than any rounding of either form
+// (relative band 1e-5, against errors of a few 1e-7); pairs inside the band
+// take the exact test.
+AVBD_HD bool sphere_overlap_fast(float4 pi, float4 pj, float ri, float rj) {
+    const float dx = pi.x - pj.x, dy = pi.y - pj.y, dz = pi.z - pj.z;
+    const float d2 = dx * dx + dy * dy + dz * dz;
+    const float r = ri + rj;
+    if (!(r > 0.f)) return sphere_overlap(pi, pj, ri, rj);   // removed (-inf) or degenerate radii
+    const float r2 = r * r;
+    if (d2 > r2 * 1.00001f) return false;
+    if (d2 < r2 * 0.99999f) return true;
+    return sphere_overlap(pi, pj, ri, rj);
+}
+
 // Returns the number of candidates owned by body i; writes them when out != 0.
 AVBD_HD int broadphase_body(const World& W, const SceneDesc& sc, int i, int2* out, int cap) {
     if (W.flags[i] & kBodyRemoved) return 0;
@@ -126,7 +141,7 @@ AVBD_HD int broadphase_body(const World& W, const SceneDesc& sc, int i, int2* ou
     int n = 0;
     for (int j = i + 1; j < end; ++j) {
         if (W.flags[j] & kBodyRemoved) continue;
-        if (!sphere_overlap(pi, W.pos[j], ri, W.scale[j].w)) continue;
+        if (!sphere_overlap_fast(pi, W.pos[j], ri, W.scale[j].w)) continue;
         if (pair_constrained(W, 0, i, j)) continue;
         if (out && n < cap) out[n] = make_int2(i, j);
         ++n;
@@ -143,7 +158,7 @@ AVBD_HD int broadphase_body_staged(const World& W, const SceneDesc& sc, int i, c
     int n = 0;
     for (int lj = li + 1; lj < sc.nbody; ++lj) {
         const float4 pj = sp[lj];
-        if (!sphere_overlap(pi, pj, pi.w, pj.w)) continue;
+        if (!sphere_overlap_fast(pi, pj, pi.w, pj.w)) continue;
         const int j = sc.body0 + lj;
         if (pair_constrained(W, 0, i, j)) continue;
         if (out && n < cap) out[n] = make_int2(i, j);

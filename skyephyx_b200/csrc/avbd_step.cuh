@@ -209,12 +209,10 @@ __device__ __noinline__ bool build_incidence(const Team& T, const World& W, cons
 }
 
 // ---------------------------------------------------------------------------
-// Jones-Plassmann first-fit colouring of the dynamic bodies of one scene.
-// Priority = (hash(local index), local index), smaller first.  A body takes
-// the smallest colour not used by its smaller-priority neighbours once all of
-// them are coloured, which equals sequential greedy colouring in priority
-// order whatever the thread schedule (each body's colour depends only on the
-// final colours of its smaller-priority neighbours).
+// Colouring of the dynamic bodies of one scene: Jones-Plassmann first-fit
+// (equal to sequential greedy colouring in priority order), largest degree
+// first, then one iterated-greedy pass that never adds colours and usually
+// removes the thin last classes (see colour_before / jp_pass).
 // ---------------------------------------------------------------------------
 __device__ __forceinline__ bool prio_less(uint32_t ha, int la, uint32_t hb, int lb) {
     return ha != hb ? ha < hb : la < lb;
@@ -434,35 +432,58 @@ __device__ bool colour_scene_cached(const Team& T, const World& W, const SceneDe
     return ok;
 }
 
-// Returns false (status TIMEOUT or CAPACITY set) if colouring could not finish.
-// The colour counts live in the team's stage (at least kMaxColours + 1 ints).
-__device__ __noinline__ bool colour_scene(const Team& T, const World& W, const SceneDesc& sc, SceneState* st,
-                                          int scene, int cur) {
+// Live incidence entries of body b: the forces and energies it takes part in.
+__device__ __forceinline__ int live_degree(const World& W, int b) {
+    const int e0 = W.inc_off[b], e1 = e0 + W.inc_cnt[b];
+    int n = 0;
+    for (int e = e0; e < e1; ++e) {
+        const uint32_t ent = W.inc[e];
+        const uint32_t kind = ent_kind(ent), idx = ent_index(ent);
+        if (kind == kEntManifold) ++n;
+        else if (kind == kEntForce) n += (W.ftype[idx] & kForceRemoved) ? 0 : 1;
+        else if (kind == kEntTet) n += W.tparam[idx].w != 0.f ? 0 : 1;
+        else n += W.rparam[idx].w != 0.f ? 0 : 1;
+    }
+    return n;
+}
+
+// Colouring priority: body u precedes body v.  Pass 0: larger live degree
+// (W.cntB) first, then (hash(local index), local index); pass 1 (iterated
+// greedy): larger pass-0 colour (W.bcur) first, then as pass 0.
+__device__ __forceinline__ bool colour_before(const World& W, int pass, int u, int v) {
+    if (pass == 1) {
+        const int pu = W.bcur[u], pv = W.bcur[v];
+        if (pu != pv) return pu > pv;
+    }
+    const int du = W.cntB[u], dv = W.cntB[v];
+    if (du != dv) return du > dv;
+    const int lu = W.local[u], lv = W.local[v];
+    return prio_less(colour_priority((uint32_t)lu), lu, colour_priority((uint32_t)lv), lv);
+}
+
+// One Jones-Plassmann pass over the scene's uncoloured (-1) bodies: a body
+// takes the smallest colour its preceding neighbours do not use once they
+// are all coloured, which equals sequential greedy colouring in priority
+// order whatever the thread schedule.  False (status TIMEOUT) if it stalls.
+__device__ bool jp_pass(const Team& T, const World& W, const SceneDesc& sc, SceneState* st, int cur, int pass) {
     int& s_remaining = T.sh->remaining;
     int& s_progress = T.sh->progress;
     int& s_maxc = T.sh->maxc;
-    int* s_count = reinterpret_cast<int*>(T.stage);
     const int tid = T.rank, nt = T.size;
     const int b0 = sc.body0, b1 = sc.body0 + sc.nbody;
     volatile int* col = W.colour;
-    for (int b = b0 + tid; b < b1; b += nt) col[b] = (W.flags[b] & (kBodyStatic | kBodyRemoved)) ? -2 : -1;
-    if (tid == 0) s_maxc = 0;
-    T.sync();
     const int max_rounds = sc.nbody + 2;
     for (int round = 0;; ++round) {
         if (tid == 0) { s_remaining = 0; s_progress = 0; }
         T.sync();
         for (int b = b0 + tid; b < b1; b += nt) {
             if (col[b] != -1) continue;
-            const int lb = W.local[b];
-            const uint32_t hb = colour_priority((uint32_t)lb);
             bool ready = true;
             for_each_neighbour(W, cur, b, [&](int n) {
                 if (!ready) return;
                 const int cn = col[n];
                 if (cn == -2) return;
-                const int ln = W.local[n];
-                if (prio_less(colour_priority((uint32_t)ln), ln, hb, lb) && cn < 0) ready = false;
+                if (cn < 0 && colour_before(W, pass, n, b)) ready = false;
             });
             if (!ready) { s_remaining = 1; continue; }
             int chosen = -1;
@@ -471,8 +492,7 @@ __device__ __noinline__ bool colour_scene(const Team& T, const World& W, const S
                 for_each_neighbour(W, cur, b, [&](int n) {
                     const int cn = col[n];
                     if (cn < base || cn >= base + 64) return;
-                    const int ln = W.local[n];
-                    if (prio_less(colour_priority((uint32_t)ln), ln, hb, lb)) used |= 1ull << (cn - base);
+                    if (colour_before(W, pass, n, b)) used |= 1ull << (cn - base);
                 });
                 if (~used) chosen = base + __ffsll((long long)~used) - 1;
             }
@@ -487,13 +507,40 @@ __device__ __noinline__ bool colour_scene(const Team& T, const World& W, const S
         T.sync();
         const int remaining = s_remaining, progress = s_progress;
         T.sync();   // every thread has read the flags before thread 0 resets them
-        if (!remaining) break;
+        if (!remaining) return true;
         if (!progress || round > max_rounds) {
             if (tid == 0) st->status = kStatusTimeout;
             T.sync();
             return false;
         }
     }
+}
+
+// Returns false (status TIMEOUT or CAPACITY set) if colouring could not finish.
+// The colour counts live in the team's stage (at least kMaxColours + 1 ints).
+// Priorities read W.cntB and W.bcur, free once the incidence is built.
+__device__ __noinline__ bool colour_scene(const Team& T, const World& W, const SceneDesc& sc, SceneState* st,
+                                          int scene, int cur) {
+    int& s_maxc = T.sh->maxc;
+    int* s_count = reinterpret_cast<int*>(T.stage);
+    const int tid = T.rank, nt = T.size;
+    const int b0 = sc.body0, b1 = sc.body0 + sc.nbody;
+    volatile int* col = W.colour;
+    for (int b = b0 + tid; b < b1; b += nt) {
+        col[b] = (W.flags[b] & (kBodyStatic | kBodyRemoved)) ? -2 : -1;
+        W.cntB[b] = live_degree(W, b);
+    }
+    if (tid == 0) s_maxc = 0;
+    T.sync();
+    if (!jp_pass(T, W, sc, st, cur, 0)) return false;
+    for (int b = b0 + tid; b < b1; b += nt) {
+        const int c = col[b];
+        W.bcur[b] = c;
+        if (c >= 0) col[b] = -1;
+    }
+    if (tid == 0) s_maxc = 0;
+    T.sync();
+    if (!jp_pass(T, W, sc, st, cur, 1)) return false;
     const int ncol = s_maxc;
     T.sync();
     // colour lists: counting sort of the dynamic bodies by colour

@@ -128,22 +128,33 @@ def lowbias32(x):
 
 
 def greedy_colours(n, static, edges):
-    """Sequential greedy colouring in (hash, index) priority order."""
+    """Sequential greedy colouring in (degree descending, hash, index) priority
+    order, then one iterated-greedy pass (first-pass colour descending first)."""
     adj = [set() for _ in range(n)]
+    deg = [0] * n
     for a, b in edges:
+        deg[a] += 1
+        deg[b] += 1
         if a != b and not static[a] and not static[b]:
             adj[a].add(b)
             adj[b].add(a)
-    col = [-1] * n
-    for v in sorted(range(n), key=lambda i: (lowbias32(i), i)):
-        if static[v]:
-            continue
-        used = {col[u] for u in adj[v] if col[u] >= 0}
-        c = 0
-        while c in used:
-            c += 1
-        col[v] = c
-    return np.array(col, np.int32)
+
+    def greedy(order):
+        col = [-1] * n
+        for v in order:
+            if static[v]:
+                continue
+            used = {col[u] for u in adj[v] if col[u] >= 0}
+            c = 0
+            while c in used:
+                c += 1
+            col[v] = c
+        return col
+
+    order = sorted(range(n), key=lambda i: (-deg[i], lowbias32(i), i))
+    first = greedy(order)
+    order = sorted(order, key=lambda i: -first[i])   # stable: classes in reverse, same order within
+    return np.array(greedy(order), np.int32)
 
 
 def test_colouring_reuse_is_exact(Solver):
