@@ -227,6 +227,10 @@ int32_t avbd_batch_get_launch(const AvbdBatch* b, int32_t* threads_per_cta, int3
  * takes the next scene, down to a warp (or an eighth of a larger CTA).
  * 0 (the default) keeps one scene per CTA.  Autotuner knob. */
 int32_t avbd_batch_set_team_work(AvbdBatch* b, int32_t units_per_lane);
+/* Scenes of at least min_bodies bodies find broadphase candidates with a
+ * uniform grid (the same candidate set and order as the reference's all-pairs
+ * loop, which smaller scenes keep); 0 = all-pairs everywhere.  Default 128. */
+int32_t avbd_batch_set_grid_broadphase(AvbdBatch* b, int32_t min_bodies);
 /* Build of the persistent kernel: 1..4 serve CTAs of up to 256 threads with
  * about 156, 128, 80 or 64 registers per thread (spills traded for resident
  * warps); 5 and 6 serve 512 threads (128 or 64 registers), 7 serves 1024

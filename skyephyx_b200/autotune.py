@@ -37,6 +37,7 @@ SPACE = {
     "rigid_group": (1, 2),
     "fem_group": (2, 4, 8, 64),   # 64: term-per-lane flat sweep
     "team_work": (0, 2, 4, 8),    # scene work per lane below which CTAs split into teams
+    "grid_min": (0, 128, 512),    # scenes from this many bodies use the grid broadphase
 }
 
 
@@ -78,6 +79,7 @@ def apply(batch, cfg: dict) -> None:
     batch.set_kernel(cfg["variant"])
     batch.set_launch(cfg["threads"], 0)
     batch.set_team_work(cfg.get("team_work", 0))
+    batch.set_grid_broadphase(cfg.get("grid_min", 128))
 
 
 def candidates(space=SPACE):

@@ -847,6 +847,7 @@ struct AvbdBatch {
     int grid = 0;
     int stage = 0;   // float4 slots of dynamic shared memory per CTA
     int team_work = 0;   // bodies + tets per lane below which a CTA team splits (0 = never)
+    int grid_min = 128;  // scenes from this many bodies use the grid broadphase (0 = never)
     float last_ms = 0.f;
 };
 
@@ -980,6 +981,7 @@ int batch_build_graph(AvbdBatch* b) {
     cudaMemsetAsync(b->d_queue, 0, sizeof(int), b->stream);
     b->P.W.stage_bodies = b->stage;
     b->P.W.team_work = b->team_work;
+    b->P.W.grid_min = b->grid_min;
     const size_t smem = (size_t)b->stage * sizeof(float4);
     {
         const int* order = b->d_order;
@@ -1567,6 +1569,13 @@ int32_t avbd_batch_set_kernel(AvbdBatch* b, int32_t register_variant) {
 int32_t avbd_batch_set_team_work(AvbdBatch* b, int32_t units_per_lane) {
     if (!b || units_per_lane < 0) return AVBD_ERR_INVALID;
     b->team_work = units_per_lane;
+    batch_drop_graph(b);
+    return 0;
+}
+
+int32_t avbd_batch_set_grid_broadphase(AvbdBatch* b, int32_t min_bodies) {
+    if (!b || min_bodies < 0) return AVBD_ERR_INVALID;
+    b->grid_min = min_bodies;
     batch_drop_graph(b);
     return 0;
 }

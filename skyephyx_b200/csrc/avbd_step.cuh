@@ -34,9 +34,13 @@ constexpr int kStagedBodies = 2560;   // stage of a 256-thread CTA (40 KB); smal
 constexpr int kMaxTeams = 8;          // teams a CTA may split into
 
 // Scalars a team shares through shared memory.
+constexpr int kGridMaxBig = 32;   // big bodies (kept out of the broadphase grid) a scene may have
+
 struct TeamShared {
-    int q, flags, remaining, progress, maxc, carry;
+    int q, flags, remaining, progress, maxc, carry, nbig;
     int warp_tot[32];
+    int red[8];
+    int big[kGridMaxBig];
 };
 
 // Consecutive whole warps of a CTA that run one scene together: the whole CTA
@@ -616,6 +620,214 @@ __device__ __noinline__ bool dual_cta(const Team& T, const World& W, const Scene
 }
 
 // ---------------------------------------------------------------------------
+// Uniform-grid broadphase of one scene (the same candidate set and order as
+// the all-pairs loop of broadphase_body, found in about O(n) instead of
+// O(n^2)).  Cells are 2R wide, R the largest detection radius, so two
+// overlapping spheres (distance < r_i + r_j <= 2R) sit in the same or
+// adjacent cells; each body tests the bodies of its 27 neighbouring cells
+// with the exact sphere test and the joint/spring filter, and its candidate
+// list is sorted by partner index, as the reference's nested loop emits it.
+// Scratch: the team's stage after the staged poses (cell starts, 16-bit
+// items) when it fits, else W.bcur and W.cntB; W.cand_off holds each body's
+// rank in its cell before it takes the candidate offsets.  Returns the
+// candidate count; writes the pairs when they fit candcap; returns -1 when
+// the extents are not finite (the caller then uses the all-pairs loop).
+// ---------------------------------------------------------------------------
+__device__ __forceinline__ int ord_float(float f) {
+    const int i = __float_as_int(f);
+    return i >= 0 ? i : i ^ 0x7fffffff;
+}
+__device__ __forceinline__ float unord_float(int i) { return __int_as_float(i >= 0 ? i : i ^ 0x7fffffff); }
+
+__device__ __forceinline__ float4 body_sphere(const World& W, const SceneDesc& sc, const float4* sp, int li) {
+    if (sp) return sp[li];
+    const int b = sc.body0 + li;
+    float4 p = W.pos[b];
+    p.w = (W.flags[b] & kBodyRemoved) ? -INFINITY : W.scale[b].w;
+    return p;
+}
+
+struct GridDims {
+    float minx, miny, minz, inv_h;
+    int nx, ny, nz;
+    __device__ __forceinline__ int cell_axis(float v, float mn, int n) const {
+        const int c = (int)((v - mn) * inv_h);
+        return c < 0 ? 0 : (c >= n ? n - 1 : c);
+    }
+    __device__ __forceinline__ int cell(const float4& p) const {
+        return (cell_axis(p.z, minz, nz) * ny + cell_axis(p.y, miny, ny)) * nx + cell_axis(p.x, minx, nx);
+    }
+};
+
+// Cell starts (ncell + 1) and cell items (body local indices) of the grid:
+// in shared memory after the staged poses when they fit, else in per-body
+// scratch (W.bcur, W.cntB); plus the scene's big bodies (radius above rbig),
+// which stay out of the grid.
+struct GridCells {
+    const int* cstart;
+    const unsigned short* items16;   // shared-memory items
+    const int* items32;              // global items
+    const int* big;                  // local indices of the big bodies
+    int nbig;
+    float rbig;
+    __device__ __forceinline__ int item(int k) const { return items16 ? (int)items16[k] : items32[k]; }
+};
+
+template <bool WRITE>
+__device__ __forceinline__ void grid_test(const World& W, const SceneDesc& sc, const float4* sp, const float4& pi,
+                                          int li, int lj, int2* out, int& n) {
+    if (lj <= li) return;
+    const float4 pj = body_sphere(W, sc, sp, lj);
+    if (!sphere_overlap_fast(pi, pj, pi.w, pj.w)) return;
+    const int bi = sc.body0 + li, bj = sc.body0 + lj;
+    if (pair_constrained(W, 0, bi, bj)) return;
+    if (WRITE) {
+        // insert in partner order, as the all-pairs loop emits them
+        int j = n - 1;
+        while (j >= 0 && out[j].y > bj) { out[j + 1] = out[j]; --j; }
+        out[j + 1] = make_int2(bi, bj);
+    }
+    ++n;
+}
+
+template <bool WRITE>
+__device__ __forceinline__ int grid_candidates(const World& W, const SceneDesc& sc, const float4* sp, const GridDims& g,
+                                               const GridCells& gc, int li, int2* out) {
+    const float4 pi = body_sphere(W, sc, sp, li);
+    if (isinf(pi.w)) return 0;
+    int n = 0;
+    if (pi.w > gc.rbig) {
+        // a big body: its all-pairs row
+        for (int lj = li + 1; lj < sc.nbody; ++lj) grid_test<WRITE>(W, sc, sp, pi, li, lj, out, n);
+        return n;
+    }
+    const int cx = g.cell_axis(pi.x, g.minx, g.nx), cy = g.cell_axis(pi.y, g.miny, g.ny),
+              cz = g.cell_axis(pi.z, g.minz, g.nz);
+    for (int z = max(cz - 1, 0); z <= min(cz + 1, g.nz - 1); ++z)
+        for (int y = max(cy - 1, 0); y <= min(cy + 1, g.ny - 1); ++y) {
+            const int row = (z * g.ny + y) * g.nx;
+            // the three cells of a row are contiguous in the item list
+            const int k0 = gc.cstart[row + max(cx - 1, 0)], k1 = gc.cstart[row + min(cx + 1, g.nx - 1) + 1];
+            for (int k = k0; k < k1; ++k) grid_test<WRITE>(W, sc, sp, pi, li, gc.item(k), out, n);
+        }
+    for (int k = 0; k < gc.nbig; ++k) grid_test<WRITE>(W, sc, sp, pi, li, gc.big[k], out, n);
+    return n;
+}
+
+__device__ __noinline__ int broadphase_grid(const Team& T, const World& W, const SceneDesc& sc, int cur,
+                                            const float4* sp) {
+    const int tid = T.rank, nt = T.size, n = sc.nbody, b0 = sc.body0;
+    int* red = T.sh->red;
+    // 1. smallest radius; bodies above 8x it are "big" and stay out of the grid
+    if (tid == 0) red[7] = ord_float(INFINITY);
+    T.sync();
+    {
+        float rmin = INFINITY;
+        for (int li = tid; li < n; li += nt) {
+            const float4 p = body_sphere(W, sc, sp, li);
+            if (!isinf(p.w)) rmin = fminf(rmin, p.w);
+        }
+        atomicMin(&red[7], ord_float(rmin));
+    }
+    T.sync();
+    const float rbig = 8.f * unord_float(red[7]);
+    T.sync();
+    // 2. extents and largest radius of the small bodies; the big ones listed
+    int* big = T.sh->big;
+    if (tid == 0) {
+        red[0] = red[1] = red[2] = ord_float(INFINITY);
+        red[3] = red[4] = red[5] = ord_float(-INFINITY);
+        red[6] = ord_float(0.f);
+        T.sh->nbig = 0;
+    }
+    T.sync();
+    {
+        float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY}, mr = 0.f;
+        for (int li = tid; li < n; li += nt) {
+            const float4 p = body_sphere(W, sc, sp, li);
+            if (isinf(p.w)) continue;
+            if (p.w > rbig) {
+                const int k = atomicAdd(&T.sh->nbig, 1);
+                if (k < kGridMaxBig) big[k] = li;
+                continue;
+            }
+            mn[0] = fminf(mn[0], p.x); mn[1] = fminf(mn[1], p.y); mn[2] = fminf(mn[2], p.z);
+            mx[0] = fmaxf(mx[0], p.x); mx[1] = fmaxf(mx[1], p.y); mx[2] = fmaxf(mx[2], p.z);
+            mr = fmaxf(mr, p.w);
+        }
+        for (int a = 0; a < 3; ++a) {
+            atomicMin(&red[a], ord_float(mn[a]));
+            atomicMax(&red[3 + a], ord_float(mx[a]));
+        }
+        atomicMax(&red[6], ord_float(mr));
+    }
+    T.sync();
+    GridDims g;
+    g.minx = unord_float(red[0]); g.miny = unord_float(red[1]); g.minz = unord_float(red[2]);
+    const float ex = unord_float(red[3]) - g.minx, ey = unord_float(red[4]) - g.miny,
+                ez = unord_float(red[5]) - g.minz;
+    const float R = unord_float(red[6]);
+    const int nbig = T.sh->nbig;
+    T.sync();   // red[] and the count are read by every thread before they are reused
+    if (!(ex >= 0.f && ey >= 0.f && ez >= 0.f) || !(ex < 1e30f && ey < 1e30f && ez < 1e30f) || !(R < 1e30f) ||
+        !(rbig < 1e30f) || nbig > kGridMaxBig)
+        return -1;   // nothing small, non-finite extents or many big bodies: the all-pairs loop
+    // at most n / 2 cells, so the cell table fits beside the items
+    const int maxcell = max(1, n / 2);
+    float h = fmaxf(2.f * R * 1.0001f, 1e-6f);
+    for (int it = 0; it < 64; ++it) {
+        g.nx = (int)(ex / h) + 1; g.ny = (int)(ey / h) + 1; g.nz = (int)(ez / h) + 1;
+        if ((long long)g.nx * g.ny * g.nz <= maxcell) break;
+        h *= 1.25f;
+    }
+    if ((long long)g.nx * g.ny * g.nz > maxcell) return -1;
+    g.inv_h = 1.f / h;
+    const int ncell = g.nx * g.ny * g.nz;
+    // shared layout after the staged poses: int cstart[ncell + 1], ushort items[n]
+    const size_t used = sp ? (size_t)n * sizeof(float4) : 0;
+    const size_t need = (size_t)(ncell + 1) * sizeof(int) + (size_t)n * sizeof(unsigned short);
+    const bool in_smem = used + need <= (size_t)T.stage_cap * sizeof(float4) && n < 65536;
+    int* cstart = in_smem ? reinterpret_cast<int*>(reinterpret_cast<char*>(T.stage) + used) : W.bcur + b0;
+    unsigned short* items16 = in_smem ? reinterpret_cast<unsigned short*>(cstart + ncell + 1) : nullptr;
+    int* items32 = W.cntB + b0;
+    int* rank = W.cand_off + b0;   // a body's rank within its cell
+    for (int c = tid; c <= ncell; c += nt) cstart[c] = 0;
+    T.sync();
+    for (int li = tid; li < n; li += nt) {
+        const float4 p = body_sphere(W, sc, sp, li);
+        if (isinf(p.w) || p.w > rbig) continue;
+        rank[li] = atomicAdd(&cstart[g.cell(p)], 1);
+    }
+    T.sync();
+    const int placed = block_exclusive_scan(T, cstart, cstart, ncell);
+    if (tid == 0) cstart[ncell] = placed;
+    for (int li = tid; li < n; li += nt) {
+        const float4 p = body_sphere(W, sc, sp, li);
+        if (isinf(p.w) || p.w > rbig) continue;
+        const int k = cstart[g.cell(p)] + rank[li];
+        if (in_smem) items16[k] = (unsigned short)li;
+        else items32[k] = li;
+    }
+    T.sync();
+    GridCells gc;
+    gc.cstart = cstart;
+    gc.items16 = in_smem ? items16 : nullptr;
+    gc.items32 = items32;
+    gc.big = big;
+    gc.nbig = nbig;
+    gc.rbig = rbig;
+    for (int li = tid; li < n; li += nt)
+        W.cand_cnt[b0 + li] = grid_candidates<false>(W, sc, sp, g, gc, li, nullptr);
+    T.sync();
+    const int ncand = block_exclusive_scan(T, W.cand_cnt + b0, W.cand_off + b0, n);
+    if (ncand > sc.candcap) return ncand;
+    for (int li = tid; li < n; li += nt)
+        grid_candidates<true>(W, sc, sp, g, gc, li, W.cpair[cur] + sc.cand0 + W.cand_off[b0 + li]);
+    T.sync();
+    return ncand;
+}
+
+// ---------------------------------------------------------------------------
 // Whole step of one scene by one team (batched path).
 // ---------------------------------------------------------------------------
 __device__ void scene_step(const World& W, int scene, const Team& T) {
@@ -641,19 +853,25 @@ __device__ void scene_step(const World& W, int scene, const Team& T) {
         }
         T.sync();
     }
-    for (int b = b0 + tid; b < b1; b += nt)
-        W.cand_cnt[b] = staged ? broadphase_body_staged(W, sc, b, s_bodies, nullptr, 0)
-                               : broadphase_body(W, sc, b, nullptr, 0);
-    T.sync();
-    const int ncand = block_exclusive_scan(T, W.cand_cnt + b0, W.cand_off + b0, sc.nbody);
+    int ncand = (W.grid_min > 0 && sc.nbody >= W.grid_min) ? broadphase_grid(T, W, sc, cur, staged ? s_bodies : nullptr)
+                                                             : -1;
+    if (ncand < 0) {
+        for (int b = b0 + tid; b < b1; b += nt)
+            W.cand_cnt[b] = staged ? broadphase_body_staged(W, sc, b, s_bodies, nullptr, 0)
+                                   : broadphase_body(W, sc, b, nullptr, 0);
+        T.sync();
+        ncand = block_exclusive_scan(T, W.cand_cnt + b0, W.cand_off + b0, sc.nbody);
+        if (ncand <= sc.candcap) {
+            for (int b = b0 + tid; b < b1; b += nt) {
+                int2* out = W.cpair[cur] + sc.cand0 + W.cand_off[b];
+                if (staged) broadphase_body_staged(W, sc, b, s_bodies, out, W.cand_cnt[b]);
+                else broadphase_body(W, sc, b, out, W.cand_cnt[b]);
+            }
+        }
+    }
     if (ncand > sc.candcap) {
         if (tid == 0) { st->status = kStatusCapacity; st->need_cand = ncand; }
         return;
-    }
-    for (int b = b0 + tid; b < b1; b += nt) {
-        int2* out = W.cpair[cur] + sc.cand0 + W.cand_off[b];
-        if (staged) broadphase_body_staged(W, sc, b, s_bodies, out, W.cand_cnt[b]);
-        else broadphase_body(W, sc, b, out, W.cand_cnt[b]);
     }
     if (tid == 0) { st->kused[cur] = 0; st->nlive[cur] = 0; st->nmatched = 0; }
     T.sync();

@@ -335,6 +335,10 @@ class Batch:
         share a CTA with others (0: one scene per CTA); before stepping."""
         check(self._lib.avbd_batch_set_team_work(self._h, int(units_per_lane)), "set_team_work")
 
+    def set_grid_broadphase(self, min_bodies=128):
+        """Scenes of at least min_bodies use the grid broadphase (0: all-pairs)."""
+        check(self._lib.avbd_batch_set_grid_broadphase(self._h, int(min_bodies)), "set_grid_broadphase")
+
     def set_kernel(self, register_variant=1):
         """Build of the persistent kernel: 1..4 for CTAs of up to 256 threads
         (156, 128, 80 or 64 registers), 5/6 for 512 threads, 7 for 1024."""

@@ -141,3 +141,53 @@ def test_team_split_changes_nothing():
     for i, ((p0, q0), (p1, q1)) in enumerate(zip(*results)):
         assert np.array_equal(p0.view(np.uint32), p1.view(np.uint32)), f"scene {i}"
         assert np.array_equal(q0.view(np.uint32), q1.view(np.uint32)), f"scene {i}"
+
+
+GRID_BUILDERS = [
+    scenes.pyramid_wall,
+    lambda s: scenes.rigid_pile(s, 300, scenes.rng_for(4, 21), stack=True),
+    lambda s: scenes.rigid_pile(s, 400, scenes.rng_for(4, 22), stack=False),
+    lambda s: scenes.fem_scene(s, 700, scenes.rng_for(4, 23)),
+]
+
+
+def test_grid_broadphase_matches_oracle(oracle_mod):
+    """Scenes of 128+ bodies take the uniform-grid broadphase in the batch:
+    after the first step their contact points and colours equal the oracle's
+    (whose broadphase is the reference's all-pairs loop) and poses agree."""
+    from skyephyx_b200 import Batch
+    b = Batch()
+    keep = [staged(f) for f in GRID_BUILDERS]
+    for w in keep:
+        b.add_scene(w)
+    assert b.step(1) == "ok"
+    for i, f in enumerate(GRID_BUILDERS):
+        o = oracle_mod.OracleSolver()
+        f(o)
+        assert o.step_coloured() == 0
+        info = b.scene_info(i)
+        points = sum(len(v[0]) for v in o.contacts().values())
+        assert info["status"] == 0 and info["contacts"] == points, f"scene {i}: {info} vs {points}"
+        assert info["colours"] == o.colours()[1], f"scene {i}"
+        assert np.abs(o.get_state()[0] - b.get_state(i)[0]).max(initial=0.0) <= 1e-4, f"scene {i}"
+
+
+def test_grid_broadphase_equals_all_pairs_over_time():
+    """A collapsing pile and a settling stack, 30 steps: the batch (grid
+    broadphase) and the single-scene path (all-pairs broadphase kernels), both
+    with one lane per body, agree bit for bit."""
+    from skyephyx_b200 import Batch, Solver
+    for build in GRID_BUILDERS[1:3]:
+        w = Solver()
+        w.set_group(1)
+        build(w)
+        b = Batch()
+        b.set_groups(1, 4)
+        b.add_scene(staged(build))
+        for _ in range(30):
+            assert w.step() == "ok"
+        assert b.step(30) == "ok" and b.scene_status(0) == "ok"
+        pw, qw = w.get_state()[:2]
+        pb, qb = b.get_state(0)[:2]
+        assert np.array_equal(pw.view(np.uint32), pb.view(np.uint32))
+        assert np.array_equal(qw.view(np.uint32), qb.view(np.uint32))
