@@ -107,6 +107,11 @@ class ClockSampler:
                 "samples": len(sm)}
 
 
+# DRAM bytes (read + write) per launch per dynamic body: one ncu capture of
+# the 1,024-scene mix of this workload (5.29 GB over 432,494 dynamic bodies).
+TRAFFIC_PER_DYNAMIC_BODY = 5.288e9 / 432494
+
+
 def build_batch(specs, config_base=4, tuned=None):
     """Stages every scene and adds it to a Batch with the autotuned launch
     shape for this mix; returns (batch, staged, counts)."""
@@ -418,7 +423,9 @@ def main():
         "plain_gpu": {"value": plain_v, "unit": UNIT, "sample": f"first {len(plain_specs)} scenes, 3 steps each",
                       "batched_over_plain": value / plain_v if plain_v else None} if plain_v else None,
         "roofline": {"bound": "hbm", "achieved": achieved, "peak": peak, "unit": "GB/s", "frac": achieved / peak,
-                     "traffic": None, "peak_kind": peak_kind,
+                     "traffic": TRAFFIC_PER_DYNAMIC_BODY * counts["dynamic"],
+                     "traffic_note": "DRAM read+write bytes per launch from one ncu capture of the 1,024-scene "
+                                     "mix, scaled by dynamic bodies", "peak_kind": peak_kind,
                      "algorithmic_bytes_per_launch": alg_bytes},
         "clocks": clk,
         "served": served,
