@@ -848,6 +848,10 @@ struct AvbdBatch {
     int stage = 0;   // float4 slots of dynamic shared memory per CTA
     int team_work = 0;   // bodies + tets per lane below which a CTA team splits (0 = never)
     int grid_min = 128;  // scenes from this many bodies use the grid broadphase (0 = never)
+    std::vector<long long> steps_due;   // steps each slot's scene should have taken
+    int* d_fail = nullptr;               // scene steps stopped by a full table (device counter)
+    int* d_fix_order = nullptr;          // catch-up queue
+    int* d_fix_n = nullptr;
     float last_ms = 0.f;
 };
 
@@ -892,9 +896,16 @@ int batch_reserve(AvbdBatch* b, int64_t bodies, int64_t forces, int64_t tets, in
     if (b->d_order) cudaFree(b->d_order);
     if (b->d_nlive) cudaFree(b->d_nlive);
     if (b->d_queue) cudaFree(b->d_queue);
+    if (b->d_fail) cudaFree(b->d_fail);
+    if (b->d_fix_order) cudaFree(b->d_fix_order);
+    if (b->d_fix_n) cudaFree(b->d_fix_n);
     if (cudaMalloc(&b->d_order, std::max<int64_t>(nscenes, 1) * sizeof(int)) != cudaSuccess ||
-        cudaMalloc(&b->d_nlive, sizeof(int)) != cudaSuccess || cudaMalloc(&b->d_queue, sizeof(int)) != cudaSuccess)
+        cudaMalloc(&b->d_nlive, sizeof(int)) != cudaSuccess || cudaMalloc(&b->d_queue, sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&b->d_fail, sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&b->d_fix_order, std::max<int64_t>(nscenes, 1) * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&b->d_fix_n, sizeof(int)) != cudaSuccess)
         return AVBD_ERR_NOMEM;
+    cudaMemset(b->d_fail, 0, sizeof(int));
     cudaMemset(b->d_nlive, 0, sizeof(int));
     b->reserved = true;
     b->order_dirty = true;
@@ -915,6 +926,8 @@ int batch_admit(AvbdBatch* b, int slot) {
     upload_scene(b->P, h, static_incidence(h, reg), reg, scene_group(h, b->group_rigid, b->group_fem), slot,
                  b->descs[slot], b->stream);
     b->state[slot] = 1;
+    if ((int)b->steps_due.size() <= slot) b->steps_due.resize(slot + 1, 0);
+    b->steps_due[slot] = 0;
     b->order_dirty = true;
     return 0;
 }
@@ -974,6 +987,155 @@ int batch_launch_shape(AvbdBatch* b) {
     return 0;
 }
 
+int batch_build_graph(AvbdBatch* b);
+
+// Shifts the contact bases and live-slot entries of a relocated manifold table.
+__global__ void k_rebase_table(World W, int t, int cand0, int nslot, int nlive, int dk, int dc) {
+    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nslot; i += gridDim.x * blockDim.x) {
+        W.kbase[t][cand0 + i] += dk;
+        if (i < nlive) W.live[t][cand0 + i] += dc;
+    }
+}
+
+// Extends a pool's free ranges after the pool grew from old_cap to new_cap.
+void ranges_extend(Ranges& rg, int old_cap, int new_cap) {
+    if (new_cap <= old_cap) return;
+    rg.cap = new_cap;
+    rg.release(old_cap, new_cap - old_cap);
+}
+
+template <typename T>
+void copy_range(T* base, int to, int from, int n, cudaStream_t st) {
+    if (n > 0) cudaMemcpyAsync(base + to, base + from, (size_t)n * sizeof(T), cudaMemcpyDeviceToDevice, st);
+}
+
+// Gives a scene stopped by a full candidate, contact or incidence table larger
+// ranges (growing a pool when it has no room), moves its last completed
+// manifold table and that table's contacts there, and clears the status so
+// its step can run again.  The moved table is the one the next step warm
+// starts from; the other table only held the interrupted attempt.
+int batch_grow_scene(AvbdBatch* b, int slot, const SceneState& st) {
+    Pools& P = b->P;
+    Allocs& A = b->A;
+    Region& r = b->regions[slot];
+    SceneDesc& d = b->descs[slot];
+    const int t = st.cur;
+    const int nc = std::max(2 * r.ncand, st.need_cand + st.need_cand / 2 + 64);
+    const int nk = std::max(2 * r.nk, st.need_k + st.need_k / 2 + 128);
+    const int ni = r.nsinc + 2 * nc;
+    int c0 = A.cand.alloc(nc), k0 = A.k.alloc(nk), i0 = A.inc.alloc(ni);
+    if (c0 < 0 || k0 < 0 || i0 < 0) {
+        if (c0 >= 0) A.cand.release(c0, nc);
+        if (k0 >= 0) A.k.release(k0, nk);
+        if (i0 >= 0) A.inc.release(i0, ni);
+        // grow the pools, keeping every scene's contents
+        cudaStreamSynchronize(b->stream);
+        const int oc = P.ncand, ok = P.nk, oi = P.ninc;
+        const int gc = std::max(oc + nc, oc + oc / 2), gk = std::max(ok + nk, ok + ok / 2);
+        const int gi = std::max(oi + ni, oi + oi / 2);
+        if (P.grow_tables(gc, gk, oc, oc, ok, ok) != cudaSuccess) return AVBD_ERR_NOMEM;
+        if (P.grow(P.W.inc, (size_t)oi, (size_t)gi, (size_t)oi) != cudaSuccess) return AVBD_ERR_NOMEM;
+        P.ninc = gi;
+        ranges_extend(A.cand, oc, gc);
+        ranges_extend(A.k, ok, gk);
+        ranges_extend(A.inc, oi, gi);
+        batch_drop_graph(b);   // the graph holds the old pool pointers
+        c0 = A.cand.alloc(nc); k0 = A.k.alloc(nk); i0 = A.inc.alloc(ni);
+        if (c0 < 0 || k0 < 0 || i0 < 0) return AVBD_ERR_NOMEM;
+    }
+    World& W = P.W;
+    cudaStream_t s = b->stream;
+    const int nslot = st.ncand[t], ncont = st.kused[t];
+    copy_range(W.cpair[t], c0, r.cand0, nslot, s);
+    copy_range(W.cn[t], c0, r.cand0, nslot, s);
+    copy_range(W.cfric[t], c0, r.cand0, nslot, s);
+    copy_range(W.kbase[t], c0, r.cand0, nslot, s);
+    copy_range(W.cbirth[t], c0, r.cand0, nslot, s);
+    copy_range(W.live[t], c0, r.cand0, nslot, s);
+    copy_range(W.kid[t], k0, r.k0, ncont, s);
+    copy_range(W.krA[t], k0, r.k0, ncont, s);
+    copy_range(W.krB[t], k0, r.k0, ncont, s);
+    copy_range(W.kn[t], k0, r.k0, ncont, s);
+    copy_range(W.kt1[t], k0, r.k0, ncont, s);
+    copy_range(W.kt2[t], k0, r.k0, ncont, s);
+    copy_range(W.krAw[t], k0, r.k0, ncont, s);
+    copy_range(W.krBw[t], k0, r.k0, ncont, s);
+    copy_range(W.kpen[t], k0, r.k0, ncont, s);
+    copy_range(W.klam[t], k0, r.k0, ncont, s);
+    if (nslot > 0)
+        k_rebase_table<<<blocks_for(nslot), kThreads, 0, s>>>(W, t, c0, nslot, st.nlive[t], k0 - r.k0, c0 - r.cand0);
+    A.cand.release(r.cand0, r.ncand);
+    A.k.release(r.k0, r.nk);
+    A.inc.release(r.inc0, r.ninc);
+    r.cand0 = c0; r.ncand = nc; r.k0 = k0; r.nk = nk; r.inc0 = i0; r.ninc = ni;
+    d.cand0 = c0; d.candcap = nc; d.k0 = k0; d.kcap = nk; d.inc0 = i0; d.inccap = ni;
+    SceneState fixed = st;
+    fixed.status = kStatusOk;
+    fixed.need_cand = fixed.need_k = fixed.need_inc = 0;
+    cudaMemcpyAsync(P.d_scenes + slot, &d, sizeof(SceneDesc), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(P.d_sstate + slot, &fixed, sizeof(SceneState), cudaMemcpyHostToDevice, s);
+    cudaStreamSynchronize(s);
+    return 0;
+}
+
+// Runs one step of the listed scenes only (same kernel build and launch shape).
+int batch_step_listed(AvbdBatch* b, const std::vector<int>& slots) {
+    const int n = (int)slots.size();
+    cudaStream_t s = b->stream;
+    cudaMemcpyAsync(b->d_fix_order, slots.data(), n * sizeof(int), cudaMemcpyHostToDevice, s);
+    cudaMemcpyAsync(b->d_fix_n, &n, sizeof(int), cudaMemcpyHostToDevice, s);
+    cudaMemsetAsync(b->d_queue, 0, sizeof(int), s);
+    World W = b->P.W;
+    W.stage_bodies = b->stage;
+    W.team_work = b->team_work;
+    W.grid_min = b->grid_min;
+    W.fail_count = b->d_fail;
+    const int* order = b->d_fix_order;
+    const int* nlive = b->d_fix_n;
+    int* queue = b->d_queue;
+    void* args[] = {&W, &order, &nlive, &queue};
+    if (cudaLaunchKernel((const void*)kBatchVariants[b->variant].fn, dim3(b->grid), dim3(b->threads), args,
+                         (size_t)b->stage * sizeof(float4), s) != cudaSuccess)
+        return AVBD_ERR_CUDA;
+    return cudaStreamSynchronize(s) == cudaSuccess ? 0 : AVBD_ERR_CUDA;
+}
+
+// After a batched step: scenes a full table stopped get larger tables and
+// take the steps they missed (a few rounds, in case one growth is not enough).
+int batch_fix_capacity(AvbdBatch* b) {
+    const int nslots = (int)b->state.size();
+    std::vector<SceneState> hs(nslots);
+    for (int round = 0; round < 4; ++round) {
+        int fails = 0;
+        cudaMemcpy(&fails, b->d_fail, sizeof(int), cudaMemcpyDeviceToHost);
+        if (fails == 0) return 0;
+        cudaMemset(b->d_fail, 0, sizeof(int));
+        if (cudaMemcpy(hs.data(), b->P.d_sstate, nslots * sizeof(SceneState), cudaMemcpyDeviceToHost) != cudaSuccess)
+            return AVBD_ERR_CUDA;
+        std::vector<int> grown;
+        for (int i = 0; i < nslots; ++i) {
+            if (b->state[i] != 1 || hs[i].status != kStatusCapacity) continue;
+            if (!(hs[i].need_cand || hs[i].need_k || hs[i].need_inc)) continue;   // colour slots: not growable
+            if (batch_grow_scene(b, i, hs[i]) == 0) grown.push_back(i);
+        }
+        if (grown.empty()) return 0;
+        if (!b->graph) batch_build_graph(b);
+        // catch up: every grown scene takes the steps it missed
+        for (;;) {
+            std::vector<int> due;
+            if (cudaMemcpy(hs.data(), b->P.d_sstate, nslots * sizeof(SceneState), cudaMemcpyDeviceToHost) !=
+                cudaSuccess)
+                return AVBD_ERR_CUDA;
+            for (int i : grown)
+                if (hs[i].status == kStatusOk && hs[i].step < b->steps_due[i]) due.push_back(i);
+            if (due.empty()) break;
+            int r = batch_step_listed(b, due);
+            if (r) return r;
+        }
+    }
+    return 0;
+}
+
 int batch_build_graph(AvbdBatch* b) {
     batch_drop_graph(b);
     cudaGraph_t g;
@@ -982,6 +1144,7 @@ int batch_build_graph(AvbdBatch* b) {
     b->P.W.stage_bodies = b->stage;
     b->P.W.team_work = b->team_work;
     b->P.W.grid_min = b->grid_min;
+    b->P.W.fail_count = b->d_fail;
     const size_t smem = (size_t)b->stage * sizeof(float4);
     {
         const int* order = b->d_order;
@@ -1357,6 +1520,9 @@ int32_t avbd_batch_destroy(AvbdBatch* b) {
     if (b->d_order) cudaFree(b->d_order);
     if (b->d_nlive) cudaFree(b->d_nlive);
     if (b->d_queue) cudaFree(b->d_queue);
+    if (b->d_fail) cudaFree(b->d_fail);
+    if (b->d_fix_order) cudaFree(b->d_fix_order);
+    if (b->d_fix_n) cudaFree(b->d_fix_n);
     if (b->e0) cudaEventDestroy(b->e0);
     if (b->e1) cudaEventDestroy(b->e1);
     if (b->stream) cudaStreamDestroy(b->stream);
@@ -1431,13 +1597,18 @@ int32_t avbd_batch_step(AvbdBatch* b, int32_t steps) {
     if (!b->grid) batch_launch_shape(b);
     b->P.W.P = to_params(b->params);
     if (!b->graph && (r = batch_build_graph(b))) return r;
+    cudaMemsetAsync(b->d_fail, 0, sizeof(int), b->stream);
     cudaEventRecord(b->e0, b->stream);
     for (int i = 0; i < steps; ++i)
         if (cudaGraphLaunch(b->graph, b->stream) != cudaSuccess) return AVBD_ERR_CUDA;
     cudaEventRecord(b->e1, b->stream);
     if (cudaStreamSynchronize(b->stream) != cudaSuccess) return AVBD_ERR_CUDA;
     cudaEventElapsedTime(&b->last_ms, b->e0, b->e1);
-    return cudaGetLastError() == cudaSuccess ? AVBD_STATUS_OK : AVBD_ERR_CUDA;
+    if (cudaGetLastError() != cudaSuccess) return AVBD_ERR_CUDA;
+    for (size_t i = 0; i < b->state.size() && i < b->steps_due.size(); ++i)
+        if (b->state[i] == 1) b->steps_due[i] += steps;
+    if ((r = batch_fix_capacity(b))) return r;
+    return AVBD_STATUS_OK;
 }
 
 int32_t avbd_batch_num_scenes(const AvbdBatch* b) {

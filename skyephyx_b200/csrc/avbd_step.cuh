@@ -870,7 +870,11 @@ __device__ void scene_step(const World& W, int scene, const Team& T) {
         }
     }
     if (ncand > sc.candcap) {
-        if (tid == 0) { st->status = kStatusCapacity; st->need_cand = ncand; }
+        if (tid == 0) {
+            st->status = kStatusCapacity;
+            st->need_cand = ncand;
+            if (W.fail_count) atomicAdd(W.fail_count, 1);
+        }
         return;
     }
     if (tid == 0) { st->kused[cur] = 0; st->nlive[cur] = 0; st->nmatched = 0; }
@@ -881,7 +885,11 @@ __device__ void scene_step(const World& W, int scene, const Team& T) {
     narrowphase_cta(T, W, sc, st, cur, ncand, old_count);
     T.sync();
     if (st->need_k) {
-        if (tid == 0) { st->status = kStatusCapacity; st->need_k = st->kused[cur]; }
+        if (tid == 0) {
+            st->status = kStatusCapacity;
+            st->need_k = st->kused[cur];
+            if (W.fail_count) atomicAdd(W.fail_count, 1);
+        }
         return;
     }
     if (tid == 0) { st->ncand[cur] = ncand; st->cur = cur; }
@@ -892,7 +900,10 @@ __device__ void scene_step(const World& W, int scene, const Team& T) {
     T.sync();
     // incidence
     if (!build_incidence(T, W, sc, st, cur)) {
-        if (tid == 0) st->status = kStatusCapacity;
+        if (tid == 0) {
+            st->status = kStatusCapacity;
+            if (W.fail_count) atomicAdd(W.fail_count, 1);
+        }
         return;
     }
     AVBD_PHASE(2);

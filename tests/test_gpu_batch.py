@@ -191,3 +191,48 @@ def test_grid_broadphase_equals_all_pairs_over_time():
         pb, qb = b.get_state(0)[:2]
         assert np.array_equal(pw.view(np.uint32), pb.view(np.uint32))
         assert np.array_equal(qw.view(np.uint32), qb.view(np.uint32))
+
+
+def test_batch_grows_full_tables():
+    """A scene whose contacts outgrow its tables (a self-colliding block of
+    0.05 m particles) gets larger tables and takes the steps it missed: it
+    ends on the same step count, and bitwise on the same poses, as the
+    single-scene path, which grows its tables in place.  Its batch neighbour
+    is unaffected."""
+    from skyephyx_b200 import Batch, Solver
+    block = lambda s: scenes.fem_block(s, nx=9, ny=4, nz=4)
+    small = lambda s: scenes.pyramid_wall(s, rows=5)
+    w = Solver()
+    w.set_group(1)
+    block(w)
+    for _ in range(5):
+        assert w.step() == "ok"
+    b = Batch()
+    b.set_groups(1, 1)
+    b.add_scene(staged(block))
+    b.add_scene(staged(small))
+    assert b.step(2) == "ok"
+    assert b.step(3) == "ok"
+    for i in (0, 1):
+        info = b.scene_info(i)
+        assert info["status"] == 0 and info["steps"] == 5, f"scene {i}: {info}"
+    nbody = b.get_state(0)[0].shape[0]
+    assert b.scene_info(0)["candidates"] > 16 * nbody + 64   # beyond the first table: it did grow
+    pw, qw = w.get_state()[:2]
+    pb, qb = b.get_state(0)[:2]
+    assert np.array_equal(pw.view(np.uint32), pb.view(np.uint32))
+    assert np.array_equal(qw.view(np.uint32), qb.view(np.uint32))
+    assert same(b.get_state(1)[:2], alone_steps(small, 5))
+
+
+def same(a, b):
+    return all(np.array_equal(x.view(np.uint32), y.view(np.uint32)) for x, y in zip(a, b))
+
+
+def alone_steps(build, steps):
+    from skyephyx_b200 import Batch
+    b = Batch()
+    b.set_groups(1, 1)
+    b.add_scene(staged(build))
+    assert b.step(steps) == "ok"
+    return b.get_state(0)[:2]
