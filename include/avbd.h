@@ -124,6 +124,18 @@ int32_t avbd_make_tet_volume(AvbdWorld* w, float ox, float oy, float oz, int32_t
                              float cell_size, float youngs_modulus, float poisson_ratio, float particle_mass,
                              float friction, int32_t pin_min_x);
 
+/* Solver::RemoveBody (solver.hpp:49, solver.cpp:104-115) and Mesh::~Mesh (geometry.cpp:11-25):
+ * the body and every force and energy on it stop taking part.  Ids stay
+ * stable (the reference swap-removes and renumbers).  Valid before or after
+ * the first step. */
+int32_t avbd_remove_body(AvbdWorld* w, int32_t body);
+/* Solver::RemoveForce (solver.hpp:47): a joint or spring by force id. */
+int32_t avbd_remove_force(AvbdWorld* w, int32_t force);
+/* Solver::RemoveEnergy (solver.hpp:48): a Neo-Hookean tet or StVK triangle
+ * by the id its add call returned (the two kinds are numbered apart). */
+int32_t avbd_remove_neohookean_tet(AvbdWorld* w, int32_t tet);
+int32_t avbd_remove_stvk_tri(AvbdWorld* w, int32_t tri);
+
 /* Solver::Step() (solver.cpp:199-627) with the world's params. */
 int32_t avbd_step(AvbdWorld* w);
 /* Sets stepValue/numIterations, then steps. */

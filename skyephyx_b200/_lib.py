@@ -64,6 +64,10 @@ SIGNATURES = [
     ("avbd_add_stvk_tri", [_V, _I, C.c_float, C.c_float], C.c_int32),
     ("avbd_make_tet_volume", [_V, C.c_float, C.c_float, C.c_float, C.c_int32, C.c_int32, C.c_int32, C.c_float,
                               C.c_float, C.c_float, C.c_float, C.c_float, C.c_int32], C.c_int32),
+    ("avbd_remove_body", [_V, C.c_int32], C.c_int32),
+    ("avbd_remove_force", [_V, C.c_int32], C.c_int32),
+    ("avbd_remove_neohookean_tet", [_V, C.c_int32], C.c_int32),
+    ("avbd_remove_stvk_tri", [_V, C.c_int32], C.c_int32),
     ("avbd_step", [_V], C.c_int32),
     ("avbd_step_dt", [_V, C.c_float, C.c_int32], C.c_int32),
     ("avbd_num_bodies", [_V], C.c_int32),

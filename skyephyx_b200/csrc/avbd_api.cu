@@ -179,6 +179,30 @@ __global__ void k_remove_oob(World W) {
     }
 }
 
+// RemoveBody / RemoveForce / RemoveEnergy on an uploaded world: the same marks
+// as the out-of-bounds removal, plus a topology bump so the colouring is redone.
+// kind 0 body, 1 force, 2 tet, 3 triangle; idx is the global index.
+__global__ void k_remove_item(World W, int kind, int idx) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    if (kind == 0) {
+        W.flags[idx] |= kBodyRemoved;
+        for (int e = W.sinc_off[idx]; e < W.sinc_off[idx] + W.sinc_n[idx]; ++e) {
+            const uint32_t ent = W.sinc[e];
+            const uint32_t k = ent_kind(ent), i = ent_index(ent);
+            if (k == kEntForce) W.ftype[i] |= kForceRemoved;
+            else if (k == kEntTet) W.tparam[i].w = 1.f;
+            else if (k == kEntTri) W.rparam[i].w = 1.f;
+        }
+    } else if (kind == 1) {
+        W.ftype[idx] |= kForceRemoved;
+    } else if (kind == 2) {
+        W.tparam[idx].w = 1.f;
+    } else {
+        W.rparam[idx].w = 1.f;
+    }
+    W.sstate[0].topo += 1;
+}
+
 __global__ void k_collide(World W, int a, int b, uint32_t* ids, float* data, int* n) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
     Collision col;
@@ -1314,6 +1338,46 @@ int32_t avbd_add_stvk_tri(AvbdWorld* w, const int32_t v[3], float E, float nu) {
     int r = w->h.add_stvk_tri(v, E, nu);
     return r < 0 ? AVBD_ERR_INVALID : r;
 }
+
+// kind 0 body, 1 force, 2 tet, 3 triangle (see k_remove_item).
+static int32_t world_remove(AvbdWorld* w, int kind, int32_t id) {
+    if (!w) return AVBD_ERR_INVALID;
+    HostScene& h = w->h;
+    const int n = kind == 0 ? h.nbody() : kind == 1 ? h.nforce() : kind == 2 ? h.ntet() : h.ntri();
+    if (id < 0 || id >= n) return AVBD_ERR_INVALID;
+    if (!w->uploaded) {
+        if (kind == 0) {
+            h.flags[id] |= kBodyRemoved;
+            for (int f = 0; f < h.nforce(); ++f)
+                if (h.fbody[f].x == id || h.fbody[f].y == id) h.ftype[f] |= kForceRemoved;
+            for (int t = 0; t < h.ntet(); ++t) {
+                const int4 v = h.tidx[t];
+                if (v.x == id || v.y == id || v.z == id || v.w == id) h.tparam[t].w = 1.f;
+            }
+            for (int t = 0; t < h.ntri(); ++t) {
+                const int4 v = h.ridx[t];
+                if (v.x == id || v.y == id || v.z == id) h.rparam[t].w = 1.f;
+            }
+        } else if (kind == 1) {
+            h.ftype[id] |= kForceRemoved;
+        } else if (kind == 2) {
+            h.tparam[id].w = 1.f;
+        } else {
+            h.rparam[id].w = 1.f;
+        }
+        return 0;
+    }
+    if (cudaSetDevice(w->device) != cudaSuccess) return AVBD_ERR_CUDA;
+    const SceneDesc& d = w->descs[0];
+    const int base = kind == 0 ? d.body0 : kind == 1 ? d.force0 : kind == 2 ? d.tet0 : d.tri0;
+    k_remove_item<<<1, 32, 0, w->stream>>>(w->P.W, kind, base + id);
+    return cudaStreamSynchronize(w->stream) == cudaSuccess ? 0 : AVBD_ERR_CUDA;
+}
+
+int32_t avbd_remove_body(AvbdWorld* w, int32_t body) { return world_remove(w, 0, body); }
+int32_t avbd_remove_force(AvbdWorld* w, int32_t force) { return world_remove(w, 1, force); }
+int32_t avbd_remove_neohookean_tet(AvbdWorld* w, int32_t tet) { return world_remove(w, 2, tet); }
+int32_t avbd_remove_stvk_tri(AvbdWorld* w, int32_t tri) { return world_remove(w, 3, tri); }
 
 int32_t avbd_make_tet_volume(AvbdWorld* w, float ox, float oy, float oz, int32_t nx, int32_t ny, int32_t nz,
                              float cell, float E, float nu, float pm, float friction, int32_t pin) {

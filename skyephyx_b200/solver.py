@@ -237,6 +237,19 @@ class Solver:
                                              counts.ctypes.data_as(ip)), "collide_noalloc")
         return ids, data, counts
 
+    def remove_body(self, body: int):
+        """Solver::RemoveBody: the body and its forces and energies stop taking part (ids stay stable)."""
+        check(self._lib.avbd_remove_body(self._h, int(body)), "remove_body")
+
+    def remove_force(self, force: int):
+        """Solver::RemoveForce for a joint or spring id."""
+        check(self._lib.avbd_remove_force(self._h, int(force)), "remove_force")
+
+    def remove_energy(self, energy: int, kind: str = "tet"):
+        """Solver::RemoveEnergy for a Neo-Hookean tet ("tet") or StVK triangle ("tri") id."""
+        fn = self._lib.avbd_remove_neohookean_tet if kind == "tet" else self._lib.avbd_remove_stvk_tri
+        check(fn(self._h, int(energy)), "remove_energy")
+
     def set_group(self, group=0):
         """Lanes per body in the primal sweep (0 = by scene kind); before the first step."""
         check(self._lib.avbd_set_group(self._h, int(group)), "set_group")

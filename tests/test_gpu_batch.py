@@ -211,13 +211,16 @@ def test_batch_grows_full_tables():
     b.set_groups(1, 1)
     b.add_scene(staged(block))
     b.add_scene(staged(small))
-    assert b.step(2) == "ok"
+    assert b.step(1) == "ok"
+    nbody = b.get_state(0)[0].shape[0]
+    first = b.scene_info(0)
+    # more candidates than the scene's first table holds: it did grow
+    assert first["steps"] == 1 and first["candidates"] > 16 * nbody + 64, first
+    assert b.step(1) == "ok"
     assert b.step(3) == "ok"
     for i in (0, 1):
         info = b.scene_info(i)
         assert info["status"] == 0 and info["steps"] == 5, f"scene {i}: {info}"
-    nbody = b.get_state(0)[0].shape[0]
-    assert b.scene_info(0)["candidates"] > 16 * nbody + 64   # beyond the first table: it did grow
     pw, qw = w.get_state()[:2]
     pb, qb = b.get_state(0)[:2]
     assert np.array_equal(pw.view(np.uint32), pb.view(np.uint32))

@@ -172,3 +172,64 @@ def test_colouring_reuse_is_exact(Solver):
         ref = greedy_colours(n, static, edges)
         assert np.array_equal(col, ref), f"step {k + 1}"
         assert ncol == (ref.max() + 1 if (ref >= 0).any() else 0)
+
+
+def facade_scene_py(s):
+    """The scene of tests/cpp/facade_scene.cpp, through the Python API."""
+    s.add_body(0, 1.0, 0.5, (0.0, -0.5, 0.0), (20.0, 1.0, 20.0), is_static=True)
+    prev = -1
+    for i in range(4):
+        b = s.add_body(0, 1000.0, 0.5, (0.125 * i, 0.5 + 1.0 * i, 0.0), (1.0, 1.0, 1.0), vel=(0.0, 0.0, 0.25 * i))
+        if prev >= 0 and i == 3:
+            s.add_joint(prev, (0.0, 0.5, 0.0), b, (0.0, -0.5, 0.0))
+        prev = b
+    spring = s.add_spring(-1, (3.0, 5.0, 0.0), prev, (0.0, 0.0, 0.0), 1000.0)
+    s.add_spring(-1, (-3.0, 5.0, 0.0), prev, (0.0, 0.0, 0.0), 500.0)
+    s.remove_force(spring)
+    s.make_tet_volume(4.0, 1.0, 0.0, 3, 2, 2, 0.5, 1e4, 0.3, 1.0, 0.5, True)
+
+
+def test_cpp_facade_matches_python(Solver, tmp_path):
+    """A program on the C++ facade (avbd::Solver, the reference's method
+    names) and the Python API build the same scene, with a force removed
+    before the first step, and reach the same poses bit for bit."""
+    import os
+    import shutil
+    import subprocess
+    from skyephyx_b200 import build
+    lib = build.build()
+    gxx = shutil.which("g++")
+    if not gxx:
+        pytest.skip("no g++")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    exe = tmp_path / "facade_scene"
+    subprocess.run([gxx, "-std=c++17", "-O1", "-I", os.path.join(root, "include"),
+                    os.path.join(root, "tests", "cpp", "facade_scene.cpp"), "-L", os.path.dirname(lib), "-lavbd",
+                    "-Wl,-rpath," + os.path.dirname(lib), "-o", str(exe)], check=True)
+    out = subprocess.run([str(exe)], capture_output=True, text=True, check=True).stdout.split()
+    got = np.array([int(x, 16) for x in out], np.uint32).reshape(-1, 7)
+    g = Solver()
+    facade_scene_py(g)
+    for _ in range(5):
+        assert g.step() == "ok"
+    p, q = g.get_state()[:2]
+    ref = np.concatenate([p.view(np.uint32), q.view(np.uint32)], axis=1)
+    assert np.array_equal(got, ref)
+
+
+def test_remove_body_mid_run(Solver):
+    """RemoveBody after the first steps: the body stops (its pose is kept),
+    its manifolds go, and the rest of the scene steps on."""
+    g = Solver()
+    scenes.level_pyramid(g)
+    for _ in range(3):
+        assert g.step() == "ok"
+    top = g.num_bodies - 1
+    g.remove_body(top)
+    kept = g.get_state()[0][top].copy()
+    for _ in range(5):
+        assert g.step() == "ok"
+    p = g.get_state()[0]
+    assert np.array_equal(p[top], kept)
+    assert all(top not in pair for pair in g.contacts())
+    assert np.isfinite(p).all()

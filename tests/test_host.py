@@ -162,3 +162,21 @@ def test_max_over_ranks_gloo(tmp_path):
     assert all(p.returncode == 0 for p in procs)
     vals = [float(line.split()[2]) for o in outs for line in o.splitlines() if line.startswith("MAX")]
     assert vals == [11.0, 11.0]
+
+
+def test_cpp_facade_compiles_and_links(tmp_path):
+    """include/avbd.hpp (the C++ facade with the reference Solver's method
+    names) compiles against include/avbd.h and links against the library."""
+    import shutil
+    import subprocess
+    from skyephyx_b200 import build
+    lib = build.build()
+    gxx = shutil.which("g++")
+    if not gxx:
+        pytest.skip("no g++")
+    root = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+    out = tmp_path / "facade_scene"
+    cmd = [gxx, "-std=c++17", "-O1", "-I", os.path.join(root, "include"), os.path.join(root, "tests", "cpp", "facade_scene.cpp"),
+           "-L", os.path.dirname(lib), "-lavbd", "-Wl,-rpath," + os.path.dirname(lib), "-o", str(out)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
