@@ -22,6 +22,7 @@ from __future__ import annotations
 
 import argparse
 import json
+import math
 import os
 import subprocess
 import sys
@@ -187,6 +188,64 @@ def run_plain_sample(specs, steps, warmup):
     return total_iters / total_s, total_iters, total_s
 
 
+CONFIG_SCENES = {
+    "C1 pyramid wall (210 boxes)": lambda s: __import__("skyephyx_b200.scenes", fromlist=["x"]).pyramid_wall(s),
+    "C2 Neo-Hookean block (41x11x11, 20,000 tets, 0.05 m)":
+        lambda s: __import__("skyephyx_b200.scenes", fromlist=["x"]).fem_block(s),
+    "C3 large mixed (32,768 boxes, 64x32 hinge chains, 2,048 springs)":
+        lambda s: __import__("skyephyx_b200.scenes", fromlist=["x"]).mixed_large(s),
+}
+
+
+def rot_err(qa, qb):
+    """Angle of the rotation between two (w, x, y, z) quaternions, per body
+    (2 atan2(|v|, |w|) of qa* qb: well conditioned near zero)."""
+    qa = qa.astype(np.float64)
+    qb = qb.astype(np.float64)
+    w = qa[:, 0] * qb[:, 0] + np.sum(qa[:, 1:] * qb[:, 1:], axis=1)
+    v = qa[:, 0:1] * qb[:, 1:] - qb[:, 0:1] * qa[:, 1:] - np.cross(qa[:, 1:], qb[:, 1:])
+    return 2.0 * np.arctan2(np.linalg.norm(v, axis=1), np.abs(w))
+
+
+def plain_configs(steps=5):
+    """Each reference config as one scene on the single-scene GPU path:
+    body-iters/s over `steps` steps after one, the max position / rotation
+    error after that first step against the colour-ordered oracle, and the
+    reference's own sequential Step() on one host core (SURVEY config timing)."""
+    from oracle import oracle
+    from skyephyx_b200 import Solver
+    out = {}
+    for name, build in CONFIG_SCENES.items():
+        s = Solver(iterations=ITERS)
+        build(s)
+        status = s.step()
+        pg, qg = s.get_state()[:2]
+        o = oracle.OracleSolver(iterations=ITERS)
+        build(o)
+        o.step_coloured()
+        po, qo = o.get_state()[:2]
+        ok = np.isfinite(po).all() and np.isfinite(pg).all()
+        pos_err = float(np.abs(po - pg).max()) if ok else None
+        rot = float(rot_err(qo, qg).max()) if ok else None
+        t0 = time.perf_counter()
+        for _ in range(steps):
+            status = s.step()
+        dt = time.perf_counter() - t0
+        ndyn = s.num_dynamic
+        s.close()
+        c = oracle.OracleSolver(iterations=ITERS, fast=True)
+        build(c)
+        t1 = time.perf_counter()
+        c.step()
+        cpu_s = time.perf_counter() - t1
+        out[name] = {"plain_gpu": ndyn * ITERS * steps / dt, "ms_per_step": dt * 1e3 / steps,
+                     "dynamic_bodies": ndyn, "status": status,
+                     "step1_max_pos_err_m": pos_err, "step1_max_rot_err_rad": rot,
+                     "cpu_reference_1core": ndyn * ITERS / cpu_s, "cpu_ms_per_step": cpu_s * 1e3,
+                     "unit": UNIT}
+    return out
+
+
 def cpu_baseline(specs, steps, threads):
     """The reference step (oracle build of the reference sources, Release-like flags) on host threads."""
     from oracle import oracle
@@ -203,22 +262,52 @@ def cpu_baseline(specs, steps, threads):
     return dyn * ITERS * steps / (ms / 1e3), dyn, ms
 
 
+def serve_sizes(n, seed):
+    """Box counts of the served requests, log-uniform 8..2,048 like the batched mix."""
+    rng = np.random.default_rng(seed)
+    return [int(math.exp(rng.uniform(math.log(8), math.log(2048)))) for _ in range(n)]
+
+
+def serve_replay(sizes, fraction=0.01, seed_base=0x5EED0005):
+    """Step 1 of a sampled `fraction` of the served requests on the GPU against
+    the colour-ordered oracle: the max position and rotation error."""
+    from oracle import oracle
+    from skyephyx_b200 import Solver, scenes
+    picks = list(range(0, len(sizes), max(1, int(round(1.0 / fraction)))))
+    pos_err = rot = 0.0
+    for i in picks:
+        g = Solver(iterations=ITERS)
+        scenes.served_scene(g, sizes[i], seed_base + i)
+        g.step()
+        o = oracle.OracleSolver(iterations=ITERS)
+        scenes.served_scene(o, sizes[i], seed_base + i)
+        o.step_coloured()
+        pg, qg = g.get_state()[:2]
+        po, qo = o.get_state()[:2]
+        g.close()
+        pos_err = max(pos_err, float(np.abs(pg - po).max()))
+        rot = max(rot, float(rot_err(qg, qo).max()))
+    return {"requests": len(picks), "step1_max_pos_err_m": pos_err, "step1_max_rot_err_rad": rot}
+
+
 def serve_bench(rate, window, cap_s, budget_gb, launch=None, seed_base=0x5EED0005):
     """Continuous batching at `rate` Poisson arrivals/s for `window` s: each
-    request is a seeded scene of the batched mix simulated for U{60..600}
-    steps; admission by free pool space in an HBM budget.  Returns throughput
-    and arrival-to-completion latency of the requests completed within
-    `window + cap_s` seconds, plus the backlog left."""
+    request is a seeded scene of the batched mix's size composed like the
+    large mixed scene (boxes in a container, one hinge link and one spring
+    per 16 boxes), simulated for U{60..600} steps; admission by free pool
+    space in an HBM budget.  Returns throughput and arrival-to-completion
+    latency of the requests completed within `window + cap_s` seconds, the
+    backlog left, and a 1% step-1 replay against the oracle."""
     from skyephyx_b200 import Solver, scenes
     from skyephyx_b200.serve import Request, Server, poisson_arrivals
     arrivals = poisson_arrivals(rate, window, seed=seed_base)
     rng = np.random.default_rng(seed_base + 1)
-    specs = scenes.batch_mix_specs(n_scenes=len(arrivals), config=5)
+    sizes = serve_sizes(len(arrivals), seed_base + 2)
     srv = Server(budget_bytes=int(budget_gb * (1 << 30)), max_scenes=16384, launch=launch, keep_results=False)
     t_build = time.perf_counter()
-    for i, (t, sp) in enumerate(zip(arrivals, specs)):
+    for i, (t, n) in enumerate(zip(arrivals, sizes)):
         s = Solver(iterations=ITERS)
-        scenes.build_spec(s, sp, config=5)
+        scenes.served_scene(s, n, seed_base + i)
         srv.submit(Request(rid=i, scene=s, steps=int(rng.integers(60, 601)), arrival=t))
     build_s = time.perf_counter() - t_build
     srv.start()
@@ -231,7 +320,9 @@ def serve_bench(rate, window, cap_s, budget_gb, launch=None, seed_base=0x5EED000
             "scenes_per_s": st.get("completed", 0) / elapsed, "body_iters_per_s": srv.body_iters / elapsed,
             "p50_s": st.get("p50_s"), "p99_s": st.get("p99_s"), "ticks": srv.ticks, "elapsed_s": elapsed,
             "keeps_up": backlog == 0 and elapsed <= window + 5.0, "budget_gb": budget_gb,
-            "build_s": build_s}
+            "build_s": build_s, "workload": "requests: box counts log-uniform 8-2048 in a container, one hinge "
+                                            "link and one spring per 16 boxes, U{60..600} steps",
+            "replay": serve_replay(sizes, seed_base=seed_base)}
 
 
 def dist_env():
@@ -286,6 +377,7 @@ def main():
     ap.add_argument("--cpu-scenes", type=int, default=128)
     ap.add_argument("--no-cpu", action="store_true")
     ap.add_argument("--no-serve", action="store_true")
+    ap.add_argument("--no-configs", action="store_true")
     ap.add_argument("--serve-only", action="store_true")
     ap.add_argument("--serve-rate", type=float, default=2000.0)
     ap.add_argument("--serve-window", type=float, default=3.0)
@@ -385,6 +477,8 @@ def main():
     plain_specs = specs[: args.plain_scenes]
     plain_v = run_plain_sample(plain_specs, steps=3, warmup=1)[0] if plain_specs else None
 
+    configs = None if (args.no_configs or ws > 1) else plain_configs()
+
     cpu = None
     if not args.no_cpu:
         cpu_specs = specs[: args.cpu_scenes]
@@ -430,6 +524,7 @@ def main():
         "clocks": clk,
         "served": served,
         "cpu_baseline": cpu,
+        "configs": configs,
         "status_counts": bad,
         "build_s": build_s,
         "wall_ms_per_step": wall * 1e3 / args.steps,

@@ -92,18 +92,18 @@ def fem_block(s, nx=41, ny=11, nz=11, cell=0.05, E=1e5, nu=0.3, density=1000.0, 
     return s.make_tet_volume(origin[0], origin[1], origin[2], nx, ny, nz, cell, E, nu, pm, friction, pin)
 
 
-def mixed_large(s, n_boxes=32768, n_chains=64, links=32, n_springs=2048, seed_scene=0):
+def mixed_large(s, n_boxes=32768, n_chains=64, links=32, n_springs=2048, seed_scene=0, nxz=50, config=3):
     """Plain large mixed rigid scene: `n_boxes` boxes with edges U[0.5, 1.5] m on
-    a jittered lattice inside a 5-static-box container, `n_chains` hinge chains
-    of `links` links anchored in the world, `n_springs` springs between random
-    box pairs (k log-uniform [1e2, 1e5] N/m, rest = initial distance)."""
-    rng = rng_for(3, seed_scene)
+    a jittered lattice (`nxz` x `nxz` per layer) inside a 5-static-box
+    container, `n_chains` hinge chains of `links` links anchored in the world,
+    `n_springs` springs between random box pairs (k log-uniform [1e2, 1e5]
+    N/m, rest = initial distance)."""
+    rng = rng_for(config, seed_scene)
     # container: floor 84 x 1 x 84 (top at y = 0) + 4 walls 1 x 30 x 84
     s.add_body(CUBE, 1.0, 0.5, v3(0, -0.5, 0), v3(84, 1, 84), is_static=True)
     for (x, z, sx, sz) in ((-42.5, 0, 1, 84), (42.5, 0, 1, 84), (0, -42.5, 84, 1), (0, 42.5, 84, 1)):
         s.add_body(CUBE, 1.0, 0.5, v3(x, 15, z), v3(sx, 30, sz), is_static=True)
     pitch = 1.6
-    nxz = 50
     idx = np.arange(n_boxes)
     i, k, j = idx % nxz, (idx // nxz) % nxz, idx // (nxz * nxz)
     edge = rng.uniform(0.5, 1.5, (n_boxes, 3))
@@ -130,6 +130,16 @@ def mixed_large(s, n_boxes=32768, n_chains=64, links=32, n_springs=2048, seed_sc
         k = 10.0 ** rng.uniform(2.0, 5.0)
         s.add_spring(boxes[a], v3(0, 0, 0), boxes[b], v3(0, 0, 0), k, -1.0, False)
     return boxes
+
+
+def served_scene(s, n_boxes, seed):
+    """A served request: a scene of the batched mix's size composed like the
+    large mixed scene: boxes in the container on a compact lattice (about 8
+    layers), plus one world-anchored hinge link and one spring per 16 boxes."""
+    nxz = max(2, int(math.ceil(math.sqrt(n_boxes / 8.0))))
+    per = max(1, n_boxes // 16)
+    return mixed_large(s, n_boxes=n_boxes, n_chains=per, links=1, n_springs=per, seed_scene=seed, nxz=nxz,
+                       config=5)
 
 
 def rigid_pile(s, n_boxes, rng, stack=True):
