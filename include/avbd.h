@@ -153,6 +153,18 @@ int32_t avbd_get_state(AvbdWorld* w, float* pos, float* quat_wxyz, float* vel, f
 int32_t avbd_set_state(AvbdWorld* w, const float* pos, const float* quat_wxyz, const float* vel,
                        const float* omega);
 
+/* Snapshot / restore of a stepped world (device-resident state, byte for
+ * byte: bodies, forces, energies, both manifold tables and their contacts,
+ * colour lists, counters).  No counterpart in the reference.  The buffer may
+ * be host or device memory (copies use unified addressing); size it with
+ * avbd_snapshot_bytes.  avbd_restore takes a snapshot of the same world, or
+ * of a world built the same way, whose tables have not grown since: then the
+ * next steps repeat bit for bit (deterministic replay, pre-emption).  Returns
+ * AVBD_ERR_STATE before the first step or when the table sizes differ. */
+int64_t avbd_snapshot_bytes(const AvbdWorld* w);
+int32_t avbd_snapshot(AvbdWorld* w, void* dst, int64_t bytes);
+int32_t avbd_restore(AvbdWorld* w, const void* src, int64_t bytes);
+
 /* Live contact manifolds after the last step (parity introspection).
  * Returns the count; fills up to max entries: pairs (A,B) body ids, counts,
  * ids (8 per manifold, unused = 0xFFFFFFFF) and data (8 x 16 floats per

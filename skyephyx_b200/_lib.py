@@ -68,6 +68,9 @@ SIGNATURES = [
     ("avbd_remove_force", [_V, C.c_int32], C.c_int32),
     ("avbd_remove_neohookean_tet", [_V, C.c_int32], C.c_int32),
     ("avbd_remove_stvk_tri", [_V, C.c_int32], C.c_int32),
+    ("avbd_snapshot_bytes", [_V], C.c_int64),
+    ("avbd_snapshot", [_V, _V, C.c_int64], C.c_int32),
+    ("avbd_restore", [_V, _V, C.c_int64], C.c_int32),
     ("avbd_step", [_V], C.c_int32),
     ("avbd_step_dt", [_V, C.c_float, C.c_int32], C.c_int32),
     ("avbd_num_bodies", [_V], C.c_int32),

@@ -303,6 +303,7 @@ struct Pools {
     int nb = 0, nf = 0, nt = 0, nr = 0, ns = 0;
     int ncand = 0, nk = 0, ninc = 0, nsinc = 0, nsp = 0;
     std::vector<void*> owned;
+    std::vector<size_t> owned_bytes;   // size of each owned allocation (snapshots)
     SceneDesc* d_scenes = nullptr;
     SceneState* d_sstate = nullptr;
 
@@ -310,6 +311,7 @@ struct Pools {
     void release() {
         for (void* p : owned) cudaFree(p);
         owned.clear();
+        owned_bytes.clear();
         W = World{};
     }
     template <typename T>
@@ -319,6 +321,7 @@ struct Pools {
         if (e != cudaSuccess) return e;
         cudaMemset(q, 0, std::max<size_t>(n, 1) * sizeof(T));
         owned.push_back(q);
+        owned_bytes.push_back(std::max<size_t>(n, 1) * sizeof(T));
         p = static_cast<T*>(q);
         return cudaSuccess;
     }
@@ -331,7 +334,11 @@ struct Pools {
     }
     void forget(void* p) {
         auto it = std::find(owned.begin(), owned.end(), p);
-        if (it != owned.end()) { cudaFree(p); owned.erase(it); }
+        if (it != owned.end()) {
+            cudaFree(p);
+            owned_bytes.erase(owned_bytes.begin() + (it - owned.begin()));
+            owned.erase(it);
+        }
     }
 
     cudaError_t allocate_all() {
@@ -1337,6 +1344,83 @@ int32_t avbd_add_stvk_tri(AvbdWorld* w, const int32_t v[3], float E, float nu) {
     if (!v) return AVBD_ERR_INVALID;
     int r = w->h.add_stvk_tri(v, E, nu);
     return r < 0 ? AVBD_ERR_INVALID : r;
+}
+
+// ---- snapshot / restore of a stepped world: every device allocation of the
+// world byte for byte (bodies, forces, energies, both manifold tables and
+// their contacts, incidence, colour lists and counters) after a header. ----
+struct SnapshotHeader {
+    uint32_t magic;     // 'AVSN'
+    uint32_t version;
+    int32_t nalloc;
+    int32_t stopped;
+    int64_t total;
+};
+constexpr uint32_t kSnapshotMagic = 0x4e535641u;
+
+static int64_t snapshot_bytes(const AvbdWorld* w) {
+    int64_t n = sizeof(SnapshotHeader) + (int64_t)w->P.owned_bytes.size() * sizeof(int64_t);
+    for (size_t b : w->P.owned_bytes) n += (int64_t)b;
+    return n;
+}
+
+int64_t avbd_snapshot_bytes(const AvbdWorld* w) {
+    if (!w) return AVBD_ERR_INVALID;
+    if (!w->uploaded) return AVBD_ERR_STATE;
+    return snapshot_bytes(w);
+}
+
+int32_t avbd_snapshot(AvbdWorld* w, void* dst, int64_t bytes) {
+    if (!w || !dst) return AVBD_ERR_INVALID;
+    if (!w->uploaded) return AVBD_ERR_STATE;
+    if (bytes < snapshot_bytes(w)) return AVBD_ERR_INVALID;
+    if (cudaSetDevice(w->device) != cudaSuccess) return AVBD_ERR_CUDA;
+    const Pools& P = w->P;
+    std::vector<char> head(sizeof(SnapshotHeader) + P.owned_bytes.size() * sizeof(int64_t));
+    SnapshotHeader h{kSnapshotMagic, 1u, (int32_t)P.owned.size(), w->stopped ? 1 : 0, snapshot_bytes(w)};
+    std::memcpy(head.data(), &h, sizeof(h));
+    for (size_t i = 0; i < P.owned_bytes.size(); ++i) {
+        const int64_t b = (int64_t)P.owned_bytes[i];
+        std::memcpy(head.data() + sizeof(h) + i * sizeof(int64_t), &b, sizeof(b));
+    }
+    char* out = static_cast<char*>(dst);
+    if (cudaMemcpyAsync(out, head.data(), head.size(), cudaMemcpyDefault, w->stream) != cudaSuccess)
+        return AVBD_ERR_CUDA;
+    size_t off = head.size();
+    for (size_t i = 0; i < P.owned.size(); ++i) {
+        if (cudaMemcpyAsync(out + off, P.owned[i], P.owned_bytes[i], cudaMemcpyDefault, w->stream) != cudaSuccess)
+            return AVBD_ERR_CUDA;
+        off += P.owned_bytes[i];
+    }
+    return cudaStreamSynchronize(w->stream) == cudaSuccess ? 0 : AVBD_ERR_CUDA;
+}
+
+int32_t avbd_restore(AvbdWorld* w, const void* src, int64_t bytes) {
+    if (!w || !src) return AVBD_ERR_INVALID;
+    if (!w->uploaded) return AVBD_ERR_STATE;
+    if (cudaSetDevice(w->device) != cudaSuccess) return AVBD_ERR_CUDA;
+    Pools& P = w->P;
+    const char* in = static_cast<const char*>(src);
+    SnapshotHeader h{};
+    if (bytes < (int64_t)sizeof(h)) return AVBD_ERR_INVALID;
+    if (cudaMemcpy(&h, in, sizeof(h), cudaMemcpyDefault) != cudaSuccess) return AVBD_ERR_CUDA;
+    if (h.magic != kSnapshotMagic || h.version != 1u || bytes < h.total) return AVBD_ERR_INVALID;
+    // the world's tables must have the sizes they had when the snapshot was taken
+    if (h.nalloc != (int32_t)P.owned.size() || h.total != snapshot_bytes(w)) return AVBD_ERR_STATE;
+    std::vector<int64_t> sizes(h.nalloc);
+    if (cudaMemcpy(sizes.data(), in + sizeof(h), sizes.size() * sizeof(int64_t), cudaMemcpyDefault) != cudaSuccess)
+        return AVBD_ERR_CUDA;
+    for (size_t i = 0; i < sizes.size(); ++i)
+        if (sizes[i] != (int64_t)P.owned_bytes[i]) return AVBD_ERR_STATE;
+    size_t off = sizeof(h) + sizes.size() * sizeof(int64_t);
+    for (size_t i = 0; i < P.owned.size(); ++i) {
+        if (cudaMemcpyAsync(P.owned[i], in + off, P.owned_bytes[i], cudaMemcpyDefault, w->stream) != cudaSuccess)
+            return AVBD_ERR_CUDA;
+        off += P.owned_bytes[i];
+    }
+    if (cudaStreamSynchronize(w->stream) != cudaSuccess) return AVBD_ERR_CUDA;
+    w->stopped = h.stopped != 0;
+    return sync_state(w);
 }
 
 // kind 0 body, 1 force, 2 tet, 3 triangle (see k_remove_item).

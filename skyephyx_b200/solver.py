@@ -237,6 +237,18 @@ class Solver:
                                              counts.ctypes.data_as(ip)), "collide_noalloc")
         return ids, data, counts
 
+    def snapshot(self) -> np.ndarray:
+        """Device state of a stepped world as a host byte array (see avbd_snapshot)."""
+        n = check(self._lib.avbd_snapshot_bytes(self._h), "snapshot_bytes")
+        buf = np.empty(n, np.uint8)
+        check(self._lib.avbd_snapshot(self._h, buf.ctypes.data, n), "snapshot")
+        return buf
+
+    def restore(self, buf: np.ndarray):
+        """Puts back a snapshot taken from this world (or one built the same way)."""
+        buf = np.ascontiguousarray(buf, dtype=np.uint8)
+        check(self._lib.avbd_restore(self._h, buf.ctypes.data, buf.size), "restore")
+
     def remove_body(self, body: int):
         """Solver::RemoveBody: the body and its forces and energies stop taking part (ids stay stable)."""
         check(self._lib.avbd_remove_body(self._h, int(body)), "remove_body")
