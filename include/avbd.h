@@ -118,6 +118,16 @@ int32_t avbd_add_joint(AvbdWorld* w, int32_t body_a, const float r_a[3], int32_t
 int32_t avbd_add_neohookean_tet(AvbdWorld* w, const int32_t v[4], float youngs_modulus, float poisson_ratio);
 /* STVKFEM triangle membrane (energy.hpp:90-92, stvkfem.cpp:5-35). Returns energy id. */
 int32_t avbd_add_stvk_tri(AvbdWorld* w, const int32_t v[3], float youngs_modulus, float poisson_ratio);
+/* St. Venant-Kirchhoff tet (no reference counterpart: the reference has the
+ * StVK triangle only, stvkfem.cpp).  Psi = mu tr(E^2) + lambda/2 tr(E)^2 with
+ * E = (F^T F - I)/2, the Neo-Hookean tet's rest data, projection modes and
+ * vertex-Hessian reconstruction; below 1% of its rest volume an element takes
+ * STVKFEM's isotropic penalty.  Shares the tet id space. Returns the tet id. */
+int32_t avbd_add_stvk_tet(AvbdWorld* w, const int32_t v[4], float youngs_modulus, float poisson_ratio);
+/* makeTetVolume's particles and tets (geometry.cpp:30-94) with StVK tets. */
+int32_t avbd_make_stvk_tet_volume(AvbdWorld* w, float ox, float oy, float oz, int32_t nx, int32_t ny, int32_t nz,
+                                  float cell_size, float youngs_modulus, float poisson_ratio, float particle_mass,
+                                  float friction, int32_t pin_min_x);
 /* GeometryHelpers::makeTetVolume (geometry.cpp:30-94): nx*ny*nz particles,
  * 5 Neo-Hookean tets per hex. Returns the id of the first particle. */
 int32_t avbd_make_tet_volume(AvbdWorld* w, float ox, float oy, float oz, int32_t nx, int32_t ny, int32_t nz,

@@ -462,6 +462,110 @@ int orc_add_nh_tet(void* h, const int* v, float E, float nu) {
     return (int)o->energies.size() - 1;
 }
 
+// St. Venant-Kirchhoff tet: no counterpart in the reference (which has the StVK
+// triangle only).  Restated here from the energy Psi = mu tr(E^2) +
+// lambda/2 tr(E)^2, E = (F^T F - I)/2, on the reference's own machinery: the
+// rest data exactly as the NeoHookeanFEM constructor (neohookeanfem.cpp:5-37),
+// NeoHookeanMath::svd / ProjectEigenvalues / ReconstructVertexHessian
+// (math.cpp), and the principal-stretch eigen-system of StVK: scaling block
+// d2psi/ds_i ds_j of psi = mu/4 sum (s_i^2 - 1)^2 + lambda/8 (sum s_i^2 - 3)^2
+// and twist / flip eigenvalues (psi_i +- psi_j)/(s_i +- s_j) in closed form,
+// ordered as NeoHookeanMath::ComputeEnergyHessian orders its own.  An element
+// below 1% of its rest volume takes STVKFEM's isotropic penalty
+// (stvkfem.cpp:75-86).  Parity against a reference implementation is unpinned.
+struct StvkTetEnergy : Energy {
+    Mesh *body0, *body1, *body2, *body3;
+    float restVolume, lameMu, lameLambda;
+    Eigen::Matrix3f DmInv;
+    Eigen::Vector3f gradN0, gradN1, gradN2, gradN3;
+    float trustRegionThreshold = 0.01f;
+
+    StvkTetEnergy(Solver* solver, Mesh* b0, Mesh* b1, Mesh* b2, Mesh* b3, float E, float nu)
+        : Energy(solver, {b0, b1, b2, b3}), body0(b0), body1(b1), body2(b2), body3(b3) {
+        lameMu = E / (2.f * (1.f + nu));
+        lameLambda = E * nu / ((1.f + nu) * (1.f - 2.f * nu));
+        const Eigen::Vector3f p0 = b0->transform.GetPosition(), p1 = b1->transform.GetPosition();
+        const Eigen::Vector3f p2 = b2->transform.GetPosition(), p3 = b3->transform.GetPosition();
+        Eigen::Matrix3f Dm;
+        Dm.col(0) = p1 - p0;
+        Dm.col(1) = p2 - p0;
+        Dm.col(2) = p3 - p0;
+        DmInv = Dm.inverse();
+        restVolume = std::abs(Dm.determinant()) / 6.f;
+        const Eigen::Matrix3f DmInvT = DmInv.transpose();
+        gradN1 = DmInvT.col(0);
+        gradN2 = DmInvT.col(1);
+        gradN3 = DmInvT.col(2);
+        gradN0 = -gradN1 - gradN2 - gradN3;
+    }
+    bool Initialize() override { return true; }
+    int numBodies() const override { return 4; }
+    void AddLineData(std::vector<GPULineData>&) const override {}
+    void AddDebugPointData(std::vector<GPUDebugPointData>&) const override {}
+
+    void ComputeEnergyTerms(Mesh* mesh, EigenProjectionMode projectionMode, float trustRegionRho) override {
+        using namespace NeoHookeanMath;
+        const Eigen::Vector3f p0 = body0->transform.GetPosition(), p1 = body1->transform.GetPosition();
+        const Eigen::Vector3f p2 = body2->transform.GetPosition(), p3 = body3->transform.GetPosition();
+        const Eigen::Matrix3f F = DeformationGradient(p0, p1, p2, p3, DmInv);
+        const float J = F.determinant();
+        Eigen::Vector3f gradN = gradN0;
+        if (mesh == body1) gradN = gradN1;
+        else if (mesh == body2) gradN = gradN2;
+        else if (mesh == body3) gradN = gradN3;
+        grad.setZero();
+        hess.setZero();
+        if (J < 0.01f) {
+            const float stiff = lameMu + lameLambda;
+            grad.head<3>() = restVolume * ((stiff * F) * gradN);
+            hess.block<3, 3>(0, 0) = restVolume * stiff * Eigen::Matrix3f::Identity();
+            return;
+        }
+        const Eigen::Matrix3f E = 0.5f * (F.transpose() * F - Eigen::Matrix3f::Identity());
+        const Eigen::Matrix3f S = 2.f * lameMu * E + lameLambda * E.trace() * Eigen::Matrix3f::Identity();
+        const Eigen::Matrix3f P = F * S;
+        grad.head<3>() = P * gradN * restVolume;
+
+        const SVDDecomposition d = svd(F);
+        const float s0 = d.S(0), s1 = d.S(1), s2 = d.S(2);
+        const float q0 = s0 * s0, q1 = s1 * s1, q2 = s2 * s2;
+        const float mu = lameMu, lam = lameLambda;
+        const float c = 0.5f * lam * (q0 + q1 + q2 - 3.f);
+        HessianDecomposition h{};
+        h.eigenValues[3] = mu * (q0 - s0 * s1 + q1 - 1.f) + c;   // twist (0,1)
+        h.eigenValues[4] = mu * (q0 - s0 * s2 + q2 - 1.f) + c;   // twist (0,2)
+        h.eigenValues[5] = mu * (q1 - s1 * s2 + q2 - 1.f) + c;   // twist (1,2)
+        h.eigenValues[6] = mu * (q0 + s0 * s1 + q1 - 1.f) + c;   // flip (0,1)
+        h.eigenValues[7] = mu * (q0 + s0 * s2 + q2 - 1.f) + c;   // flip (0,2)
+        h.eigenValues[8] = mu * (q1 + s1 * s2 + q2 - 1.f) + c;   // flip (1,2)
+        Eigen::Matrix3f a;
+        a(0, 0) = mu * (3.f * q0 - 1.f) + c + lam * q0;
+        a(1, 1) = mu * (3.f * q1 - 1.f) + c + lam * q1;
+        a(2, 2) = mu * (3.f * q2 - 1.f) + c + lam * q2;
+        a(0, 1) = a(1, 0) = lam * s0 * s1;
+        a(0, 2) = a(2, 0) = lam * s0 * s2;
+        a(1, 2) = a(2, 1) = lam * s1 * s2;
+        Eigen::SelfAdjointEigenSolver<Eigen::Matrix3f> es(a);
+        for (int k = 0; k < 3; ++k) {
+            h.eigenValues[k] = es.eigenvalues()(k);
+            h.scalingVectors[k] = es.eigenvectors().col(k);
+        }
+        float proj[9];
+        for (int i = 0; i < 9; ++i) proj[i] = h.eigenValues[i];
+        ProjectEigenvalues(proj, 9, projectionMode, trustRegionRho, trustRegionThreshold);
+        hess.block<3, 3>(0, 0) = ReconstructVertexHessian(d, h, proj, gradN, restVolume);
+    }
+};
+
+int orc_add_stvk_tet(void* h, const int* v, float E, float nu) {
+    Orc* o = static_cast<Orc*>(h);
+    Mesh* b[4];
+    for (int i = 0; i < 4; ++i) if (!(b[i] = body_or_null(o, v[i]))) return -1;
+    Energy* e = o->solver.AddEnergy(std::make_unique<StvkTetEnergy>(&o->solver, b[0], b[1], b[2], b[3], E, nu));
+    o->energies.push_back(e);
+    return (int)o->energies.size() - 1;
+}
+
 // STVKFEM triangle membrane (energy.hpp:90-92, stvkfem.cpp:5-35).
 int orc_add_stvk_tri(void* h, const int* v, float E, float nu) {
     Orc* o = static_cast<Orc*>(h);
@@ -485,6 +589,28 @@ int orc_make_tet_volume(void* h, float ox, float oy, float oz, int nx, int ny, i
     for (size_t i = b0; i < o->solver.solverBodies.size(); ++i) o->bodies.push_back(o->solver.solverBodies[i].get());
     for (size_t i = e0; i < o->solver.solverEnergies.size(); ++i)
         o->energies.push_back(o->solver.solverEnergies[i].get());
+    return first;
+}
+
+// makeTetVolume's particles and tets (geometry.cpp:30-94) with StVK tets: the
+// reference builds the volume with Neo-Hookean tets, which are then replaced,
+// in creation order, by StVK tets on the same bodies.
+int orc_make_stvk_tet_volume(void* h, float ox, float oy, float oz, int nx, int ny, int nz, float cell, float E,
+                             float nu, float particle_mass, float friction, int pin_min_x) {
+    Orc* o = static_cast<Orc*>(h);
+    const size_t e0 = o->solver.solverEnergies.size();
+    const int first = orc_make_tet_volume(h, ox, oy, oz, nx, ny, nz, cell, E, nu, particle_mass, friction, pin_min_x);
+    std::vector<NeoHookeanFEM*> made;
+    for (size_t i = e0; i < o->solver.solverEnergies.size(); ++i)
+        made.push_back(static_cast<NeoHookeanFEM*>(o->solver.solverEnergies[i].get()));
+    const size_t k0 = o->energies.size() - made.size();
+    o->energies.resize(k0);
+    for (NeoHookeanFEM* nh : made) {
+        Mesh* b[4] = {nh->body0, nh->body1, nh->body2, nh->body3};
+        o->solver.RemoveEnergy(nh);
+        o->energies.push_back(o->solver.AddEnergy(std::make_unique<StvkTetEnergy>(&o->solver, b[0], b[1], b[2], b[3],
+                                                                                  E, nu)));
+    }
     return first;
 }
 

@@ -60,6 +60,9 @@ def _lib(fast: bool = False):
         "orc_add_stvk_tri": ([vp, ip, C.c_float, C.c_float], C.c_int),
         "orc_make_tet_volume": ([vp, C.c_float, C.c_float, C.c_float, C.c_int, C.c_int, C.c_int, C.c_float,
                                  C.c_float, C.c_float, C.c_float, C.c_float, C.c_int], C.c_int),
+        "orc_make_stvk_tet_volume": ([vp, C.c_float, C.c_float, C.c_float, C.c_int, C.c_int, C.c_int, C.c_float,
+                                      C.c_float, C.c_float, C.c_float, C.c_float, C.c_int], C.c_int),
+        "orc_add_stvk_tet": ([vp, ip, C.c_float, C.c_float], C.c_int),
         "orc_step": ([vp], C.c_int),
         "orc_step_coloured": ([vp, C.c_int], C.c_int),
         "orc_step_many": ([C.POINTER(vp), C.c_int, C.c_int, C.c_int, C.c_int], C.c_double),
@@ -160,6 +163,16 @@ class OracleSolver:
     def add_stvk_tri(self, v, E, nu):
         iv = (C.c_int * 3)(*[int(x) for x in v])
         return self._lib.orc_add_stvk_tri(self._h, iv, float(E), float(nu))
+
+    def add_stvk_tet(self, v, E, nu):
+        iv = (C.c_int * 4)(*[int(x) for x in v])
+        return self._lib.orc_add_stvk_tet(self._h, iv, float(E), float(nu))
+
+    def make_stvk_tet_volume(self, ox, oy, oz, nx, ny, nz, cell, E, nu, particle_mass=1.0, friction=0.5,
+                             pin_min_x=False):
+        return self._lib.orc_make_stvk_tet_volume(self._h, float(ox), float(oy), float(oz), int(nx), int(ny),
+                                                  int(nz), float(cell), float(E), float(nu), float(particle_mass),
+                                                  float(friction), int(bool(pin_min_x)))
 
     def make_tet_volume(self, ox, oy, oz, nx, ny, nz, cell, E, nu, particle_mass=1.0, friction=0.5,
                         pin_min_x=False):

@@ -64,6 +64,9 @@ SIGNATURES = [
     ("avbd_add_stvk_tri", [_V, _I, C.c_float, C.c_float], C.c_int32),
     ("avbd_make_tet_volume", [_V, C.c_float, C.c_float, C.c_float, C.c_int32, C.c_int32, C.c_int32, C.c_float,
                               C.c_float, C.c_float, C.c_float, C.c_float, C.c_int32], C.c_int32),
+    ("avbd_make_stvk_tet_volume", [_V, C.c_float, C.c_float, C.c_float, C.c_int32, C.c_int32, C.c_int32, C.c_float,
+                              C.c_float, C.c_float, C.c_float, C.c_float, C.c_int32], C.c_int32),
+    ("avbd_add_stvk_tet", [_V, _I, C.c_float, C.c_float], C.c_int32),
     ("avbd_remove_body", [_V, C.c_int32], C.c_int32),
     ("avbd_remove_force", [_V, C.c_int32], C.c_int32),
     ("avbd_remove_neohookean_tet", [_V, C.c_int32], C.c_int32),

@@ -365,7 +365,7 @@ struct Pools {
         A(alloc(W.fk, 6 * (size_t)nf)); A(alloc(W.ffrac, 6 * (size_t)nf)); A(alloc(W.ffmin, 6 * (size_t)nf));
         A(alloc(W.ffmax, 6 * (size_t)nf)); A(alloc(W.fpen, 6 * (size_t)nf)); A(alloc(W.flam, 6 * (size_t)nf));
         A(alloc(W.tidx, nt)); A(alloc(W.tDmInv, 9 * (size_t)nt)); A(alloc(W.tgradN, 12 * (size_t)nt));
-        A(alloc(W.tparam, nt)); A(alloc(W.fterm, 4 * (size_t)nt));
+        A(alloc(W.tparam, nt)); A(alloc(W.fterm, 4 * (size_t)nt)); A(alloc(W.tkind, nt));
         A(alloc(W.ridx, nr)); A(alloc(W.rDmInv, nr)); A(alloc(W.rgradN, 6 * (size_t)nr)); A(alloc(W.rparam, nr));
         A(alloc(W.inc, ninc));
         for (int t = 0; t < 2; ++t) A(alloc_tables(t, ncand, nk));
@@ -588,6 +588,7 @@ void upload_scene(Pools& P, const HostScene& h, const StaticInc& si, const Regio
     for (auto& t : ti) { t.x += d.body0; t.y += d.body0; t.z += d.body0; t.w += d.body0; }
     put(W.tidx, ti, d.tet0, st); put(W.tDmInv, h.tDmInv, 9 * (size_t)d.tet0, st);
     put(W.tgradN, h.tgradN, 12 * (size_t)d.tet0, st); put(W.tparam, h.tparam, d.tet0, st);
+    put(W.tkind, h.tkind, d.tet0, st);
     std::vector<int4> ri = h.ridx;
     for (auto& t : ri) { t.x += d.body0; t.y += d.body0; t.z += d.body0; }
     put(W.ridx, ri, d.tri0, st); put(W.rDmInv, h.rDmInv, d.tri0, st);
@@ -1463,6 +1464,20 @@ int32_t avbd_remove_force(AvbdWorld* w, int32_t force) { return world_remove(w, 
 int32_t avbd_remove_neohookean_tet(AvbdWorld* w, int32_t tet) { return world_remove(w, 2, tet); }
 int32_t avbd_remove_stvk_tri(AvbdWorld* w, int32_t tri) { return world_remove(w, 3, tri); }
 
+int32_t avbd_add_stvk_tet(AvbdWorld* w, const int32_t v[4], float E, float nu) {
+    AVBD_STAGING_ONLY(w);
+    if (!v) return AVBD_ERR_INVALID;
+    int r = w->h.add_stvk_tet(v, E, nu);
+    return r < 0 ? AVBD_ERR_INVALID : r;
+}
+
+int32_t avbd_make_stvk_tet_volume(AvbdWorld* w, float ox, float oy, float oz, int32_t nx, int32_t ny, int32_t nz,
+                                  float cell, float E, float nu, float pm, float friction, int32_t pin) {
+    AVBD_STAGING_ONLY(w);
+    int r = w->h.make_tet_volume(ox, oy, oz, nx, ny, nz, cell, E, nu, pm, friction, pin != 0, kTetStvk);
+    return r < 0 ? AVBD_ERR_INVALID : r;
+}
+
 int32_t avbd_make_tet_volume(AvbdWorld* w, float ox, float oy, float oz, int32_t nx, int32_t ny, int32_t nz,
                              float cell, float E, float nu, float pm, float friction, int32_t pin) {
     AVBD_STAGING_ONLY(w);
@@ -1852,7 +1867,7 @@ constexpr int64_t kBytesPerBody = 15 * 16 + 18 * 4;        // float4 state + per
 constexpr int64_t kBytesPerCand = 2 * (8 + 4 + 4 + 4 + 4 + 4);  // two manifold tables
 constexpr int64_t kBytesPerContact = 2 * (4 + 9 * 16);      // two contact pools
 constexpr int64_t kBytesPerForce = 4 + 8 + 6 * 16 + 6 * 6 * 4;
-constexpr int64_t kBytesPerTet = 16 + 36 + 48 + 16 + 16;
+constexpr int64_t kBytesPerTet = 16 + 36 + 48 + 16 + 16 + 4;
 constexpr int64_t kBytesPerTri = 16 + 16 + 24 + 16;
 
 int64_t avbd_scene_footprint_bytes(const AvbdWorld* w) {

@@ -53,6 +53,10 @@ constexpr int kMaxColours = 1024;     // colour slots per scene
 constexpr int kColourWorkBuckets = 16; // work classes used to order bodies within a colour
 constexpr int kGroupFlat = 64;         // SceneDesc::group of scenes swept term-per-lane (AVBD_GROUP_FLAT)
 
+// tet energy models
+constexpr int kTetNeoHookean = 0;      // NeoHookeanFEM (neohookeanfem.cpp)
+constexpr int kTetStvk = 1;            // St. Venant-Kirchhoff tet (no reference counterpart)
+
 // body flags
 constexpr int kBodyStatic = 1;
 constexpr int kBodyParticle = 2;
@@ -219,6 +223,7 @@ struct World {
     float* tDmInv;      // 9 per tet, column-major
     float* tgradN;      // 12 per tet: gradN0..3
     float4* tparam;     // restVolume, mu, lambda
+    int* tkind;         // energy model of each tet (kTetNeoHookean, kTetStvk)
 
     // ---- StVK triangles ----
     int4* ridx;

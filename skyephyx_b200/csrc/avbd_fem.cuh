@@ -189,6 +189,59 @@ AVBD_HD void s3_add_outer(S3& h, float lam, V3 w) {
     h.xy += lam * (w.y * w.x); h.xz += lam * (w.z * w.x); h.yz += lam * (w.z * w.y);
 }
 
+// Vertex block of the projected Hessian from a decomposition F = U S V^T
+// (NeoHookeanMath::ReconstructVertexHessian, math.cpp:196-231): the scaling
+// block a.. (3x3, symmetric) and the twist / flip eigenvalues ev[3..8]
+// (ev[0..2] are filled here), each mode contracted with V^T gradN.
+AVBD_HD void vertex_hessian(const M3& U, const M3& V, V3 gradN, float a00, float a11, float a22, float a01, float a02,
+                            float a12, float (&ev)[9], int mode, float rho, float restVolume, S3& H) {
+    const float vg0 = dot(V.c[0], gradN), vg1 = dot(V.c[1], gradN), vg2 = dot(V.c[2], gradN);
+    s3_zero(H);
+    // Scaling modes: sum_k proj(lam_k) w_k w_k^T = M proj(A) M^T with M = [vg0 u0, vg1 u1, vg2 u2]
+    // (math.cpp:196-202).  When A is positive definite (all Cholesky pivots > 0) both ABSOLUTE and
+    // CLAMP projections leave it unchanged up to the 1e-6 floor, so proj(A) = A needs no eigensolve.
+    const float piv0 = a00;
+    const float l10 = a01 / piv0, l20 = a02 / piv0;
+    const float piv1 = a11 - l10 * a01;
+    const float l21 = (a12 - l20 * a01) / piv1;
+    const float piv2 = a22 - l20 * a02 - l21 * l21 * piv1;
+    if (piv0 > 0.f && piv1 > 0.f && piv2 > 0.f) {
+        const V3 m0 = vg0 * U.c[0], m1 = vg1 * U.c[1], m2 = vg2 * U.c[2];
+        // B = M A (columns), H += B M^T
+        const V3 b0 = a00 * m0 + a01 * m1 + a02 * m2;
+        const V3 b1 = a01 * m0 + a11 * m1 + a12 * m2;
+        const V3 b2 = a02 * m0 + a12 * m1 + a22 * m2;
+        H.xx += b0.x * m0.x + b1.x * m1.x + b2.x * m2.x;
+        H.yy += b0.y * m0.y + b1.y * m1.y + b2.y * m2.y;
+        H.zz += b0.z * m0.z + b1.z * m1.z + b2.z * m2.z;
+        H.xy += b0.y * m0.x + b1.y * m1.x + b2.y * m2.x;
+        H.xz += b0.z * m0.x + b1.z * m1.x + b2.z * m2.x;
+        H.yz += b0.z * m0.y + b1.z * m1.y + b2.z * m2.y;
+        project_eigenvalues(ev + 3, 6, mode, rho);
+    } else {
+        V3 w;
+        M3 Q;
+        eig3(a00, a11, a22, a01, a02, a12, w, Q);
+        ev[0] = w.x; ev[1] = w.y; ev[2] = w.z;
+        project_eigenvalues(ev, 9, mode, rho);
+#pragma unroll
+        for (int k = 0; k < 3; ++k) {
+            V3 c = Q.c[k];
+            V3 ww = (c.x * vg0) * U.c[0] + (c.y * vg1) * U.c[1] + (c.z * vg2) * U.c[2];
+            s3_add_outer(H, ev[k], ww);
+        }
+    }
+    const float is2 = 0.70710678118f;
+    s3_add_outer(H, ev[3], is2 * (vg1 * U.c[0] - vg0 * U.c[1]));
+    s3_add_outer(H, ev[4], is2 * (vg2 * U.c[0] - vg0 * U.c[2]));
+    s3_add_outer(H, ev[5], is2 * (vg2 * U.c[1] - vg1 * U.c[2]));
+    s3_add_outer(H, ev[6], is2 * (vg1 * U.c[0] + vg0 * U.c[1]));
+    s3_add_outer(H, ev[7], is2 * (vg2 * U.c[0] + vg0 * U.c[2]));
+    s3_add_outer(H, ev[8], is2 * (vg2 * U.c[1] + vg1 * U.c[2]));
+    H.xx *= restVolume; H.yy *= restVolume; H.zz *= restVolume;
+    H.xy *= restVolume; H.xz *= restVolume; H.yz *= restVolume;
+}
+
 // NeoHookeanFEM::ComputeEnergyTerms for vertex `role` of the tet
 // (neohookeanfem.cpp:40-83, HandleInvertedElement :86-110).
 AVBD_HD void neohookean_terms(V3 p0, V3 p1, V3 p2, V3 p3, const float* DmInv, V3 gradN, float restVolume, float mu,
@@ -238,51 +291,73 @@ AVBD_HD void neohookean_terms(V3 p0, V3 p1, V3 p2, V3 p3, const float* DmInv, V3
     // scaling block A (math.cpp:112-119)
     const float a00 = mu + diagExtra / (s0 * s0), a11 = mu + diagExtra / (s1 * s1), a22 = mu + diagExtra / (s2 * s2);
     const float a01 = lambda * s2 / J, a02 = lambda * s1 / J, a12 = lambda * s0 / J;
-    const float vg0 = dot(V.c[0], gradN), vg1 = dot(V.c[1], gradN), vg2 = dot(V.c[2], gradN);
-    s3_zero(H);
-    // Scaling modes: sum_k proj(lam_k) w_k w_k^T = M proj(A) M^T with M = [vg0 u0, vg1 u1, vg2 u2]
-    // (math.cpp:196-202).  When A is positive definite (all Cholesky pivots > 0) both ABSOLUTE and
-    // CLAMP projections leave it unchanged up to the 1e-6 floor, so proj(A) = A needs no eigensolve.
-    const float piv0 = a00;
-    const float l10 = a01 / piv0, l20 = a02 / piv0;
-    const float piv1 = a11 - l10 * a01;
-    const float l21 = (a12 - l20 * a01) / piv1;
-    const float piv2 = a22 - l20 * a02 - l21 * l21 * piv1;
-    if (piv0 > 0.f && piv1 > 0.f && piv2 > 0.f) {
-        const V3 m0 = vg0 * U.c[0], m1 = vg1 * U.c[1], m2 = vg2 * U.c[2];
-        // B = M A (columns), H += B M^T
-        const V3 b0 = a00 * m0 + a01 * m1 + a02 * m2;
-        const V3 b1 = a01 * m0 + a11 * m1 + a12 * m2;
-        const V3 b2 = a02 * m0 + a12 * m1 + a22 * m2;
-        H.xx += b0.x * m0.x + b1.x * m1.x + b2.x * m2.x;
-        H.yy += b0.y * m0.y + b1.y * m1.y + b2.y * m2.y;
-        H.zz += b0.z * m0.z + b1.z * m1.z + b2.z * m2.z;
-        H.xy += b0.y * m0.x + b1.y * m1.x + b2.y * m2.x;
-        H.xz += b0.z * m0.x + b1.z * m1.x + b2.z * m2.x;
-        H.yz += b0.z * m0.y + b1.z * m1.y + b2.z * m2.y;
-        project_eigenvalues(ev + 3, 6, mode, rho);
-    } else {
-        V3 w;
-        M3 Q;
-        eig3(a00, a11, a22, a01, a02, a12, w, Q);
-        ev[0] = w.x; ev[1] = w.y; ev[2] = w.z;
-        project_eigenvalues(ev, 9, mode, rho);
+    vertex_hessian(U, V, gradN, a00, a11, a22, a01, a02, a12, ev, mode, rho, restVolume, H);
+}
+
+// St. Venant-Kirchhoff tet, vertex `role` (no reference counterpart; restated
+// from the StVK energy Psi = mu tr(E^2) + lambda/2 tr(E)^2, E = (F^T F - I)/2,
+// in the style of NeoHookeanFEM / STVKFEM).  Principal-stretch form
+// psi = mu/4 sum (s_i^2 - 1)^2 + lambda/8 (sum s_i^2 - 3)^2 gives the scaling
+// block d2psi/ds_i ds_j and the twist / flip eigenvalues (psi_i +- psi_j) /
+// (s_i +- s_j) in closed form; projection and reconstruction are the
+// Neo-Hookean ones.  An element below 1% of its rest volume takes the
+// isotropic penalty of STVKFEM::HandleInvertedElement (stvkfem.cpp:75-86).
+AVBD_HD void stvk_tet_terms(V3 p0, V3 p1, V3 p2, V3 p3, const float* DmInv, V3 gradN, float restVolume, float mu,
+                            float lambda, int mode, float rho, V3& grad, S3& H) {
+    M3 Ds;
+    Ds.c[0] = p1 - p0; Ds.c[1] = p2 - p0; Ds.c[2] = p3 - p0;
+    M3 F;
+#pragma unroll
+    for (int j = 0; j < 3; ++j)
+        F.c[j] = Ds.c[0] * DmInv[3 * j + 0] + Ds.c[1] * DmInv[3 * j + 1] + Ds.c[2] * DmInv[3 * j + 2];
+    const float J = det3(F);
+    if (J < 0.01f) {
+        const float stiff = mu + lambda;
+        grad = (restVolume * stiff) * matvec(F, gradN);
+        const float d = restVolume * stiff;
+        H.xx = d; H.yy = d; H.zz = d; H.xy = 0.f; H.xz = 0.f; H.yz = 0.f;
+        return;
+    }
+    // E = (F^T F - I) / 2, P = F (2 mu E + lambda tr(E) I)
+    float C[3][3];
+#pragma unroll
+    for (int i = 0; i < 3; ++i)
+#pragma unroll
+        for (int j = 0; j < 3; ++j) C[i][j] = dot(F.c[i], F.c[j]);
+    const float trE = 0.5f * (C[0][0] + C[1][1] + C[2][2] - 3.f);
+    M3 P;
+#pragma unroll
+    for (int j = 0; j < 3; ++j) {
+        V3 col = v3(0.f, 0.f, 0.f);
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            V3 c = Q.c[k];
-            V3 ww = (c.x * vg0) * U.c[0] + (c.y * vg1) * U.c[1] + (c.z * vg2) * U.c[2];
-            s3_add_outer(H, ev[k], ww);
+            const float Ekj = 0.5f * (C[k][j] - (k == j ? 1.f : 0.f));
+            const float Skj = 2.f * mu * Ekj + (k == j ? lambda * trE : 0.f);
+            col = col + F.c[k] * Skj;
         }
+        P.c[j] = col;
     }
-    const float is2 = 0.70710678118f;
-    s3_add_outer(H, ev[3], is2 * (vg1 * U.c[0] - vg0 * U.c[1]));
-    s3_add_outer(H, ev[4], is2 * (vg2 * U.c[0] - vg0 * U.c[2]));
-    s3_add_outer(H, ev[5], is2 * (vg2 * U.c[1] - vg1 * U.c[2]));
-    s3_add_outer(H, ev[6], is2 * (vg1 * U.c[0] + vg0 * U.c[1]));
-    s3_add_outer(H, ev[7], is2 * (vg2 * U.c[0] + vg0 * U.c[2]));
-    s3_add_outer(H, ev[8], is2 * (vg2 * U.c[1] + vg1 * U.c[2]));
-    H.xx *= restVolume; H.yy *= restVolume; H.zz *= restVolume;
-    H.xy *= restVolume; H.xz *= restVolume; H.yz *= restVolume;
+    grad = matvec(P, gradN) * restVolume;
+
+    M3 U, V;
+    V3 S;
+    svd3(F, U, S, V);
+    const float s0 = S.x, s1 = S.y, s2 = S.z;
+    const float q0 = s0 * s0, q1 = s1 * s1, q2 = s2 * s2;
+    const float c = 0.5f * lambda * (q0 + q1 + q2 - 3.f);
+    float ev[9];
+    ev[0] = ev[1] = ev[2] = 0.f;
+    ev[3] = mu * (q0 - s0 * s1 + q1 - 1.f) + c;   // twist (0,1)
+    ev[4] = mu * (q0 - s0 * s2 + q2 - 1.f) + c;   // twist (0,2)
+    ev[5] = mu * (q1 - s1 * s2 + q2 - 1.f) + c;   // twist (1,2)
+    ev[6] = mu * (q0 + s0 * s1 + q1 - 1.f) + c;   // flip (0,1)
+    ev[7] = mu * (q0 + s0 * s2 + q2 - 1.f) + c;   // flip (0,2)
+    ev[8] = mu * (q1 + s1 * s2 + q2 - 1.f) + c;   // flip (1,2)
+    const float a00 = mu * (3.f * q0 - 1.f) + c + lambda * q0;
+    const float a11 = mu * (3.f * q1 - 1.f) + c + lambda * q1;
+    const float a22 = mu * (3.f * q2 - 1.f) + c + lambda * q2;
+    const float a01 = lambda * s0 * s1, a02 = lambda * s0 * s2, a12 = lambda * s1 * s2;
+    vertex_hessian(U, V, gradN, a00, a11, a22, a01, a02, a12, ev, mode, rho, restVolume, H);
 }
 
 // STVKFEM::ComputeEnergyTerms for vertex `role` of the triangle

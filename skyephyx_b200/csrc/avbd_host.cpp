@@ -200,7 +200,16 @@ int HostScene::add_nh_tet(const int* v, float E, float nu) {
     for (int k = 0; k < 4; ++k)
         for (int i = 0; i < 3; ++i) tgradN.push_back(g[k][i]);
     tparam.push_back(mk4(restVolume, mu, lam, 0.f));
+    tkind.push_back(kTetNeoHookean);
     return ntet() - 1;
+}
+
+// St. Venant-Kirchhoff tet: the same rest-shape data as the Neo-Hookean tet
+// (Dm^-1, rest volume, shape gradients, Lame parameters); only the energy differs.
+int HostScene::add_stvk_tet(const int* v, float E, float nu) {
+    const int t = add_nh_tet(v, E, nu);
+    if (t >= 0) tkind.back() = kTetStvk;
+    return t;
 }
 
 int HostScene::add_stvk_tri(const int* v, float E, float nu) {
@@ -234,7 +243,7 @@ int HostScene::add_stvk_tri(const int* v, float E, float nu) {
 }
 
 int HostScene::make_tet_volume(float ox, float oy, float oz, int nx, int ny, int nz, float cell, float E, float nu,
-                               float pm, float fr, bool pin_min_x) {
+                               float pm, float fr, bool pin_min_x, int model) {
     if (nx < 2 || ny < 2 || nz < 2) return -1;
     const int first = nbody();
     std::vector<int> parts((size_t)nx * ny * nz);
@@ -258,11 +267,10 @@ int HostScene::make_tet_volume(float ox, float oy, float oz, int nx, int ny, int
                 const int t2[4] = {v[5], v[1], v[4], v[7]};
                 const int t3[4] = {v[6], v[4], v[2], v[7]};
                 const int t4[4] = {v[1], v[2], v[4], v[7]};
-                add_nh_tet(t0, E, nu);
-                add_nh_tet(t1, E, nu);
-                add_nh_tet(t2, E, nu);
-                add_nh_tet(t3, E, nu);
-                add_nh_tet(t4, E, nu);
+                for (const int* t : {t0, t1, t2, t3, t4}) {
+                    if (model == kTetStvk) add_stvk_tet(t, E, nu);
+                    else add_nh_tet(t, E, nu);
+                }
             }
     return first;
 }

@@ -29,6 +29,7 @@ struct HostScene {
     std::vector<int4> tidx;
     std::vector<float> tDmInv, tgradN;
     std::vector<float4> tparam;
+    std::vector<int> tkind;   // kTetNeoHookean or kTetStvk
     // StVK triangles
     std::vector<int4> ridx;
     std::vector<float4> rDmInv;
@@ -53,9 +54,10 @@ struct HostScene {
     int add_spring(int a, const float* rA, int b, const float* rB, float k, float rest, bool rope, float fracture);
     int add_joint(int a, const float* rA, int b, const float* rB, const float* k, const float* fracture);
     int add_nh_tet(const int* v, float E, float nu);
+    int add_stvk_tet(const int* v, float E, float nu);
     int add_stvk_tri(const int* v, float E, float nu);
     int make_tet_volume(float ox, float oy, float oz, int nx, int ny, int nz, float cell, float E, float nu,
-                        float particle_mass, float friction_, bool pin_min_x);
+                        float particle_mass, float friction_, bool pin_min_x, int model = kTetNeoHookean);
 
     // Static incidence (forces then energies per body) and joint/spring partner
     // lists.  Offsets are relative to the scene's own entry / partner arrays;

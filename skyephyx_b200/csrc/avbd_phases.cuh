@@ -736,15 +736,19 @@ AVBD_HD void sys_zero(Sys6& s) {
 }
 
 // Gradient and projected Hessian of tet `idx` for its vertex `role`
-// (NeoHookeanFEM::ComputeEnergyTerms, neohookeanfem.cpp:40-90); false for a
-// removed tet.
+// (NeoHookeanFEM::ComputeEnergyTerms, neohookeanfem.cpp:40-90, or the StVK
+// tet); false for a removed tet.
 AVBD_HD bool tet_term(const World& W, int idx, int role, V3& g, S3& H) {
     const int4 v = W.tidx[idx];
     const float4 tp = W.tparam[idx];
     if (tp.w != 0.f) return false;   // removed energy
     const float* gn = W.tgradN + (size_t)idx * 12 + role * 3;
-    neohookean_terms(v3(W.pos[v.x]), v3(W.pos[v.y]), v3(W.pos[v.z]), v3(W.pos[v.w]), W.tDmInv + (size_t)idx * 9,
-                     v3(gn[0], gn[1], gn[2]), tp.x, tp.y, tp.z, W.P.projection_mode, W.P.trust_region_rho, g, H);
+    if (W.tkind[idx] == kTetStvk)
+        stvk_tet_terms(v3(W.pos[v.x]), v3(W.pos[v.y]), v3(W.pos[v.z]), v3(W.pos[v.w]), W.tDmInv + (size_t)idx * 9,
+                       v3(gn[0], gn[1], gn[2]), tp.x, tp.y, tp.z, W.P.projection_mode, W.P.trust_region_rho, g, H);
+    else
+        neohookean_terms(v3(W.pos[v.x]), v3(W.pos[v.y]), v3(W.pos[v.z]), v3(W.pos[v.w]), W.tDmInv + (size_t)idx * 9,
+                         v3(gn[0], gn[1], gn[2]), tp.x, tp.y, tp.z, W.P.projection_mode, W.P.trust_region_rho, g, H);
     return true;
 }
 

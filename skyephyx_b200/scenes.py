@@ -132,6 +132,13 @@ def mixed_large(s, n_boxes=32768, n_chains=64, links=32, n_springs=2048, seed_sc
     return boxes
 
 
+def stvk_block(s, nx=9, ny=4, nz=4, cell=0.2, E=1e5, nu=0.3, density=1000.0, pin=True, friction=0.5):
+    """The Neo-Hookean block's particles and tets with StVK tets (config 2's
+    StVK rerun; cell 0.2 m by default so particle boxes do not touch)."""
+    pm = density * cell ** 3
+    return s.make_stvk_tet_volume(0.0, 0.0, 0.0, nx, ny, nz, cell, E, nu, pm, friction, pin)
+
+
 def served_scene(s, n_boxes, seed):
     """A served request: a scene of the batched mix's size composed like the
     large mixed scene: boxes in the container on a compact lattice (about 8

@@ -143,6 +143,19 @@ class Solver:
         iv = (C.c_int32 * 3)(*[int(x) for x in v])
         return check(self._lib.avbd_add_stvk_tri(self._h, iv, float(E), float(nu)), "add_stvk_tri")
 
+    def add_stvk_tet(self, v, E, nu):
+        """St. Venant-Kirchhoff tet (no reference counterpart). Returns the tet id."""
+        iv = (C.c_int32 * 4)(*[int(x) for x in v])
+        return check(self._lib.avbd_add_stvk_tet(self._h, iv, float(E), float(nu)), "add_stvk_tet")
+
+    def make_stvk_tet_volume(self, ox, oy, oz, nx, ny, nz, cell, E, nu, particle_mass=1.0, friction=0.5,
+                             pin_min_x=False):
+        """makeTetVolume's particles and tets with StVK tets. Returns the first particle id."""
+        return check(self._lib.avbd_make_stvk_tet_volume(self._h, float(ox), float(oy), float(oz), int(nx), int(ny),
+                                                         int(nz), float(cell), float(E), float(nu),
+                                                         float(particle_mass), float(friction), int(bool(pin_min_x))),
+                     "make_stvk_tet_volume")
+
     def make_tet_volume(self, ox, oy, oz, nx, ny, nz, cell, E, nu, particle_mass=1.0, friction=0.5,
                         pin_min_x=False):
         """GeometryHelpers::makeTetVolume (geometry.cpp:30-94). Returns the first particle id."""

@@ -86,6 +86,7 @@ FEM_BUILDERS = [
     lambda s: scenes.fem_scene(s, 1500, scenes.rng_for(4, 4)),
     fem_on_ground,
     scenes.level_soft_beam,
+    lambda s: scenes.stvk_block(s),
 ]
 
 

@@ -50,6 +50,8 @@ SCENES["fem_block_9x4x4"] = lambda s: scenes.fem_block(s, nx=9, ny=4, nz=4)
 SCENES["mixed_small"] = lambda s: scenes.mixed_large(s, n_boxes=300, n_chains=3, links=8, n_springs=40)
 SCENES["rigid_pile_64"] = lambda s: scenes.rigid_pile(s, 64, scenes.rng_for(4, 7), stack=False)
 SCENES["fem_scene_600"] = lambda s: scenes.fem_scene(s, 600, scenes.rng_for(4, 3))
+SCENES["stvk_block_9x4x4"] = lambda s: scenes.stvk_block(s)
+SCENES["stvk_beam"] = lambda s: s.make_stvk_tet_volume(-3.0, 0.0, -0.9, 9, 3, 3, 0.9, 8000.0, 0.3, 1.0, 0.5, True)
 
 
 @pytest.mark.parametrize("name", sorted(SCENES))
@@ -67,7 +69,8 @@ def test_one_step_parity(oracle_mod, Solver, name):
     assert rot_err(qo, qg).max(initial=0.0) <= ROT_TOL
 
 
-@pytest.mark.parametrize("name", ["pyramid_wall_210", "joint_playground", "cloth", "mixed_small", "soft_beam"])
+@pytest.mark.parametrize("name", ["pyramid_wall_210", "joint_playground", "cloth", "mixed_small", "soft_beam",
+                                  "stvk_beam"])
 def test_ten_steps_close(oracle_mod, Solver, name):
     """Ten steps stay close to the oracle (errors compound, so the bar is 10x looser).
     The self-colliding 0.05 m FEM block is left out: its equal, overlapping

@@ -119,3 +119,23 @@ def test_colouring_is_proper(oracle_mod):
     for (a, b), _ in c.items():
         if col[a] >= 0 and col[b] >= 0:
             assert col[a] != col[b]
+
+
+def test_stvk_tet_oracle_is_sane(oracle_mod):
+    """The StVK tet restatement (no reference counterpart): at small strain it
+    moves a pinned beam like the reference's Neo-Hookean tet; under large
+    sag it stays finite and stiffer-in-tension behaviour does not blow up."""
+    from skyephyx_b200 import scenes
+    nh = oracle_mod.OracleSolver()
+    nh.make_tet_volume(-3.0, 0.0, -0.9, 9, 3, 3, 0.9, 8000.0, 0.3, 1.0, 0.5, True)
+    sv = oracle_mod.OracleSolver()
+    sv.make_stvk_tet_volume(-3.0, 0.0, -0.9, 9, 3, 3, 0.9, 8000.0, 0.3, 1.0, 0.5, True)
+    for o in (nh, sv):
+        assert o.step_coloured() == 0
+    p_nh, p_sv = nh.get_state()[0], sv.get_state()[0]
+    assert np.abs(p_nh - p_sv).max() < 1e-4
+    big = oracle_mod.OracleSolver()
+    scenes.stvk_block(big)
+    for _ in range(60):
+        big.step_coloured()
+    assert np.isfinite(big.get_state()[0]).all()
