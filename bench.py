@@ -238,11 +238,44 @@ def plain_configs(steps=5):
         t1 = time.perf_counter()
         c.step()
         cpu_s = time.perf_counter() - t1
-        out[name] = {"plain_gpu": ndyn * ITERS * steps / dt, "ms_per_step": dt * 1e3 / steps,
+        if name.startswith("C1"):
+            cpu_extra = {"long_horizon": long_horizon(build)}
+        else:
+            cpu_extra = {}
+        out[name] = {**cpu_extra, "plain_gpu": ndyn * ITERS * steps / dt, "ms_per_step": dt * 1e3 / steps,
                      "dynamic_bodies": ndyn, "status": status,
                      "step1_max_pos_err_m": pos_err, "step1_max_rot_err_rad": rot,
                      "cpu_reference_1core": ndyn * ITERS / cpu_s, "cpu_ms_per_step": cpu_s * 1e3,
                      "unit": UNIT}
+    return out
+
+
+def max_penetration(contacts):
+    """Deepest contact penetration (m) among live manifolds (data[:, 0])."""
+    depth = [float(d[:, 0].max()) for _, d in contacts.values() if len(d)]
+    return max(depth) if depth else 0.0
+
+
+def long_horizon(build, steps=600):
+    """C1 over `steps` steps on the single-scene GPU path and through the
+    reference's own sequential Step(): the largest drift of any dynamic body
+    from its initial position and the deepest penetration at the end."""
+    from oracle import oracle
+    from skyephyx_b200 import Solver
+    out = {"steps": steps}
+    for label, solver in (("gpu", Solver(iterations=ITERS)), ("reference", oracle.OracleSolver(iterations=ITERS,
+                                                                                               fast=True))):
+        build(solver)
+        p0 = solver.get_state()[0].copy()
+        for _ in range(steps):
+            solver.step()
+        p = solver.get_state()[0]
+        moving = np.abs(p - p0).max(axis=1)
+        out[label] = {"max_drift_m": float(moving.max()), "median_drift_m": float(np.median(moving)),
+                      "max_penetration_m": max_penetration(solver.contacts()),
+                      "finite": bool(np.isfinite(p).all())}
+        if hasattr(solver, "close"):
+            solver.close()
     return out
 
 
