@@ -261,6 +261,9 @@ int32_t avbd_batch_get_launch(const AvbdBatch* b, int32_t* threads_per_cta, int3
  * takes the next scene, down to a warp (or an eighth of a larger CTA).
  * 0 (the default) keeps one scene per CTA.  Autotuner knob. */
 int32_t avbd_batch_set_team_work(AvbdBatch* b, int32_t units_per_lane);
+/* The same threshold for scenes with tets (their per-colour finish leaves
+ * most of a team idle, which a second scene on the CTA can use). Default 0. */
+int32_t avbd_batch_set_fem_team_work(AvbdBatch* b, int32_t units_per_lane);
 /* Scenes of at least min_bodies bodies find broadphase candidates with a
  * uniform grid (the same candidate set and order as the reference's all-pairs
  * loop, which smaller scenes keep); 0 = all-pairs everywhere.  Default 128. */

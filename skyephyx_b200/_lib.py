@@ -105,6 +105,7 @@ SIGNATURES = [
     ("avbd_batch_get_launch", [_V, _I, _I], C.c_int32),
     ("avbd_batch_set_kernel", [_V, C.c_int32], C.c_int32),
     ("avbd_batch_set_team_work", [_V, C.c_int32], C.c_int32),
+    ("avbd_batch_set_fem_team_work", [_V, C.c_int32], C.c_int32),
     ("avbd_batch_set_grid_broadphase", [_V, C.c_int32], C.c_int32),
     ("avbd_batch_last_ms", [_V], C.c_float),
     ("avbd_batch_set_groups", [_V, C.c_int32, C.c_int32], C.c_int32),

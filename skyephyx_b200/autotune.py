@@ -38,6 +38,7 @@ SPACE = {
     "fem_group": (2, 4, 8, 64),   # 64: term-per-lane flat sweep
     "team_work": (0, 2, 4, 8),    # scene work per lane below which CTAs split into teams
     "grid_min": (0, 128, 512),    # scenes from this many bodies use the grid broadphase
+    "fem_team_work": (0, 4, 8, 16),   # the split threshold for scenes with tets
 }
 
 
@@ -79,6 +80,7 @@ def apply(batch, cfg: dict) -> None:
     batch.set_kernel(cfg["variant"])
     batch.set_launch(cfg["threads"], 0)
     batch.set_team_work(cfg.get("team_work", 0))
+    batch.set_fem_team_work(cfg.get("fem_team_work", 0))
     batch.set_grid_broadphase(cfg.get("grid_min", 128))
 
 

@@ -3,12 +3,16 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <atomic>
 #include <cmath>
 #include <cstdio>
+#include <cstdlib>
 #include <cstring>
 #include <map>
 #include <memory>
+#include <mutex>
 #include <new>
+#include <thread>
 #include <vector>
 
 #include "../../include/avbd.h"
@@ -236,9 +240,10 @@ __global__ void k_collide(World W, int a, int b, uint32_t* ids, float* data, int
 // Team::min_size(), so small scenes run several to a CTA without waiting on
 // each other's barriers.
 __device__ __forceinline__ bool scene_fits_half(const World& W, int scene, int team_size) {
-    if (W.team_work <= 0 || team_size / 2 < Team::min_size()) return false;
     const SceneDesc& d = W.scenes[scene];
-    return (long long)(d.nbody + d.ntet) <= (long long)W.team_work * (team_size / 2);
+    const int work = d.ntet > 0 ? W.fem_team_work : W.team_work;
+    if (work <= 0 || team_size / 2 < Team::min_size()) return false;
+    return (long long)(d.nbody + d.ntet) <= (long long)work * (team_size / 2);
 }
 
 template <int MAXT, int MINB>
@@ -314,12 +319,14 @@ struct Pools {
         owned_bytes.clear();
         W = World{};
     }
+    // zero = false for arrays every reader finds written first (contact points:
+    // the narrowphase fills a slot before any phase reads it)
     template <typename T>
-    cudaError_t alloc(T*& p, size_t n) {
+    cudaError_t alloc(T*& p, size_t n, bool zero = true) {
         void* q = nullptr;
         cudaError_t e = cudaMalloc(&q, std::max<size_t>(n, 1) * sizeof(T));
         if (e != cudaSuccess) return e;
-        cudaMemset(q, 0, std::max<size_t>(n, 1) * sizeof(T));
+        if (zero) cudaMemset(q, 0, std::max<size_t>(n, 1) * sizeof(T));
         owned.push_back(q);
         owned_bytes.push_back(std::max<size_t>(n, 1) * sizeof(T));
         p = static_cast<T*>(q);
@@ -378,9 +385,10 @@ struct Pools {
 #define A(expr) if ((e = (expr)) != cudaSuccess) return e
         A(alloc(W.cpair[t], nc)); A(alloc(W.cn[t], nc)); A(alloc(W.cfric[t], nc)); A(alloc(W.kbase[t], nc));
         A(alloc(W.cbirth[t], nc)); A(alloc(W.live[t], nc));
-        A(alloc(W.kid[t], k)); A(alloc(W.krA[t], k)); A(alloc(W.krB[t], k)); A(alloc(W.kn[t], k));
-        A(alloc(W.kt1[t], k)); A(alloc(W.kt2[t], k)); A(alloc(W.krAw[t], k)); A(alloc(W.krBw[t], k));
-        A(alloc(W.kpen[t], k)); A(alloc(W.klam[t], k));
+        A(alloc(W.kid[t], k, false)); A(alloc(W.krA[t], k, false)); A(alloc(W.krB[t], k, false));
+        A(alloc(W.kn[t], k, false)); A(alloc(W.kt1[t], k, false)); A(alloc(W.kt2[t], k, false));
+        A(alloc(W.krAw[t], k, false)); A(alloc(W.krBw[t], k, false)); A(alloc(W.kpen[t], k, false));
+        A(alloc(W.klam[t], k, false));
 #undef A
         return e;
     }
@@ -441,13 +449,9 @@ int scene_group(const HostScene& h, int rigid_group, int fem_group) {
 void scene_caps(const HostScene& h, int& candcap, int& kcap) {
     const int n = h.nbody();
     candcap = 16 * n + 64;   // a body in a column stack overlaps ~18 circumscribed spheres (owns ~9)
-    kcap = 24 * n + 128;
+    kcap = 8 * n + 128;      // live contact points average ~1.5 per body; a scene that needs more grows
 }
 
-template <typename T>
-void put(T* dst, const std::vector<T>& src, size_t at, cudaStream_t st) {
-    if (!src.empty()) cudaMemcpyAsync(dst + at, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, st);
-}
 
 // First-fit allocator of index ranges in one pool, with coalescing frees.
 struct Ranges {
@@ -539,10 +543,86 @@ bool place_scene(Allocs& A, const HostScene& h, int candcap, int kcap, int nsinc
     return ok;
 }
 
+// Where upload_scene's data goes.  DirectSink: straight to the device, one
+// copy per array of the scene.  StagedSink: into one host buffer per device
+// array at the scene's offsets, flushed with one copy per array, for packing
+// many scenes into fresh (zeroed) pools at once.
+struct DirectSink {
+    cudaStream_t st;
+    template <typename T>
+    void put(T* dst, const std::vector<T>& src, size_t at) {
+        if (!src.empty()) cudaMemcpyAsync(dst + at, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, st);
+    }
+    template <typename T>
+    void zero(T* dst, size_t at, size_t n) {
+        if (n) cudaMemsetAsync(dst + at, 0, n * sizeof(T), st);
+    }
+    void finish() { cudaStreamSynchronize(st); }   // the caller's host vectors are temporaries
+};
+
+struct StagedSink {
+    struct Buf {
+        char* host = nullptr;   // calloc'd: untouched pages read as zero and cost nothing
+        size_t cap = 0, lo = SIZE_MAX, hi = 0;
+    };
+    std::map<char*, Buf> bufs;
+    const Pools* P = nullptr;   // allocation sizes: each buffer is sized once to its pool array
+    cudaStream_t st = nullptr;
+    std::mutex m;               // scenes are staged from several host threads
+    bool overflow = false;      // a write outside its pool array (never expected)
+    ~StagedSink() {
+        for (auto& kv : bufs) std::free(kv.second.host);
+    }
+    // The host buffer of pool array `dst` with [off, off + n) marked written;
+    // null (and overflow set) if that range lies outside the array.
+    char* span(void* dst, size_t off, size_t n) {
+        std::lock_guard<std::mutex> lock(m);
+        Buf& b = bufs[static_cast<char*>(dst)];
+        if (!b.host) {
+            size_t cap = off + n;
+            if (P)
+                for (size_t i = 0; i < P->owned.size(); ++i)
+                    if (P->owned[i] == dst) cap = std::max(cap, P->owned_bytes[i]);
+            b.host = static_cast<char*>(std::calloc(cap, 1));
+            b.cap = b.host ? cap : 0;
+        }
+        if (b.cap < off + n) {
+            overflow = true;
+            return nullptr;
+        }
+        b.lo = std::min(b.lo, off);
+        b.hi = std::max(b.hi, off + n);
+        return b.host;
+    }
+    template <typename T>
+    void put(T* dst, const std::vector<T>& src, size_t at) {
+        if (src.empty()) return;
+        if (char* h = span(dst, at * sizeof(T), src.size() * sizeof(T)))
+            std::memcpy(h + at * sizeof(T), src.data(), src.size() * sizeof(T));
+    }
+    template <typename T>
+    void zero(T* dst, size_t at, size_t n) {
+        if (!n) return;
+        if (char* h = span(dst, at * sizeof(T), n * sizeof(T))) std::memset(h + at * sizeof(T), 0, n * sizeof(T));
+    }
+    void finish() {}
+    bool flush() {
+        for (auto& kv : bufs)
+            if (kv.second.hi > kv.second.lo)
+                cudaMemcpyAsync(kv.first + kv.second.lo, kv.second.host + kv.second.lo, kv.second.hi - kv.second.lo,
+                                cudaMemcpyHostToDevice, st);
+        cudaStreamSynchronize(st);
+        for (auto& kv : bufs) std::free(kv.second.host);
+        bufs.clear();
+        return !overflow;
+    }
+};
+
 // Writes a placed scene (as staged) into the pools and its descriptor/state
 // into scene slot `slot`.
+template <typename Sink>
 void upload_scene(Pools& P, const HostScene& h, const StaticInc& si, const Region& r, int group, int slot,
-                  SceneDesc& d, cudaStream_t st) {
+                  SceneDesc& d, Sink& sink) {
     d.body0 = r.body0; d.nbody = r.nbody;
     d.force0 = r.force0; d.nforce = r.nforce;
     d.tet0 = r.tet0; d.ntet = r.ntet;
@@ -553,49 +633,45 @@ void upload_scene(Pools& P, const HostScene& h, const StaticInc& si, const Regio
     d.ndynamic = h.ndynamic();
     d.group = group;
     World& W = P.W;
-    put(W.pos, h.pos, d.body0, st); put(W.rot, h.rot, d.body0, st); put(W.scale, h.scale, d.body0, st);
-    put(W.vel, h.vel, d.body0, st); put(W.omega, h.omega, d.body0, st); put(W.massI, h.massI, d.body0, st);
-    put(W.flags, h.flags, d.body0, st); put(W.friction, h.friction, d.body0, st);
-    put(W.lpos, h.pos, d.body0, st); put(W.lrot, h.rot, d.body0, st);
-    put(W.ipos, h.pos, d.body0, st); put(W.irot, h.rot, d.body0, st);
-    if (d.nbody) {
-        cudaMemsetAsync(W.pvel + d.body0, 0, d.nbody * sizeof(float4), st);
-        cudaMemsetAsync(W.reset_flag + d.body0, 0, d.nbody * sizeof(int), st);
-    }
+    sink.put(W.pos, h.pos, d.body0); sink.put(W.rot, h.rot, d.body0); sink.put(W.scale, h.scale, d.body0);
+    sink.put(W.vel, h.vel, d.body0); sink.put(W.omega, h.omega, d.body0); sink.put(W.massI, h.massI, d.body0);
+    sink.put(W.flags, h.flags, d.body0); sink.put(W.friction, h.friction, d.body0);
+    sink.put(W.lpos, h.pos, d.body0); sink.put(W.lrot, h.rot, d.body0);
+    sink.put(W.ipos, h.pos, d.body0); sink.put(W.irot, h.rot, d.body0);
+    sink.zero(W.pvel, d.body0, d.nbody);
+    sink.zero(W.reset_flag, d.body0, d.nbody);
     std::vector<int> tmp(d.nbody);
     for (int b = 0; b < d.nbody; ++b) tmp[b] = b;
-    put(W.local, tmp, d.body0, st);
+    sink.put(W.local, tmp, d.body0);
     for (int b = 0; b < d.nbody; ++b) tmp[b] = si.off[b] + r.sinc0;
-    put(const_cast<int*>(W.sinc_off), tmp, d.body0, st);
-    put(const_cast<int*>(W.sinc_n), si.cnt, d.body0, st);
-    put(const_cast<int*>(W.sinc_nf), si.nf, d.body0, st);
-    put(const_cast<uint32_t*>(W.sinc), si.ent, r.sinc0, st);
+    sink.put(const_cast<int*>(W.sinc_off), tmp, d.body0);
+    sink.put(const_cast<int*>(W.sinc_n), si.cnt, d.body0);
+    sink.put(const_cast<int*>(W.sinc_nf), si.nf, d.body0);
+    sink.put(const_cast<uint32_t*>(W.sinc), si.ent, r.sinc0);
     for (int b = 0; b < d.nbody; ++b) tmp[b] = si.poff[b] + r.sp0;
-    put(const_cast<int*>(W.spartner_off), tmp, d.body0, st);
-    put(const_cast<int*>(W.spartner_n), si.pcnt, d.body0, st);
-    put(reinterpret_cast<int2*>(const_cast<int*>(W.spartner)), si.partners, r.sp0, st);
+    sink.put(const_cast<int*>(W.spartner_off), tmp, d.body0);
+    sink.put(const_cast<int*>(W.spartner_n), si.pcnt, d.body0);
+    sink.put(reinterpret_cast<int2*>(const_cast<int*>(W.spartner)), si.partners, r.sp0);
     std::vector<int2> fb = h.fbody;
     for (auto& ab : fb) { if (ab.x >= 0) ab.x += d.body0; ab.y += d.body0; }
-    put(W.ftype, h.ftype, d.force0, st); put(W.fbody, fb, d.force0, st); put(W.frA, h.frA, d.force0, st);
-    put(W.frB, h.frB, d.force0, st); put(W.fq, h.fq, d.force0, st); put(W.fparam, h.fparam, d.force0, st);
-    put(W.fk, h.fk, 6 * (size_t)d.force0, st); put(W.ffrac, h.ffrac, 6 * (size_t)d.force0, st);
-    put(W.ffmin, h.ffmin, 6 * (size_t)d.force0, st); put(W.ffmax, h.ffmax, 6 * (size_t)d.force0, st);
-    if (d.nforce) {
-        cudaMemsetAsync(W.fpen + 6 * (size_t)d.force0, 0, 6 * (size_t)d.nforce * sizeof(float), st);
-        cudaMemsetAsync(W.flam + 6 * (size_t)d.force0, 0, 6 * (size_t)d.nforce * sizeof(float), st);
-    }
+    sink.put(W.ftype, h.ftype, d.force0); sink.put(W.fbody, fb, d.force0); sink.put(W.frA, h.frA, d.force0);
+    sink.put(W.frB, h.frB, d.force0); sink.put(W.fq, h.fq, d.force0); sink.put(W.fparam, h.fparam, d.force0);
+    sink.put(W.fk, h.fk, 6 * (size_t)d.force0); sink.put(W.ffrac, h.ffrac, 6 * (size_t)d.force0);
+    sink.put(W.ffmin, h.ffmin, 6 * (size_t)d.force0); sink.put(W.ffmax, h.ffmax, 6 * (size_t)d.force0);
+    sink.zero(W.fpen, 6 * (size_t)d.force0, 6 * (size_t)d.nforce);
+    sink.zero(W.flam, 6 * (size_t)d.force0, 6 * (size_t)d.nforce);
     std::vector<int4> ti = h.tidx;
     for (auto& t : ti) { t.x += d.body0; t.y += d.body0; t.z += d.body0; t.w += d.body0; }
-    put(W.tidx, ti, d.tet0, st); put(W.tDmInv, h.tDmInv, 9 * (size_t)d.tet0, st);
-    put(W.tgradN, h.tgradN, 12 * (size_t)d.tet0, st); put(W.tparam, h.tparam, d.tet0, st);
-    put(W.tkind, h.tkind, d.tet0, st);
+    sink.put(W.tidx, ti, d.tet0); sink.put(W.tDmInv, h.tDmInv, 9 * (size_t)d.tet0);
+    sink.put(W.tgradN, h.tgradN, 12 * (size_t)d.tet0); sink.put(W.tparam, h.tparam, d.tet0);
+    sink.put(W.tkind, h.tkind, d.tet0);
     std::vector<int4> ri = h.ridx;
     for (auto& t : ri) { t.x += d.body0; t.y += d.body0; t.z += d.body0; }
-    put(W.ridx, ri, d.tri0, st); put(W.rDmInv, h.rDmInv, d.tri0, st);
-    put(W.rgradN, h.rgradN, 6 * (size_t)d.tri0, st); put(W.rparam, h.rparam, d.tri0, st);
-    cudaMemcpyAsync(P.d_scenes + slot, &d, sizeof(SceneDesc), cudaMemcpyHostToDevice, st);
-    cudaMemsetAsync(P.d_sstate + slot, 0, sizeof(SceneState), st);
-    cudaStreamSynchronize(st);   // the host vectors above are temporaries
+    sink.put(W.ridx, ri, d.tri0); sink.put(W.rDmInv, h.rDmInv, d.tri0);
+    sink.put(W.rgradN, h.rgradN, 6 * (size_t)d.tri0); sink.put(W.rparam, h.rparam, d.tri0);
+    sink.put(P.d_scenes, std::vector<SceneDesc>(1, d), slot);
+    sink.zero(P.d_sstate, slot, 1);
+    sink.finish();
 }
 
 // Static incidence entries and joint/spring partner entries a scene needs.
@@ -692,7 +768,8 @@ int upload(AvbdWorld* w) {
     Region reg;
     if (!place_scene(A, w->h, cc, kc, nsinc, nsp, reg)) return AVBD_ERR_NOMEM;
     w->descs.assign(1, SceneDesc{});
-    upload_scene(P, w->h, static_incidence(w->h, reg), reg, g, 0, w->descs[0], w->stream);
+    DirectSink sink{w->stream};
+    upload_scene(P, w->h, static_incidence(w->h, reg), reg, g, 0, w->descs[0], sink);
     if (cudaGetLastError() != cudaSuccess) return AVBD_ERR_CUDA;
     P.W.P = to_params(w->params);
     w->uploaded = true;
@@ -879,6 +956,7 @@ struct AvbdBatch {
     int grid = 0;
     int stage = 0;   // float4 slots of dynamic shared memory per CTA
     int team_work = 0;   // bodies + tets per lane below which a CTA team splits (0 = never)
+    int fem_team_work = 0;   // the same for scenes with tets
     int grid_min = 128;  // scenes from this many bodies use the grid broadphase (0 = never)
     std::vector<long long> steps_due;   // steps each slot's scene should have taken
     int* d_fail = nullptr;               // scene steps stopped by a full table (device counter)
@@ -909,7 +987,7 @@ int batch_reserve(AvbdBatch* b, int64_t bodies, int64_t forces, int64_t tets, in
                   int64_t nsinc, int64_t nsp) {
     int r = batch_stream(b);
     if (r) return r;
-    const int64_t ncand = 16 * bodies + 64 * nscenes, nk = 24 * bodies + 128 * nscenes;
+    const int64_t ncand = 16 * bodies + 64 * nscenes, nk = 8 * bodies + 128 * nscenes;
     const int64_t ninc = nsinc + 2 * ncand;
     const int64_t lim = 0x07FFFFFF;   // incidence entries index 27 bits
     if (bodies > lim || forces > lim || tets > lim || tris > lim || ncand > lim || nk > INT32_MAX || ninc > INT32_MAX ||
@@ -945,18 +1023,34 @@ int batch_reserve(AvbdBatch* b, int64_t bodies, int64_t forces, int64_t tets, in
     return 0;
 }
 
-// Places and uploads the staged scene of `slot`; AVBD_ERR_NOMEM if the pools are full.
-int batch_admit(AvbdBatch* b, int slot) {
+// Takes pool ranges for the staged scene of `slot`; AVBD_ERR_NOMEM if the pools are full.
+int batch_place(AvbdBatch* b, int slot) {
     if (slot >= b->P.ns) return AVBD_ERR_NOMEM;
-    HostScene& h = b->scenes[slot];
+    const HostScene& h = b->scenes[slot];
     int cc, kc, nsinc, nsp;
     scene_caps(h, cc, kc);
     static_counts(h, nsinc, nsp);
     Region reg;
     if (!place_scene(b->A, h, cc, kc, nsinc, nsp, reg)) return AVBD_ERR_NOMEM;
     b->regions[slot] = reg;
+    return 0;
+}
+
+// Writes a placed scene through `sink` and marks it live.
+template <typename Sink>
+void batch_upload(AvbdBatch* b, int slot, Sink& sink) {
+    const HostScene& h = b->scenes[slot];
+    const Region& reg = b->regions[slot];
     upload_scene(b->P, h, static_incidence(h, reg), reg, scene_group(h, b->group_rigid, b->group_fem), slot,
-                 b->descs[slot], b->stream);
+                 b->descs[slot], sink);
+}
+
+// Places and uploads the staged scene of `slot` (live admission).
+int batch_admit(AvbdBatch* b, int slot) {
+    int r = batch_place(b, slot);
+    if (r) return r;
+    DirectSink sink{b->stream};
+    batch_upload(b, slot, sink);
     b->state[slot] = 1;
     if ((int)b->steps_due.size() <= slot) b->steps_due.resize(slot + 1, 0);
     b->steps_due[slot] = 0;
@@ -995,9 +1089,34 @@ int batch_pack(AvbdBatch* b) {
     }
     int r = batch_reserve(b, nb, nf, nt, nr, (int64_t)b->scenes.size(), nsinc, nsp);
     if (r) return r;
+    // fresh pools: place every scene, stage them into host arrays from all host
+    // threads (their ranges are disjoint), then one copy per device array
+    std::vector<int> slots;
     for (size_t i = 0; i < b->scenes.size(); ++i)
-        if (b->state[i] == 2 && (r = batch_admit(b, (int)i))) return r;
-    return 0;
+        if (b->state[i] == 2) {
+            if ((r = batch_place(b, (int)i))) return r;
+            slots.push_back((int)i);
+        }
+    StagedSink staged;
+    staged.st = b->stream;
+    staged.P = &b->P;
+    std::atomic<size_t> next{0};
+    auto work = [&]() {
+        for (size_t k = next++; k < slots.size(); k = next++) batch_upload(b, slots[k], staged);
+    };
+    const unsigned nthreads = std::max(1u, std::min(16u, std::thread::hardware_concurrency()));
+    std::vector<std::thread> pool;
+    for (unsigned t = 1; t < nthreads && slots.size() > 64; ++t) pool.emplace_back(work);
+    work();
+    for (auto& th : pool) th.join();
+    if (!staged.flush()) return AVBD_ERR_STATE;
+    for (int i : slots) {
+        b->state[i] = 1;
+        if ((int)b->steps_due.size() <= i) b->steps_due.resize(i + 1, 0);
+        b->steps_due[i] = 0;
+    }
+    b->order_dirty = true;
+    return cudaGetLastError() == cudaSuccess ? 0 : AVBD_ERR_CUDA;
 }
 
 int batch_launch_shape(AvbdBatch* b) {
@@ -1120,6 +1239,7 @@ int batch_step_listed(AvbdBatch* b, const std::vector<int>& slots) {
     World W = b->P.W;
     W.stage_bodies = b->stage;
     W.team_work = b->team_work;
+    W.fem_team_work = b->fem_team_work;
     W.grid_min = b->grid_min;
     W.fail_count = b->d_fail;
     const int* order = b->d_fix_order;
@@ -1175,6 +1295,7 @@ int batch_build_graph(AvbdBatch* b) {
     cudaMemsetAsync(b->d_queue, 0, sizeof(int), b->stream);
     b->P.W.stage_bodies = b->stage;
     b->P.W.team_work = b->team_work;
+    b->P.W.fem_team_work = b->fem_team_work;
     b->P.W.grid_min = b->grid_min;
     b->P.W.fail_count = b->d_fail;
     const size_t smem = (size_t)b->stage * sizeof(float4);
@@ -1903,6 +2024,13 @@ int32_t avbd_batch_set_kernel(AvbdBatch* b, int32_t register_variant) {
 int32_t avbd_batch_set_team_work(AvbdBatch* b, int32_t units_per_lane) {
     if (!b || units_per_lane < 0) return AVBD_ERR_INVALID;
     b->team_work = units_per_lane;
+    batch_drop_graph(b);
+    return 0;
+}
+
+int32_t avbd_batch_set_fem_team_work(AvbdBatch* b, int32_t units_per_lane) {
+    if (!b || units_per_lane < 0) return AVBD_ERR_INVALID;
+    b->fem_team_work = units_per_lane;
     batch_drop_graph(b);
     return 0;
 }

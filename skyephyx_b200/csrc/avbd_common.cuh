@@ -138,6 +138,7 @@ struct World {
     int nscenes;
     int stage_bodies;   // batched kernel: float4 slots of dynamic shared memory per CTA
     int team_work;      // batched kernel: bodies + tets per lane below which a team splits (0 = never)
+    int fem_team_work;  // the same for scenes with tets (0 = never)
     int grid_min;       // batched kernel: scenes from this many bodies use the grid broadphase (0 = never)
     int* fail_count;    // batched kernel: scene steps stopped by a full table (host grows and catches up)
     const SceneDesc* scenes;

@@ -279,36 +279,59 @@ void HostScene::build_static_incidence(std::vector<int>& off, std::vector<int>& 
                                        std::vector<uint32_t>& ent, std::vector<int>& poff, std::vector<int>& pcnt,
                                        std::vector<int2>& partners, int body_base, int force_base, int tet_base,
                                        int tri_base) const {
+    // counting sort by body: per body its forces in force order, then its
+    // tets in tet order, then its triangles; partners in force order
     const int n = nbody();
-    std::vector<std::vector<uint32_t>> fe(n), ee(n);
-    std::vector<std::vector<int2>> pp(n);
+    nf.assign(n, 0);
+    pcnt.assign(n, 0);
+    std::vector<int> ne(n, 0);
     for (int f = 0; f < nforce(); ++f) {
         const int2 ab = fbody[f];
         if (ab.x >= 0) {
-            fe[ab.x].push_back(ent_make(kEntForce, 0, (uint32_t)(force_base + f)));
-            pp[ab.x].push_back(make_int2(body_base + ab.y, force_base + f));
-            pp[ab.y].push_back(make_int2(body_base + ab.x, force_base + f));
+            ++nf[ab.x];
+            ++pcnt[ab.x];
+            ++pcnt[ab.y];
         }
-        fe[ab.y].push_back(ent_make(kEntForce, 1, (uint32_t)(force_base + f)));
+        ++nf[ab.y];
+    }
+    for (int t = 0; t < ntet(); ++t) {
+        ++ne[tidx[t].x]; ++ne[tidx[t].y]; ++ne[tidx[t].z]; ++ne[tidx[t].w];
+    }
+    for (int t = 0; t < ntri(); ++t) {
+        ++ne[ridx[t].x]; ++ne[ridx[t].y]; ++ne[ridx[t].z];
+    }
+    off.resize(n);
+    cnt.resize(n);
+    poff.resize(n);
+    int acc = 0, pacc = 0;
+    for (int b = 0; b < n; ++b) {
+        off[b] = acc;
+        cnt[b] = nf[b] + ne[b];
+        acc += cnt[b];
+        poff[b] = pacc;
+        pacc += pcnt[b];
+    }
+    ent.resize(acc);
+    partners.resize(pacc);
+    std::vector<int> fcur(n, 0), ecur(n, 0), pcur(n, 0);
+    for (int f = 0; f < nforce(); ++f) {
+        const int2 ab = fbody[f];
+        if (ab.x >= 0) {
+            ent[off[ab.x] + fcur[ab.x]++] = ent_make(kEntForce, 0, (uint32_t)(force_base + f));
+            partners[poff[ab.x] + pcur[ab.x]++] = make_int2(body_base + ab.y, force_base + f);
+            partners[poff[ab.y] + pcur[ab.y]++] = make_int2(body_base + ab.x, force_base + f);
+        }
+        ent[off[ab.y] + fcur[ab.y]++] = ent_make(kEntForce, 1, (uint32_t)(force_base + f));
     }
     for (int t = 0; t < ntet(); ++t) {
         const int v[4] = {tidx[t].x, tidx[t].y, tidx[t].z, tidx[t].w};
-        for (int r = 0; r < 4; ++r) ee[v[r]].push_back(ent_make(kEntTet, (uint32_t)r, (uint32_t)(tet_base + t)));
+        for (int r = 0; r < 4; ++r)
+            ent[off[v[r]] + nf[v[r]] + ecur[v[r]]++] = ent_make(kEntTet, (uint32_t)r, (uint32_t)(tet_base + t));
     }
     for (int t = 0; t < ntri(); ++t) {
         const int v[3] = {ridx[t].x, ridx[t].y, ridx[t].z};
-        for (int r = 0; r < 3; ++r) ee[v[r]].push_back(ent_make(kEntTri, (uint32_t)r, (uint32_t)(tri_base + t)));
-    }
-    off.clear(); cnt.clear(); nf.clear(); ent.clear(); poff.clear(); pcnt.clear(); partners.clear();
-    for (int b = 0; b < n; ++b) {
-        off.push_back((int)ent.size());
-        nf.push_back((int)fe[b].size());
-        ent.insert(ent.end(), fe[b].begin(), fe[b].end());
-        ent.insert(ent.end(), ee[b].begin(), ee[b].end());
-        cnt.push_back((int)ent.size() - off.back());
-        poff.push_back((int)partners.size());
-        partners.insert(partners.end(), pp[b].begin(), pp[b].end());
-        pcnt.push_back((int)partners.size() - poff.back());
+        for (int r = 0; r < 3; ++r)
+            ent[off[v[r]] + nf[v[r]] + ecur[v[r]]++] = ent_make(kEntTri, (uint32_t)r, (uint32_t)(tri_base + t));
     }
 }
 

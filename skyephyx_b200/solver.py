@@ -373,6 +373,10 @@ class Batch:
         share a CTA with others (0: one scene per CTA); before stepping."""
         check(self._lib.avbd_batch_set_team_work(self._h, int(units_per_lane)), "set_team_work")
 
+    def set_fem_team_work(self, units_per_lane=0):
+        """The team split threshold for scenes with tets (0: one scene per CTA)."""
+        check(self._lib.avbd_batch_set_fem_team_work(self._h, int(units_per_lane)), "set_fem_team_work")
+
     def set_grid_broadphase(self, min_bodies=128):
         """Scenes of at least min_bodies use the grid broadphase (0: all-pairs)."""
         check(self._lib.avbd_batch_set_grid_broadphase(self._h, int(min_bodies)), "set_grid_broadphase")
