@@ -350,6 +350,7 @@ struct Pools {
 
     cudaError_t allocate_all() {
         cudaError_t e = cudaSuccess;
+        if (nb >= kMaxPoolBodies) return cudaErrorInvalidValue;   // tet-term records keep ids in 28 bits
 #define A(expr) if ((e = (expr)) != cudaSuccess) return e
         A(alloc(d_scenes, ns));
         A(alloc(d_sstate, ns));
@@ -372,7 +373,9 @@ struct Pools {
         A(alloc(W.fk, 6 * (size_t)nf)); A(alloc(W.ffrac, 6 * (size_t)nf)); A(alloc(W.ffmin, 6 * (size_t)nf));
         A(alloc(W.ffmax, 6 * (size_t)nf)); A(alloc(W.fpen, 6 * (size_t)nf)); A(alloc(W.flam, 6 * (size_t)nf));
         A(alloc(W.tidx, nt)); A(alloc(W.tDmInv, 9 * (size_t)nt)); A(alloc(W.tgradN, 12 * (size_t)nt));
-        A(alloc(W.tparam, nt)); A(alloc(W.fterm, 4 * (size_t)nt)); A(alloc(W.tkind, nt));
+        A(alloc(W.tparam, nt)); A(alloc(W.tkind, nt));
+        A(alloc(W.trv, 4 * (size_t)nt)); A(alloc(W.trm0, 4 * (size_t)nt)); A(alloc(W.trm1, 4 * (size_t)nt));
+        A(alloc(W.trm2, 4 * (size_t)nt));
         A(alloc(W.ridx, nr)); A(alloc(W.rDmInv, nr)); A(alloc(W.rgradN, 6 * (size_t)nr)); A(alloc(W.rparam, nr));
         A(alloc(W.inc, ninc));
         for (int t = 0; t < 2; ++t) A(alloc_tables(t, ncand, nk));

@@ -56,6 +56,12 @@ constexpr int kGroupFlat = 64;         // SceneDesc::group of scenes swept term-
 // tet energy models
 constexpr int kTetNeoHookean = 0;      // NeoHookeanFEM (neohookeanfem.cpp)
 constexpr int kTetStvk = 1;            // St. Venant-Kirchhoff tet (no reference counterpart)
+// Top bits of a tet-term record's first vertex id (ids stay below kMaxPoolBodies).
+constexpr int kTermRoleShift = 28;     // 2 bits: the vertex the term is for
+constexpr uint32_t kTermStvk = 1u << 30;
+constexpr uint32_t kTermRemoved = 1u << 31;
+constexpr uint32_t kTermIdMask = (1u << kTermRoleShift) - 1u;
+constexpr long long kMaxPoolBodies = 1ll << kTermRoleShift;
 
 // body flags
 constexpr int kBodyStatic = 1;
@@ -235,7 +241,15 @@ struct World {
     // ---- colouring ----
     int* col_list;      // per scene region [body0, body0+nbody): bodies grouped by colour
     int* col_tinc;      // flat-sweep scenes: inclusive prefix of tet terms over the scene's col_list
-    uint32_t* fterm;    // flat-sweep scenes: tet-term entries in colour-list order, 4 slots per tet from 4 * tet0
+    // Flat-sweep scenes: one record per tet term in colour-list order (4 slots
+    // per tet from 4 * tet0), written with the colouring so the sweep reads
+    // them coalesced instead of gathering tet data.  trv: the tet's vertex ids,
+    // .x carrying the term's role, model and removal in its top bits
+    // (kTermRoleShift...); trm0..2: Dm^-1 (column-major), restVolume, mu, lambda.
+    int4* trv;
+    float4* trm0;       // Dm^-1[0..3]
+    float4* trm1;       // Dm^-1[4..7]
+    float4* trm2;       // Dm^-1[8], restVolume, mu, lambda
     int* col_start;     // per scene kMaxColours+1 offsets (scene * (kMaxColours+1))
 
     Params P;

@@ -752,6 +752,46 @@ AVBD_HD bool tet_term(const World& W, int idx, int role, V3& g, S3& H) {
     return true;
 }
 
+// The record of a tet term for the flat sweep (slot q of the tet-term
+// records), from the tet's data; made with the colouring.
+__device__ __forceinline__ void write_term_record(const World& W, size_t q, uint32_t ent) {
+    const int idx = (int)ent_index(ent);
+    const int4 v = W.tidx[idx];
+    const float4 tp = W.tparam[idx];
+    const float* D = W.tDmInv + (size_t)idx * 9;
+    uint32_t x = (uint32_t)v.x | (ent_role(ent) << kTermRoleShift);
+    if (W.tkind[idx] == kTetStvk) x |= kTermStvk;
+    if (tp.w != 0.f) x |= kTermRemoved;
+    W.trv[q] = make_int4((int)x, v.y, v.z, v.w);
+    W.trm0[q] = make_float4(D[0], D[1], D[2], D[3]);
+    W.trm1[q] = make_float4(D[4], D[5], D[6], D[7]);
+    W.trm2[q] = make_float4(D[8], tp.x, tp.y, tp.z);
+}
+
+// tet_term from the record in slot q: streamed loads (each record is read
+// once per sweep) and the shape gradient of the term's vertex rebuilt from
+// Dm^-1 with the host's operations (gradN1..3 = rows of Dm^-1, gradN0 =
+// -g1 - g2 - g3), so the values equal the stored ones bit for bit.
+__device__ __forceinline__ bool tet_term_record(const World& W, size_t q, V3& g, S3& H) {
+    const int4 a = __ldcs(W.trv + q);
+    const uint32_t x = (uint32_t)a.x;
+    if (x & kTermRemoved) return false;
+    const float4 m0 = __ldcs(W.trm0 + q), m1 = __ldcs(W.trm1 + q), m2 = __ldcs(W.trm2 + q);
+    const float D[9] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w, m2.x};
+    const uint32_t role = (x >> kTermRoleShift) & 3u;
+    V3 gn;
+    if (role == 0) gn = v3(((-D[0]) - D[1]) - D[2], ((-D[3]) - D[4]) - D[5], ((-D[6]) - D[7]) - D[8]);
+    else if (role == 1) gn = v3(D[0], D[3], D[6]);
+    else if (role == 2) gn = v3(D[1], D[4], D[7]);
+    else gn = v3(D[2], D[5], D[8]);
+    const V3 p0 = v3(W.pos[x & kTermIdMask]), p1 = v3(W.pos[a.y]), p2 = v3(W.pos[a.z]), p3 = v3(W.pos[a.w]);
+    if (x & kTermStvk)
+        stvk_tet_terms(p0, p1, p2, p3, D, gn, m2.y, m2.z, m2.w, W.P.projection_mode, W.P.trust_region_rho, g, H);
+    else
+        neohookean_terms(p0, p1, p2, p3, D, gn, m2.y, m2.z, m2.w, W.P.projection_mode, W.P.trust_region_rho, g, H);
+    return true;
+}
+
 // Rounded adds: the term is rounded before it is accumulated, whether it was
 // just computed (inlined) or read back from shared memory, so every sweep
 // variant sums the same values.
@@ -853,12 +893,6 @@ AVBD_HD void particle_init_mass(const World& W, int b, Sys3& s) {
     s.r[0] = m * dl.x; s.r[1] = m * dl.y; s.r[2] = m * dl.z;
 }
 
-AVBD_HD void particle_add_energy(Sys3& s, float gx, float gy, float gz, float hxx, float hyy, float hzz, float hxy,
-                                 float hxz, float hyz) {
-    s.r[0] = XADD(s.r[0], gx); s.r[1] = XADD(s.r[1], gy); s.r[2] = XADD(s.r[2], gz);
-    s.a[0][0] = XADD(s.a[0][0], hxx); s.a[1][1] = XADD(s.a[1][1], hyy); s.a[2][2] = XADD(s.a[2][2], hzz);
-    s.a[1][0] = XADD(s.a[1][0], hxy); s.a[2][0] = XADD(s.a[2][0], hxz); s.a[2][1] = XADD(s.a[2][1], hyz);
-}
 
 AVBD_HD void particle_finish(const World& W, int b, Sys3& s) {
     float x3[3];

@@ -310,14 +310,15 @@ __device__ __noinline__ void primal_sweep_cta_dispatch(const Team& T, const Worl
 // ---------------------------------------------------------------------------
 // Term-per-lane primal sweep of one colour, for scenes whose energies are all
 // tetrahedra.  Up to nslots (particle, tet) terms of the colour are
-// evaluated at once, one per lane, into shared memory; then one lane per
-// particle adds its inertia, its force and manifold rows and its tet terms in
-// incidence order (the reference's order) and solves.  Lanes stay busy
+// evaluated at once, one per lane, into shared memory; then each particle
+// adds its inertia, its force and manifold rows and its tet terms in
+// incidence order (the reference's order) and solves, its nine sums split
+// over up to nine lanes when the chunk has few particles.  Lanes stay busy
 // whatever the particles' degrees.  tinc (the scene's col_tinc) holds the
-// inclusive prefix of tet terms over the colour list and fterm the terms'
-// incidence entries in that order (both made with the colouring); the colour
-// occupies list positions [c0, c1).  sm: 9 * nslots words of shared memory (the
-// broadphase's stage, reused).
+// inclusive prefix of tet terms over the colour list, and the tet-term
+// records from rec0 on hold the terms in that order (both made with the
+// colouring); the colour occupies list positions [c0, c1).  sm: 9 * nslots
+// words of shared memory (the broadphase's stage, reused).
 // ---------------------------------------------------------------------------
 
 __device__ __forceinline__ int tet_terms(const World& W, int b) { return W.sinc_n[b] - W.sinc_nf[b]; }
@@ -345,8 +346,83 @@ __device__ __noinline__ void flat_finish_body(const World& W, int cur, int b, in
     primal_finish(W, b, s);
 }
 
+// Value of component k (the slots' order: gradient x y z, Hessian xx yy zz,
+// xy xz yz) of a particle system.
+__device__ __forceinline__ float sys3_component(const Sys3& s, int k) {
+    return k == 0 ? s.r[0] : k == 1 ? s.r[1] : k == 2 ? s.r[2] : k == 3 ? s.a[0][0] : k == 4 ? s.a[1][1]
+         : k == 5 ? s.a[2][2] : k == 6 ? s.a[1][0] : k == 7 ? s.a[2][0] : s.a[2][1];
+}
+
+// Finish of the particles [v, vend) of a flat chunk whose terms sit in the
+// slots, L lanes per particle (L in 1, 3, 9; 32 / L particles per warp): lane
+// `sub` of a particle's group adds components [sub * 9/L, (sub + 1) * 9/L) of
+// its terms, each in incidence order from the inertia's value, so every sum
+// is the one a single lane makes; the group's first lane gathers the nine
+// sums by shuffles and solves.  A particle with force or manifold rows, or a
+// rigid body, is finished by its first lane alone.  The loop bound is
+// uniform over each warp, so the shuffles run with the whole warp.
+template <int L>
+__device__ __noinline__ void flat_finish_split(const Team& T, const World& W, int cur, const int* list,
+                                                  const int* tinc, int base, int v, int vend, float alpha,
+                                                  bool write_stick, const float* sm, int nslots) {
+    constexpr int G = 32 / L, C = 9 / L;
+    const int lane = T.rank & 31, grp = lane / L, sub = lane - grp * L;
+    const int stride = (T.size >> 5) * G;
+    for (int j0 = v + (T.rank >> 5) * G; j0 < vend; j0 += stride) {
+        const int j = j0 + grp;
+        int b = -1;
+        if (grp < G && j < vend) {
+            b = list[j];
+            if (W.flags[b] & kBodyRemoved) b = -1;
+        }
+        bool lean = false;
+        int e0 = 0, e1 = 0, q0 = 0;
+        float acc[C];
+#pragma unroll
+        for (int k = 0; k < C; ++k) acc[k] = 0.f;
+        if (b >= 0) {
+            e0 = W.inc_off[b];
+            e1 = e0 + W.inc_cnt[b];
+            q0 = (j == 0 ? 0 : tinc[j - 1]) - base;
+            const int nterm = tinc[j] - base - q0;
+            lean = e1 - e0 == nterm && energy_only_particle(W, b);
+            if (lean) {
+                Sys3 s;
+                particle_init_mass(W, b, s);
+#pragma unroll
+                for (int k = 0; k < C; ++k) acc[k] = sys3_component(s, sub * C + k);
+                for (int q = q0; q < q0 + nterm; ++q)
+#pragma unroll
+                    for (int k = 0; k < C; ++k) acc[k] = XADD(acc[k], sm[(sub * C + k) * nslots + q]);
+            }
+        }
+        float f[9];
+        if constexpr (L == 1) {
+#pragma unroll
+            for (int k = 0; k < 9; ++k) f[k] = acc[k];
+        } else {
+#pragma unroll
+            for (int s = 0; s < L; ++s)
+#pragma unroll
+                for (int k = 0; k < C; ++k) f[s * C + k] = __shfl_sync(0xffffffffu, acc[k], grp * L + s);
+        }
+        if (b >= 0 && sub == 0) {
+            if (lean) {
+                Sys3 s;
+                s.r[0] = f[0]; s.r[1] = f[1]; s.r[2] = f[2];
+                s.a[0][0] = f[3]; s.a[1][1] = f[4]; s.a[2][2] = f[5];
+                s.a[1][0] = f[6]; s.a[2][0] = f[7]; s.a[2][1] = f[8];
+                s.a[0][1] = 0.f; s.a[0][2] = 0.f; s.a[1][2] = 0.f;
+                particle_finish(W, b, s);
+            } else {
+                flat_finish_body(W, cur, b, e0, e1, q0, alpha, write_stick, sm, nslots);
+            }
+        }
+    }
+}
+
 __device__ __noinline__ void primal_sweep_flat(const Team& T, const World& W, int cur, const int* list,
-                                               const int* tinc, const uint32_t* fterm, int c0, int c1, float alpha,
+                                               const int* tinc, size_t rec0, int c0, int c1, float alpha,
                                                bool write_stick) {
     float* sm = reinterpret_cast<float*>(T.stage);
     const int nslots = T.stage_cap * 4 / 9;
@@ -368,33 +444,33 @@ __device__ __noinline__ void primal_sweep_flat(const Team& T, const World& W, in
         const bool flat = total <= nslots;
         if (flat) {
             for (int q = tid; q < total; q += nt) {
-                const uint32_t ent = fterm[base + q];
                 V3 g = v3(0.f, 0.f, 0.f);
                 S3 H;
                 s3_zero(H);
-                tet_term(W, (int)ent_index(ent), (int)ent_role(ent), g, H);   // removed tets stay zero
+                tet_term_record(W, rec0 + base + q, g, H);   // removed tets stay zero
                 sm[0 * nslots + q] = g.x; sm[1 * nslots + q] = g.y; sm[2 * nslots + q] = g.z;
                 sm[3 * nslots + q] = H.xx; sm[4 * nslots + q] = H.yy; sm[5 * nslots + q] = H.zz;
                 sm[6 * nslots + q] = H.xy; sm[7 * nslots + q] = H.xz; sm[8 * nslots + q] = H.yz;
             }
             T.sync();
         }
-        for (int j = v + tid; j < vend; j += nt) {
-            const int b = list[j];
-            if (W.flags[b] & kBodyRemoved) continue;
-            const int e0 = W.inc_off[b], e1 = e0 + W.inc_cnt[b];
-            const int q0 = (j == 0 ? 0 : tinc[j - 1]) - base;
-            if (flat && e1 - e0 == tinc[j] - base - q0 && energy_only_particle(W, b)) {
-                Sys3 s;
-                particle_init_mass(W, b, s);
-                for (int q = q0; q < q0 + e1 - e0; ++q)
-                    particle_add_energy(s, sm[0 * nslots + q], sm[1 * nslots + q], sm[2 * nslots + q],
-                                        sm[3 * nslots + q], sm[4 * nslots + q], sm[5 * nslots + q],
-                                        sm[6 * nslots + q], sm[7 * nslots + q], sm[8 * nslots + q]);
-                particle_finish(W, b, s);
-                continue;
+        if (!flat) {
+            // one particle whose terms alone exceed the slots: evaluated in place
+            for (int j = v + tid; j < vend; j += nt) {
+                const int b = list[j];
+                if (W.flags[b] & kBodyRemoved) continue;
+                flat_finish_body(W, cur, b, W.inc_off[b], W.inc_off[b] + W.inc_cnt[b], -1, alpha, write_stick, sm,
+                                 nslots);
             }
-            flat_finish_body(W, cur, b, e0, e1, flat ? q0 : -1, alpha, write_stick, sm, nslots);
+        } else {
+            // as many lanes per particle as keep the team busy in one pass
+            const int np = vend - v, nw = nt >> 5;
+            if (np <= 3 * nw)
+                flat_finish_split<9>(T, W, cur, list, tinc, base, v, vend, alpha, write_stick, sm, nslots);
+            else if (np <= 10 * nw)
+                flat_finish_split<3>(T, W, cur, list, tinc, base, v, vend, alpha, write_stick, sm, nslots);
+            else
+                flat_finish_split<1>(T, W, cur, list, tinc, base, v, vend, alpha, write_stick, sm, nslots);
         }
         T.sync();
         v = vend;
@@ -405,7 +481,7 @@ __device__ __noinline__ void primal_sweep_flat(const Team& T, const World& W, in
 __device__ __forceinline__ void primal_colour(const Team& T, const World& W, const SceneDesc& sc, int cur,
                                               const int* cs, int c, float alpha, bool write_stick) {
     if (sc.group == kGroupFlat)
-        primal_sweep_flat(T, W, cur, W.col_list + sc.body0, W.col_tinc + sc.body0, W.fterm + 4 * (size_t)sc.tet0,
+        primal_sweep_flat(T, W, cur, W.col_list + sc.body0, W.col_tinc + sc.body0, 4 * (size_t)sc.tet0,
                           cs[c], cs[c + 1], alpha, write_stick);
     else
         primal_sweep_cta_dispatch(T, W, cur, W.col_list + sc.body0 + cs[c], cs[c + 1] - cs[c], alpha, write_stick,
@@ -584,14 +660,14 @@ __device__ __noinline__ bool colour_scene(const Team& T, const World& W, const S
         for (int i = tid; i < n; i += nt) tinc[i] = tet_terms(W, W.col_list[b0 + i]);
         T.sync();
         block_exclusive_scan(T, tinc, tinc, n);
-        // the tet-term entries of every listed particle, in list order
-        uint32_t* fterm = W.fterm + 4 * (size_t)sc.tet0;
+        // the tet-term records of every listed particle, in list order
+        const size_t rec0 = 4 * (size_t)sc.tet0;
         for (int i = tid; i < n; i += nt) {
             const int b = W.col_list[b0 + i];
             const int k = tet_terms(W, b);
             const uint32_t* ent = W.inc + W.inc_off[b] + W.inc_cnt[b] - k;
             const int q0 = tinc[i];
-            for (int e = 0; e < k; ++e) fterm[q0 + e] = ent[e];
+            for (int e = 0; e < k; ++e) write_term_record(W, rec0 + q0 + e, ent[e]);
             tinc[i] = q0 + k;
         }
         T.sync();
