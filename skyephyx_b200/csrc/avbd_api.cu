@@ -28,14 +28,14 @@ namespace {
 
 constexpr int kThreads = 128;
 
-__global__ void k_bp_count(World W) {
+__global__ void k_bp_count(const __grid_constant__ World W) {
     const SceneDesc sc = W.scenes[0];
     for (int b = sc.body0 + blockIdx.x * blockDim.x + threadIdx.x; b < sc.body0 + sc.nbody;
          b += gridDim.x * blockDim.x)
         W.cand_cnt[b] = broadphase_body(W, sc, b, nullptr, 0);
 }
 
-__global__ void k_scan_cand(World W) {
+__global__ void k_scan_cand(const __grid_constant__ World W) {
     __shared__ TeamShared s_team;
     const Team T = Team::cta(&s_team, nullptr, 0);
     const SceneDesc sc = W.scenes[0];
@@ -43,7 +43,7 @@ __global__ void k_scan_cand(World W) {
     if (threadIdx.x == 0) W.sstate[0].need_cand = total;
 }
 
-__global__ void k_bp_write(World W, int cur) {
+__global__ void k_bp_write(const __grid_constant__ World W, int cur) {
     const SceneDesc sc = W.scenes[0];
     for (int b = sc.body0 + blockIdx.x * blockDim.x + threadIdx.x; b < sc.body0 + sc.nbody;
          b += gridDim.x * blockDim.x)
@@ -56,21 +56,21 @@ __global__ void k_bp_write(World W, int cur) {
     }
 }
 
-__global__ void k_narrow(World W, int cur, int ncand, int old_count) {
+__global__ void k_narrow(const __grid_constant__ World W, int cur, int ncand, int old_count) {
     const SceneDesc sc = W.scenes[0];
     for (int c = sc.cand0 + blockIdx.x * blockDim.x + threadIdx.x; c < sc.cand0 + ncand;
          c += gridDim.x * blockDim.x)
         narrowphase_slot(W, sc, W.sstate, c, cur, old_count);
 }
 
-__global__ void k_force_init(World W) {
+__global__ void k_force_init(const __grid_constant__ World W) {
     const SceneDesc sc = W.scenes[0];
     for (int f = sc.force0 + blockIdx.x * blockDim.x + threadIdx.x; f < sc.force0 + sc.nforce;
          f += gridDim.x * blockDim.x)
         if (force_init(W, f)) atomicAdd(&W.sstate[0].topo, 1);
 }
 
-__global__ void k_incidence_colour(World W, int cur) {
+__global__ void k_incidence_colour(const __grid_constant__ World W, int cur) {
     __shared__ TeamShared s_team;
     __shared__ float4 s_count[(kMaxColours + 1 + 3) / 4];   // colour counts
     const Team T = Team::cta(&s_team, s_count, (kMaxColours + 1 + 3) / 4);
@@ -83,7 +83,7 @@ __global__ void k_incidence_colour(World W, int cur) {
     colour_scene_cached(T, W, sc, st, 0, cur);
 }
 
-__global__ void k_predict(World W) {
+__global__ void k_predict(const __grid_constant__ World W) {
     const SceneDesc sc = W.scenes[0];
     for (int b = sc.body0 + blockIdx.x * blockDim.x + threadIdx.x; b < sc.body0 + sc.nbody;
          b += gridDim.x * blockDim.x)
@@ -92,7 +92,8 @@ __global__ void k_predict(World W) {
 
 // One colour of the primal sweep, groups of G lanes per body across the grid.
 template <int G>
-__global__ void k_primal(World W, int cur, int first, int count, float alpha, int write_stick) {
+__global__ void k_primal(const __grid_constant__ World W, int cur, int first, int count, float alpha,
+                         int write_stick) {
     const SceneDesc sc = W.scenes[0];
     const int t = blockIdx.x * blockDim.x + threadIdx.x;
     const int lane = threadIdx.x % G, gid = t / G, ngroups = gridDim.x * blockDim.x / G;
@@ -117,7 +118,7 @@ void launch_primal(int group, const World& W, int cur, int first, int count, flo
     }
 }
 
-__global__ void k_dual(World W, int cur, int nlive, float alpha, int last) {
+__global__ void k_dual(const __grid_constant__ World W, int cur, int nlive, float alpha, int last) {
     const SceneDesc sc = W.scenes[0];
     const int n = sc.nforce + nlive;
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -129,14 +130,14 @@ __global__ void k_dual(World W, int cur, int nlive, float alpha, int last) {
     }
 }
 
-__global__ void k_fracture_reset(World W, int cur, int nlive) {
+__global__ void k_fracture_reset(const __grid_constant__ World W, int cur, int nlive) {
     if (!(W.sstate[0].flags & 8)) return;
     const SceneDesc sc = W.scenes[0];
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nlive; i += gridDim.x * blockDim.x)
         fracture_reset_slot(W, cur, W.live[cur][sc.cand0 + i]);
 }
 
-__global__ void k_fracture_clear(World W) {
+__global__ void k_fracture_clear(const __grid_constant__ World W) {
     if (!(W.sstate[0].flags & 8)) return;
     const SceneDesc sc = W.scenes[0];
     for (int b = sc.body0 + blockIdx.x * blockDim.x + threadIdx.x; b < sc.body0 + sc.nbody;
@@ -144,15 +145,15 @@ __global__ void k_fracture_clear(World W) {
         W.reset_flag[b] = 0;
 }
 
-__global__ void k_flags_clear(World W, int mask) {
+__global__ void k_flags_clear(const __grid_constant__ World W, int mask) {
     if (threadIdx.x == 0) W.sstate[0].flags &= ~mask;
 }
 
-__global__ void k_step_done(World W) {
+__global__ void k_step_done(const __grid_constant__ World W) {
     if (threadIdx.x == 0) W.sstate[0].step += 1;
 }
 
-__global__ void k_velocity(World W) {
+__global__ void k_velocity(const __grid_constant__ World W) {
     const SceneDesc sc = W.scenes[0];
     int acc = 0;
     for (int b = sc.body0 + blockIdx.x * blockDim.x + threadIdx.x; b < sc.body0 + sc.nbody;
@@ -161,7 +162,7 @@ __global__ void k_velocity(World W) {
     if (acc) atomicOr(&W.sstate[0].flags, acc);
 }
 
-__global__ void k_remove_oob(World W) {
+__global__ void k_remove_oob(const __grid_constant__ World W) {
     const SceneDesc sc = W.scenes[0];
     for (int b = sc.body0 + blockIdx.x * blockDim.x + threadIdx.x; b < sc.body0 + sc.nbody;
          b += gridDim.x * blockDim.x) {
@@ -186,7 +187,7 @@ __global__ void k_remove_oob(World W) {
 // RemoveBody / RemoveForce / RemoveEnergy on an uploaded world: the same marks
 // as the out-of-bounds removal, plus a topology bump so the colouring is redone.
 // kind 0 body, 1 force, 2 tet, 3 triangle; idx is the global index.
-__global__ void k_remove_item(World W, int kind, int idx) {
+__global__ void k_remove_item(const __grid_constant__ World W, int kind, int idx) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
     if (kind == 0) {
         W.flags[idx] |= kBodyRemoved;
@@ -207,7 +208,7 @@ __global__ void k_remove_item(World W, int kind, int idx) {
     W.sstate[0].topo += 1;
 }
 
-__global__ void k_collide(World W, int a, int b, uint32_t* ids, float* data, int* n) {
+__global__ void k_collide(const __grid_constant__ World W, int a, int b, uint32_t* ids, float* data, int* n) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
     Collision col;
     collide_box_box(v3(W.pos[a]), q4(W.rot[a]), v3(W.scale[a]), v3(W.pos[b]), q4(W.rot[b]), v3(W.scale[b]), col);
@@ -247,8 +248,8 @@ __device__ __forceinline__ bool scene_fits_half(const World& W, int scene, int t
 }
 
 template <int MAXT, int MINB>
-__global__ void __launch_bounds__(MAXT, MINB) k_batch_step(World W, const int* order, const int* nlive_ptr,
-                                                             int* queue) {
+__global__ void __launch_bounds__(MAXT, MINB) k_batch_step(const __grid_constant__ World W, const int* order,
+                                                             const int* nlive_ptr, int* queue) {
     __shared__ TeamShared s_team[kMaxTeams];
     extern __shared__ float4 s_stage[];
     const int nlive = *nlive_ptr;   // live scenes, read from device memory so the graph stays replayable
@@ -1144,7 +1145,7 @@ int batch_launch_shape(AvbdBatch* b) {
 int batch_build_graph(AvbdBatch* b);
 
 // Shifts the contact bases and live-slot entries of a relocated manifold table.
-__global__ void k_rebase_table(World W, int t, int cand0, int nslot, int nlive, int dk, int dc) {
+__global__ void k_rebase_table(const __grid_constant__ World W, int t, int cand0, int nslot, int nlive, int dk, int dc) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < nslot; i += gridDim.x * blockDim.x) {
         W.kbase[t][cand0 + i] += dk;
         if (i < nlive) W.live[t][cand0 + i] += dc;
@@ -2103,7 +2104,7 @@ static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
 constexpr int kNoAllocMaxDevices = 64;
 NoAllocScratch* g_noalloc_ptr[kNoAllocMaxDevices] = {};
 
-__global__ void k_collide_pairs_noalloc(World W, NoAllocScratch* s, int n, int nbody) {
+__global__ void k_collide_pairs_noalloc(const __grid_constant__ World W, NoAllocScratch* s, int n, int nbody) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
         const int2 ab = make_int2(s->body_a[i], s->body_b[i]);
         uint32_t* ids = s->ids + 8 * i;

@@ -159,28 +159,29 @@ AVBD_HD void eig2(float a00, float a11, float a01, float& w0, float& w1, float& 
     }
 }
 
-// ProjectEigenvalues (math.cpp:137-171)
-AVBD_HD void project_eigenvalues(float* ev, int count, int mode, float rho, float threshold = 0.01f,
-                                 float epsilon = 1e-6f) {
+// ProjectEigenvalues (math.cpp:137-171) of COUNT values; the count is a
+// template argument so the loops unroll and ev stays in registers.
+template <int COUNT>
+AVBD_HD void project_eigenvalues(float* ev, int mode, float rho, float threshold = 0.01f, float epsilon = 1e-6f) {
     bool use_abs = false;
     if (mode == 0) {
-        for (int i = 0; i < count; ++i) ev[i] = fmaxf(epsilon, ev[i]);
-        return;
+        use_abs = false;
     } else if (mode == 1) {
         use_abs = true;
     } else {
         use_abs = fabsf(rho - 1.f) > threshold;
-        if (!use_abs) {
-            for (int i = 0; i < count; ++i) ev[i] = fmaxf(epsilon, ev[i]);
-            return;
-        }
     }
-    for (int i = 0; i < count; ++i) {
+    if (!use_abs) {
+#pragma unroll
+        for (int i = 0; i < COUNT; ++i) ev[i] = fmaxf(epsilon, ev[i]);
+        return;
+    }
+#pragma unroll
+    for (int i = 0; i < COUNT; ++i) {
         ev[i] = fabsf(ev[i]);
         if (ev[i] < epsilon) ev[i] = epsilon;
     }
 }
-
 // Symmetric 3x3 accumulator (upper part implied).
 struct S3 { float xx, yy, zz, xy, xz, yz; };
 AVBD_HD void s3_zero(S3& h) { h.xx = h.yy = h.zz = h.xy = h.xz = h.yz = 0.f; }
@@ -217,13 +218,13 @@ AVBD_HD void vertex_hessian(const M3& U, const M3& V, V3 gradN, float a00, float
         H.xy += b0.y * m0.x + b1.y * m1.x + b2.y * m2.x;
         H.xz += b0.z * m0.x + b1.z * m1.x + b2.z * m2.x;
         H.yz += b0.z * m0.y + b1.z * m1.y + b2.z * m2.y;
-        project_eigenvalues(ev + 3, 6, mode, rho);
+        project_eigenvalues<6>(ev + 3, mode, rho);
     } else {
         V3 w;
         M3 Q;
         eig3(a00, a11, a22, a01, a02, a12, w, Q);
         ev[0] = w.x; ev[1] = w.y; ev[2] = w.z;
-        project_eigenvalues(ev, 9, mode, rho);
+        project_eigenvalues<9>(ev, mode, rho);
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
             V3 c = Q.c[k];
@@ -423,7 +424,7 @@ AVBD_HD void stvk_terms(V3 p0, V3 p1, V3 p2, float4 DmInv, float gnx, float gny,
     const float A01 = lambda * s0 * s1;
     float q00, q10, q01, q11;
     eig2(A00, A11, A01, ev[0], ev[1], q00, q10, q01, q11);
-    project_eigenvalues(ev, 4, mode, rho);
+    project_eigenvalues<4>(ev, mode, rho);
     // ReconstructVertexHessian (math.cpp:324-356)
     const float vg0 = vx0 * gnx + vy0 * gny;
     const float vg1 = vx1 * gnx + vy1 * gny;
