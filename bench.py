@@ -109,8 +109,9 @@ class ClockSampler:
 
 
 # DRAM bytes (read + write) per launch per dynamic body: one ncu capture of
-# the 1,024-scene mix of this workload (5.29 GB over 432,494 dynamic bodies).
-TRAFFIC_PER_DYNAMIC_BODY = 5.288e9 / 432494
+# the 1,024-scene mix of this workload (2.487 GB read + 0.899 GB written over
+# 432,494 dynamic bodies).
+TRAFFIC_PER_DYNAMIC_BODY = 3.386e9 / 432494
 
 
 def build_batch(specs, config_base=4, tuned=None):
