@@ -229,6 +229,14 @@ int32_t avbd_batch_add_scene(AvbdBatch* b, const AvbdWorld* w);
 int32_t avbd_batch_remove_scene(AvbdBatch* b, int32_t scene);
 /* Index of a live scene's first body in the pose buffers of avbd_batch_get_all_poses. */
 int32_t avbd_batch_scene_body_offset(const AvbdBatch* b, int32_t scene);
+/* Allocates the pools for the scenes added so far, chooses the launch shape
+ * and stages the scenes into page-locked host buffers; the next
+ * avbd_batch_step copies them to the device (one copy per device array) and
+ * steps.  Optional: the first avbd_batch_step does the same when it was not
+ * called.  No-op once the pools exist. */
+int32_t avbd_batch_prepare(AvbdBatch* b);
+/* Host-to-device bytes the last upload of staged scenes copied (0 before it). */
+int64_t avbd_batch_uploaded_bytes(const AvbdBatch* b);
 /* Advances every live scene by `steps` steps (one persistent kernel launch per
  * step, replayed from a CUDA graph). Returns AVBD_STATUS_OK or an error. */
 int32_t avbd_batch_step(AvbdBatch* b, int32_t steps);

@@ -92,6 +92,8 @@ SIGNATURES = [
     ("avbd_batch_reserve", [_V, C.c_int64, C.c_int64, C.c_int64, C.c_int64, C.c_int32], C.c_int32),
     ("avbd_batch_scene_body_offset", [_V, C.c_int32], C.c_int32),
     ("avbd_batch_remove_scene", [_V, C.c_int32], C.c_int32),
+    ("avbd_batch_prepare", [_V], C.c_int32),
+    ("avbd_batch_uploaded_bytes", [_V], C.c_int64),
     ("avbd_batch_step", [_V, C.c_int32], C.c_int32),
     ("avbd_batch_num_scenes", [_V], C.c_int32),
     ("avbd_batch_scene_status", [_V, C.c_int32], C.c_int32),

@@ -568,15 +568,14 @@ struct StagedSink {
     struct Buf {
         char* host = nullptr;   // calloc'd: untouched pages read as zero and cost nothing
         size_t cap = 0, lo = SIZE_MAX, hi = 0;
+        bool locked = false;    // [lo, hi) page-locked
     };
     std::map<char*, Buf> bufs;
     const Pools* P = nullptr;   // allocation sizes: each buffer is sized once to its pool array
     cudaStream_t st = nullptr;
     std::mutex m;               // scenes are staged from several host threads
     bool overflow = false;      // a write outside its pool array (never expected)
-    ~StagedSink() {
-        for (auto& kv : bufs) std::free(kv.second.host);
-    }
+    ~StagedSink() { release(); }
     // The host buffer of pool array `dst` with [off, off + n) marked written;
     // null (and overflow set) if that range lies outside the array.
     char* span(void* dst, size_t off, size_t n) {
@@ -610,15 +609,35 @@ struct StagedSink {
         if (char* h = span(dst, at * sizeof(T), n * sizeof(T))) std::memset(h + at * sizeof(T), 0, n * sizeof(T));
     }
     void finish() {}
-    bool flush() {
+    // Page-locks the written range of every buffer, so the copies run at the
+    // link's rate instead of through the driver's pageable bounce buffers.
+    void lock() {
         for (auto& kv : bufs)
-            if (kv.second.hi > kv.second.lo)
+            if (kv.second.hi > kv.second.lo && !kv.second.locked)
+                kv.second.locked = cudaHostRegister(kv.second.host + kv.second.lo, kv.second.hi - kv.second.lo,
+                                                    cudaHostRegisterDefault) == cudaSuccess;
+        cudaGetLastError();   // a refused registration leaves a pageable (slower) copy
+    }
+    // One copy per written range, then the stream is synchronised; the host
+    // buffers are kept until release() (page-locked memory is slow to free).
+    bool flush() {
+        copied = 0;
+        for (auto& kv : bufs)
+            if (kv.second.hi > kv.second.lo) {
                 cudaMemcpyAsync(kv.first + kv.second.lo, kv.second.host + kv.second.lo, kv.second.hi - kv.second.lo,
                                 cudaMemcpyHostToDevice, st);
+                copied += (int64_t)(kv.second.hi - kv.second.lo);
+            }
         cudaStreamSynchronize(st);
-        for (auto& kv : bufs) std::free(kv.second.host);
-        bufs.clear();
         return !overflow;
+    }
+    int64_t copied = 0;   // bytes the last flush copied
+    void release() {
+        for (auto& kv : bufs) {
+            if (kv.second.locked) cudaHostUnregister(kv.second.host + kv.second.lo);
+            std::free(kv.second.host);
+        }
+        bufs.clear();
     }
 };
 
@@ -967,6 +986,11 @@ struct AvbdBatch {
     int* d_fix_order = nullptr;          // catch-up queue
     int* d_fix_n = nullptr;
     float last_ms = 0.f;
+    // Scenes placed and staged into page-locked host buffers by
+    // avbd_batch_prepare, copied to the pools by the next step.
+    std::unique_ptr<StagedSink> upload;
+    bool upload_pending = false;
+    int64_t uploaded_bytes = 0;   // host-to-device bytes of the last staged upload
 };
 
 namespace {
@@ -1082,7 +1106,10 @@ void batch_sync_order(AvbdBatch* b) {
 }
 
 // First step without an explicit reservation: pools sized to the staged scenes.
-int batch_pack(AvbdBatch* b) {
+// Reserves fresh pools for every staged scene, places them, and stages them
+// into page-locked host buffers from all host threads (their ranges are
+// disjoint); the copy waits for batch_flush.
+int batch_stage(AvbdBatch* b) {
     int64_t nb = 0, nf = 0, nt = 0, nr = 0, nsinc = 0, nsp = 0;
     for (size_t i = 0; i < b->scenes.size(); ++i) {
         if (b->state[i] != 2) continue;
@@ -1093,15 +1120,15 @@ int batch_pack(AvbdBatch* b) {
     }
     int r = batch_reserve(b, nb, nf, nt, nr, (int64_t)b->scenes.size(), nsinc, nsp);
     if (r) return r;
-    // fresh pools: place every scene, stage them into host arrays from all host
-    // threads (their ranges are disjoint), then one copy per device array
     std::vector<int> slots;
     for (size_t i = 0; i < b->scenes.size(); ++i)
         if (b->state[i] == 2) {
             if ((r = batch_place(b, (int)i))) return r;
             slots.push_back((int)i);
         }
-    StagedSink staged;
+    if (b->upload) b->upload->release();
+    b->upload.reset(new StagedSink());
+    StagedSink& staged = *b->upload;
     staged.st = b->stream;
     staged.P = &b->P;
     std::atomic<size_t> next{0};
@@ -1113,13 +1140,25 @@ int batch_pack(AvbdBatch* b) {
     for (unsigned t = 1; t < nthreads && slots.size() > 64; ++t) pool.emplace_back(work);
     work();
     for (auto& th : pool) th.join();
-    if (!staged.flush()) return AVBD_ERR_STATE;
+    if (staged.overflow) return AVBD_ERR_STATE;
+    staged.lock();
     for (int i : slots) {
         b->state[i] = 1;
         if ((int)b->steps_due.size() <= i) b->steps_due.resize(i + 1, 0);
         b->steps_due[i] = 0;
+        b->scenes[i] = HostScene();   // the staged copy is what is uploaded
     }
+    b->upload_pending = true;
     b->order_dirty = true;
+    return cudaGetLastError() == cudaSuccess ? 0 : AVBD_ERR_CUDA;
+}
+
+// Copies the staged scenes into the pools (one copy per device array).
+int batch_flush(AvbdBatch* b) {
+    if (!b->upload_pending) return 0;
+    b->upload_pending = false;
+    if (!b->upload->flush()) return AVBD_ERR_STATE;
+    b->uploaded_bytes = b->upload->copied;
     return cudaGetLastError() == cudaSuccess ? 0 : AVBD_ERR_CUDA;
 }
 
@@ -1805,6 +1844,7 @@ int32_t avbd_batch_destroy(AvbdBatch* b) {
     cudaSetDevice(b->device);
     if (b->stream) cudaStreamSynchronize(b->stream);
     batch_drop_graph(b);
+    if (b->upload) b->upload->release();
     if (b->d_order) cudaFree(b->d_order);
     if (b->d_nlive) cudaFree(b->d_nlive);
     if (b->d_queue) cudaFree(b->d_queue);
@@ -1873,14 +1913,22 @@ int32_t avbd_batch_remove_scene(AvbdBatch* b, int32_t scene) {
     return 0;
 }
 
+int32_t avbd_batch_prepare(AvbdBatch* b) {
+    if (!b) return AVBD_ERR_INVALID;
+    if (b->reserved) return 0;
+    int r = batch_stage(b);
+    if (r) return r;
+    cudaSetDevice(b->device);
+    if (!b->grid) batch_launch_shape(b);
+    return cudaGetLastError() == cudaSuccess ? 0 : AVBD_ERR_CUDA;
+}
+
 int32_t avbd_batch_step(AvbdBatch* b, int32_t steps) {
     if (!b || steps < 0) return AVBD_ERR_INVALID;
     int r;
-    if (!b->reserved) {
-        if ((r = batch_pack(b))) return r;
-        for (auto& h : b->scenes) h = HostScene();
-    }
+    if (!b->reserved && (r = batch_stage(b))) return r;
     cudaSetDevice(b->device);
+    if ((r = batch_flush(b))) return r;
     batch_sync_order(b);
     if (!b->grid) batch_launch_shape(b);
     b->P.W.P = to_params(b->params);
@@ -2007,6 +2055,8 @@ int64_t avbd_scene_footprint_bytes(const AvbdWorld* w) {
     bytes += sizeof(SceneDesc) + sizeof(SceneState) + 4 * (kMaxColours + 1);
     return bytes;
 }
+
+int64_t avbd_batch_uploaded_bytes(const AvbdBatch* b) { return b ? b->uploaded_bytes : AVBD_ERR_INVALID; }
 
 int32_t avbd_batch_set_launch(AvbdBatch* b, int32_t threads, int32_t ctas_per_sm) {
     if (!b || threads < 0 || ctas_per_sm < 0 || (threads && (threads % 32 || threads > 1024))) return AVBD_ERR_INVALID;

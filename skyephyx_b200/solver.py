@@ -328,6 +328,17 @@ class Batch:
     def remove_scene(self, scene: int):
         check(self._lib.avbd_batch_remove_scene(self._h, int(scene)), "batch_remove_scene")
 
+    def prepare(self):
+        """Allocates the pools for the scenes added so far and stages them in
+        page-locked host memory; the next step() copies them to the device.
+        Optional (the first step() does it otherwise)."""
+        check(self._lib.avbd_batch_prepare(self._h), "batch_prepare")
+
+    @property
+    def uploaded_bytes(self) -> int:
+        """Host-to-device bytes the last upload of staged scenes copied."""
+        return int(self._lib.avbd_batch_uploaded_bytes(self._h))
+
     def step(self, steps: int = 1) -> str:
         r = check(self._lib.avbd_batch_step(self._h, int(steps)), "batch_step")
         return STATUS.get(r, str(r))

@@ -240,3 +240,23 @@ def alone_steps(build, steps):
     b.add_scene(staged(build))
     assert b.step(steps) == "ok"
     return b.get_state(0)[:2]
+
+
+def test_prepare_then_step_equals_step():
+    """avbd_batch_prepare (pools, launch and page-locked staging ahead of the
+    first step) changes nothing in the results."""
+    from skyephyx_b200 import Batch
+    builders = mix_builders()
+    runs = []
+    for prep in (False, True):
+        b = Batch()
+        keep = [staged(f) for f in builders]
+        for w in keep:
+            b.add_scene(w)
+        if prep:
+            b.prepare()
+            b.prepare()   # a second call is a no-op
+        assert b.step(3) == "ok"
+        runs.append([b.get_state(i)[:2] for i in range(len(builders))])
+    for a, c in zip(*runs):
+        assert same(a, c)
