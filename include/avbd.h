@@ -155,9 +155,16 @@ int32_t avbd_num_bodies(const AvbdWorld* w);
 int32_t avbd_num_dynamic_bodies(const AvbdWorld* w);
 /* Solver::emergencyStop (solver.hpp:84). */
 int32_t avbd_emergency_stop(const AvbdWorld* w);
+/* 1 while joint/spring `force` takes part in the step; 0 once a fracture
+ * disabled it (Force::Disable, force.hpp:57-66; solver.cpp:473-481) or it was
+ * removed with a body.  The reference's caller sees the same by the Force
+ * leaving Solver::solverForces. */
+int32_t avbd_force_live(AvbdWorld* w, int32_t force);
 
 /* Body state by id into caller-owned HOST buffers (any may be NULL):
- * pos n*3, quat n*4 (w,x,y,z), vel n*3, omega n*3; n = avbd_num_bodies(). */
+ * pos n*3, quat n*4 (w,x,y,z), vel n*3, omega n*3; n = avbd_num_bodies().
+ * A removed body (avbd_remove_body, or out of bounds, solver.cpp:521-534)
+ * reads NaN. */
 int32_t avbd_get_state(AvbdWorld* w, float* pos, float* quat_wxyz, float* vel, float* omega);
 /* Overwrites body state (e.g. to restore a snapshot); NULL leaves a field as is. */
 int32_t avbd_set_state(AvbdWorld* w, const float* pos, const float* quat_wxyz, const float* vel,
@@ -198,11 +205,13 @@ int32_t avbd_collide(AvbdWorld* w, int32_t body_a, int32_t body_b, uint32_t* ids
  * one fixed array of about 1.9 MB that every GPU loading this library holds
  * until exit. Outputs go to caller-owned host buffers: ids[8n] (unused =
  * 0xFFFFFFFF), data[8*13*n] (as avbd_collide), counts[n]. The world must have
- * been uploaded (stepped, or avbd_collide called, once). The first call on a
- * device looks up the scratch address, so make it before any stream capture.
- * Calls share the scratch: calls that overlap on the GPU (several threads, or
- * several worlds on one device) race. More pairs than the maximum, or an
- * unknown body id, return AVBD_ERR_INVALID. */
+ * been uploaded (stepped, or avbd_collide called, once). The call copies the
+ * pairs in from host memory and returns once the results are in the host
+ * buffers. The first call on a device looks up the scratch address, so make
+ * it before any stream capture. Calls share the scratch: calls that overlap
+ * on the GPU (several threads, or several worlds on one device) race. More
+ * pairs than the maximum, or an unknown body id, return AVBD_ERR_INVALID.
+ * The caller's current device is left as it was. */
 #define AVBD_COLLIDE_NOALLOC_MAX_PAIRS 4096
 int32_t avbd_collide_noalloc(AvbdWorld* w, int32_t n, const int32_t* body_a, const int32_t* body_b, uint32_t* ids,
                              float* data, int32_t* counts);
@@ -230,10 +239,12 @@ int32_t avbd_batch_remove_scene(AvbdBatch* b, int32_t scene);
 /* Index of a live scene's first body in the pose buffers of avbd_batch_get_all_poses. */
 int32_t avbd_batch_scene_body_offset(const AvbdBatch* b, int32_t scene);
 /* Allocates the pools for the scenes added so far, chooses the launch shape
- * and stages the scenes into page-locked host buffers; the next
- * avbd_batch_step copies them to the device (one copy per device array) and
- * steps.  Optional: the first avbd_batch_step does the same when it was not
- * called.  No-op once the pools exist. */
+ * and stages the scenes into page-locked host buffers; the scenes are copied
+ * to the device (one copy per device array) by the next batch call that
+ * touches the device: usually the first avbd_batch_step.  The page-locked
+ * buffers are held until avbd_batch_destroy.  Optional: the first
+ * avbd_batch_step stages through pageable buffers, freed after the copy,
+ * when it was not called.  No-op once the pools exist. */
 int32_t avbd_batch_prepare(AvbdBatch* b);
 /* Host-to-device bytes the last upload of staged scenes copied (0 before it). */
 int64_t avbd_batch_uploaded_bytes(const AvbdBatch* b);

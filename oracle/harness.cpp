@@ -19,7 +19,10 @@
 #include <cmath>
 #include <cstdint>
 #include <cstring>
+#include <limits>
 #include <thread>
+#include <unordered_map>
+#include <unordered_set>
 #include <vector>
 
 #include "physics/solver.hpp"
@@ -38,10 +41,10 @@ const float kMaxVelocity = 500.0f;                    // solver.cpp:15
 
 struct Orc {
     Solver solver;
-    std::vector<Mesh*> bodies;     // by creation id
+    std::vector<Mesh*> bodies;     // by creation id; null once the body is removed
     std::vector<Force*> forces;    // user forces by creation id
     std::vector<Energy*> energies; // by creation id
-    std::vector<int> colour;       // by body creation id, -1 = static/uncoloured
+    std::vector<int> colour;       // by body creation id, -1 = static/uncoloured/removed
     int num_colours = 0;
     double phase_ms[8] = {0};
 };
@@ -53,7 +56,7 @@ uint32_t colour_hash(uint32_t x) {
 }
 
 // CPU twin of the device colouring: greedy first-fit in priority order, where
-// priority is (degree descending, hash(local index), local index), degree
+// priority is (degree descending, hash(creation id), creation id), degree
 // being the number of forces and energies a body takes part in; then one
 // iterated-greedy pass (priority: first-pass colour descending, then as
 // before).  Edges join dynamic bodies that share a force (manifold, joint,
@@ -61,6 +64,15 @@ uint32_t colour_hash(uint32_t x) {
 void colour_bodies(Orc& o) {
     Solver& s = o.solver;
     const int n = (int)s.bodyPtrs.size();
+    // creation id of each body by solver index (they differ once a body was
+    // swap-removed, solver.cpp:104-115; the device keeps creation ids)
+    std::vector<int> cid(n, -1);
+    {
+        std::unordered_map<const Mesh*, int> id;
+        for (size_t i = 0; i < o.bodies.size(); ++i)
+            if (o.bodies[i]) id[o.bodies[i]] = (int)i;
+        for (int i = 0; i < n; ++i) cid[i] = id.count(s.bodyPtrs[i]) ? id[s.bodyPtrs[i]] : i;
+    }
     std::vector<std::vector<int>> adj(n);
     auto link = [&](const std::vector<Mesh*>& lb) {
         for (size_t a = 0; a < lb.size(); ++a)
@@ -83,8 +95,9 @@ void colour_bodies(Orc& o) {
     for (int i = 0; i < n; ++i) order[i] = i;
     std::sort(order.begin(), order.end(), [&](int a, int b) {
         if (deg[a] != deg[b]) return deg[a] > deg[b];
-        uint32_t ha = colour_hash((uint32_t)a), hb = colour_hash((uint32_t)b);
-        return ha != hb ? ha < hb : a < b;
+        const int ca = cid[a], cb = cid[b];
+        uint32_t ha = colour_hash((uint32_t)ca), hb = colour_hash((uint32_t)cb);
+        return ha != hb ? ha < hb : ca < cb;
     });
     auto greedy = [&](const std::vector<int>& ord, std::vector<int>& col) {
         col.assign(n, -1);
@@ -110,8 +123,24 @@ void colour_bodies(Orc& o) {
         std::stable_sort(order.begin(), order.end(), [&](int a, int b) { return prev[a] > prev[b]; });
         ncol = greedy(order, col);
     }
-    o.colour = col;
+    o.colour.assign(o.bodies.size(), -1);
+    for (int i = 0; i < n; ++i)
+        if (cid[i] >= 0 && cid[i] < (int)o.colour.size()) o.colour[cid[i]] = col[i];
     o.num_colours = ncol;
+}
+
+// Creation ids whose body or user force the solver no longer holds become
+// null: bodies removed out of bounds (solver.cpp:530-534), forces dropped by
+// Initialize() after a fracture disabled them (:293-294) or destroyed with
+// their body (geometry.cpp:11-25).
+void forget_removed(Orc& o) {
+    std::unordered_set<const Mesh*> live(o.solver.bodyPtrs.begin(), o.solver.bodyPtrs.end());
+    for (Mesh*& m : o.bodies)
+        if (m && !live.count(m)) m = nullptr;
+    std::unordered_set<const Force*> held;
+    for (auto& f : o.solver.solverForces) held.insert(f.get());
+    for (Force*& f : o.forces)
+        if (f && !held.count(f)) f = nullptr;
 }
 
 // One primal block update of one body (solver.cpp:394-448; post-stab form
@@ -226,13 +255,14 @@ int step_coloured(Orc& o, int identity_order) {
     std::vector<Mesh*> sweep;
     if (identity_order) {
         for (Mesh* m : s.bodyPtrs) sweep.push_back(m);
-        o.colour.assign(N, -1);
+        o.colour.assign(o.bodies.size(), -1);
         o.num_colours = 0;
     } else {
         colour_bodies(o);
+        // ascending colour, ascending creation id within a colour
         for (int c = 0; c < o.num_colours; ++c)
-            for (int i = 0; i < N; ++i)
-                if (o.colour[i] == c) sweep.push_back(s.bodyPtrs[i]);
+            for (size_t i = 0; i < o.bodies.size(); ++i)
+                if (o.bodies[i] && o.colour[i] == c) sweep.push_back(o.bodies[i]);
     }
     o.phase_ms[2] = ms_since(tp);
 
@@ -337,9 +367,22 @@ int step_coloured(Orc& o, int identity_order) {
             break;
         }
     }
-    if (s.emergencyStop) return 1;
+    if (s.emergencyStop) { forget_removed(o); return 1; }
     o.phase_ms[5] = ms_since(tp);
-    for (Mesh* m : oob) s.RemoveBody(m);
+    if (!oob.empty()) {
+        // The post-stabilisation sweep visits the surviving bodies only: the
+        // reference walks bodyPtrs as RemoveBody's swap leaves it (identity
+        // order), the coloured harness keeps its colour order.
+        std::unordered_set<const Mesh*> gone(oob.begin(), oob.end());
+        std::vector<Mesh*> kept;
+        for (Mesh* m : sweep)
+            if (!gone.count(m)) kept.push_back(m);
+        sweep.swap(kept);
+        for (size_t i = 0; i < o.bodies.size(); ++i)
+            if (gone.count(o.bodies[i])) { o.bodies[i] = nullptr; if (i < o.colour.size()) o.colour[i] = -1; }
+        for (Mesh* m : oob) s.RemoveBody(m);
+        if (identity_order) sweep.assign(s.bodyPtrs.begin(), s.bodyPtrs.end());
+    }
 
     tp = std::chrono::steady_clock::now();
     if (s.postStabilization)                                                // :536-597
@@ -349,6 +392,7 @@ int step_coloured(Orc& o, int identity_order) {
         }
     o.phase_ms[6] = ms_since(tp);
     o.phase_ms[7] = ms_since(t0);
+    forget_removed(o);
     return 0;
 }
 
@@ -619,6 +663,7 @@ int orc_step(void* h) {
     Orc* o = static_cast<Orc*>(h);
     if (o->solver.emergencyStop) return 1;
     o->solver.Step();
+    forget_removed(*o);
     return o->solver.emergencyStop ? 1 : 0;
 }
 
@@ -650,11 +695,88 @@ int orc_num_dynamic(void* h) {
 }
 int orc_emergency_stop(void* h) { return static_cast<Orc*>(h)->solver.emergencyStop ? 1 : 0; }
 
-// Poses by creation id: pos (n x 3), quat (n x 4, w x y z), vel/omega (n x 3).
+// Long-horizon measures of the current state, from the reference's own
+// routines, so that a GPU run (its poses written in with orc_set_state) and
+// the FP64 run are measured the same way:
+//   out[0] max |C| over hard rows (infinite stiffness: the joints' locked
+//          rows) at alpha = 0, i.e. the raw positional / torque-arm-scaled
+//          angular violation (Joint::ComputeConstraints, joint.cpp:97-124);
+//          soft rows (springs, a hinge's free rows) are not constraints;
+//   out[1] deepest penetration over every overlapping body pair: the
+//          broadphase sphere test (solver.cpp:233-256), then
+//          CollisionSpace::CollisionBoxBox (collision.cpp:271-447);
+//   out[2] kinetic energy, 1/2 m v.v + 1/2 w.(R I R^T) w of dynamic bodies;
+//   out[3] gravitational potential energy, m 9.81 y of dynamic bodies;
+//   out[4] elastic energy, the sum of Energy::cachedEnergy after
+//          ComputeEnergyTerms(nullptr, ...) (the warm start, solver.cpp:299-322);
+//   out[5] dynamic bodies whose position is not finite.
+void orc_metrics(void* h, double* out) {
+    Orc* o = static_cast<Orc*>(h);
+    Solver& s = o->solver;
+    s.RebuildPtrCaches();
+    double maxC = 0.0, maxPen = 0.0, kin = 0.0, pot = 0.0, ela = 0.0, bad = 0.0;
+    for (auto& fp : s.solverForces) {
+        Force* f = fp.get();
+        if (f->isManifold || f->disabled) continue;
+        f->ComputeConstraints(0.0f);
+        for (int i = 0; i < f->numConstraints(); ++i) {
+            if (!std::isinf(f->constraintPoints[i].stiffness)) continue;
+            const double c = std::abs((double)f->constraintPoints[i].C);
+            if (c > maxC || c != c) maxC = c;
+        }
+    }
+    const int N = (int)s.bodyPtrs.size();
+    for (int i = 0; i < N; ++i)
+        for (int j = i + 1; j < N; ++j) {
+            Mesh* a = s.bodyPtrs[i];
+            Mesh* b = s.bodyPtrs[j];
+            if (a->isStatic && b->isStatic) continue;
+            const double d = (a->transform.GetPosition() - b->transform.GetPosition()).norm();
+            if (!(d < (double)(a->detectionRadius + b->detectionRadius))) continue;
+            CollisionResult r = CollisionSpace::CollisionBoxBox(a, b);
+            for (int k = 0; k < r.numContacts; ++k)
+                maxPen = std::max(maxPen, (double)r.contactPoints[k].penetration);
+        }
+    for (Mesh* m : s.bodyPtrs) {
+        if (m->isStatic) continue;
+        const Eigen::Vector3f p = m->transform.GetPosition();
+        if (!std::isfinite(p.x()) || !std::isfinite(p.y()) || !std::isfinite(p.z())) { bad += 1.0; continue; }
+        kin += 0.5 * (double)m->mass * (double)m->velocity.squaredNorm();
+        const Eigen::Matrix3f R = m->transform.GetRotation().toRotationMatrix();
+        const Eigen::Vector3f Iw = R * (m->inertiaTensorBody * (R.transpose() * m->angularVelocity));
+        kin += 0.5 * (double)m->angularVelocity.dot(Iw);
+        pot += (double)m->mass * 9.81 * (double)p.y();
+    }
+    for (auto& ep : s.solverEnergies) {
+        ep->ComputeEnergyTerms(nullptr, s.projectionMode, s.trustRegionRho);
+        ela += (double)ep->GetCachedEnergy();
+    }
+    out[0] = maxC; out[1] = maxPen; out[2] = kin; out[3] = pot; out[4] = ela; out[5] = bad;
+}
+
+// 1 while user force `id` (a joint or spring) takes part in the step; 0 once
+// a fracture disabled it (force.hpp:57-66) or the solver dropped it.
+int orc_force_live(void* h, int id) {
+    Orc* o = static_cast<Orc*>(h);
+    if (id < 0 || id >= (int)o->forces.size()) return -1;
+    const Force* f = o->forces[id];
+    return f && !f->disabled ? 1 : 0;
+}
+
+// Poses by creation id: pos (n x 3), quat (n x 4, w x y z), vel/omega (n x 3);
+// a removed body reads NaN.
 void orc_get_state(void* h, float* pos, float* quat, float* vel, float* omega) {
     Orc* o = static_cast<Orc*>(h);
+    const float nan = std::numeric_limits<float>::quiet_NaN();
     for (size_t i = 0; i < o->bodies.size(); ++i) {
         Mesh* m = o->bodies[i];
+        if (!m) {
+            if (pos) for (int k = 0; k < 3; ++k) pos[3 * i + k] = nan;
+            if (quat) for (int k = 0; k < 4; ++k) quat[4 * i + k] = nan;
+            if (vel) for (int k = 0; k < 3; ++k) vel[3 * i + k] = nan;
+            if (omega) for (int k = 0; k < 3; ++k) omega[3 * i + k] = nan;
+            continue;
+        }
         Eigen::Vector3f p = m->transform.GetPosition();
         Quaternionf q = m->transform.GetRotation();
         if (pos) { pos[3 * i] = p.x(); pos[3 * i + 1] = p.y(); pos[3 * i + 2] = p.z(); }
@@ -669,6 +791,7 @@ void orc_set_state(void* h, const float* pos, const float* quat, const float* ve
     Orc* o = static_cast<Orc*>(h);
     for (size_t i = 0; i < o->bodies.size(); ++i) {
         Mesh* m = o->bodies[i];
+        if (!m) continue;
         if (pos) m->transform.SetPosition(Eigen::Vector3f(pos[3 * i], pos[3 * i + 1], pos[3 * i + 2]));
         if (quat) m->transform.SetRotation(Quaternionf(quat[4 * i], quat[4 * i + 1], quat[4 * i + 2], quat[4 * i + 3]));
         if (vel) m->velocity = Eigen::Vector3f(vel[3 * i], vel[3 * i + 1], vel[3 * i + 2]);
@@ -688,6 +811,7 @@ int orc_get_contacts(void* h, int max_manifolds, int* pairs, int* counts, uint32
         if (n < max_manifolds) {
             int ia = -1, ib = -1;
             for (size_t i = 0; i < o->bodies.size(); ++i) {
+                if (!o->bodies[i]) continue;
                 if (o->bodies[i] == m->bodyA) ia = (int)i;
                 if (o->bodies[i] == m->bodyB) ib = (int)i;
             }

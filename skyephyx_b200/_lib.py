@@ -79,6 +79,7 @@ SIGNATURES = [
     ("avbd_num_bodies", [_V], C.c_int32),
     ("avbd_num_dynamic_bodies", [_V], C.c_int32),
     ("avbd_emergency_stop", [_V], C.c_int32),
+    ("avbd_force_live", [_V, C.c_int32], C.c_int32),
     ("avbd_get_state", [_V, _F, _F, _F, _F], C.c_int32),
     ("avbd_set_state", [_V, _F, _F, _F, _F], C.c_int32),
     ("avbd_get_contacts", [_V, C.c_int32, _I, _I, _U, _F], C.c_int32),

@@ -4,25 +4,32 @@
 
 nvcc compiles device code for ``sm_100a`` only (no PTX for other targets).
 Host code is compiled with ``-ffp-contract=off`` so the scene staging rounds
-exactly like the reference's constructors.
+exactly like the reference's constructors.  The translation units (the host
+side, and one per build of the batched persistent kernel) compile in
+parallel.
 """
 from __future__ import annotations
 
 import os
 import subprocess
 import sys
+from concurrent.futures import ThreadPoolExecutor
 
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libavbd.so")
-SOURCES = ["avbd_api.cu", "avbd_host.cpp"]
-HEADERS = ["avbd_common.cuh", "avbd_narrow.cuh", "avbd_fem.cuh", "avbd_phases.cuh", "avbd_step.cuh", "avbd_host.h"]
+# (object name, source, extra flags)
+UNITS = [("avbd_api", "avbd_api.cu", []), ("avbd_host", "avbd_host.cpp", [])] + [
+    (f"avbd_batch_v{i}", "avbd_batch_v.cu", [f"-DAVBD_BATCH_ID={i}"]) for i in range(1, 8)]
+SOURCES = sorted({u[1] for u in UNITS})
+HEADERS = ["avbd_common.cuh", "avbd_narrow.cuh", "avbd_fem.cuh", "avbd_phases.cuh", "avbd_step.cuh", "avbd_host.h",
+           "avbd_batch.h"]
 
 NVCC_FLAGS = [
     "-gencode", "arch=compute_100a,code=sm_100a",
     "-O3", "-lineinfo", "-std=c++17",
     "-Xcompiler", "-fPIC", "-Xcompiler", "-ffp-contract=off",
-    "-Xptxas", "-warn-spills",
+    "-Xptxas", "-warn-spills", "-Xfatbin=-compress-all",
 ]
 
 
@@ -43,23 +50,41 @@ def _stale() -> bool:
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
-def build(force: bool = False, verbose: bool = False) -> str:
+def build(force: bool = False, verbose: bool = False, csrc: str = CSRC, lib: str = LIB) -> str:
     """Compiles libavbd.so if any source is newer than it; returns its path."""
-    if not force and not _stale():
-        return LIB
-    objs = []
-    for src in SOURCES:
-        obj = os.path.join(CSRC, os.path.splitext(src)[0] + ".o")
-        cmd = [_nvcc(), *NVCC_FLAGS, "-c", os.path.join(CSRC, src), "-o", obj]
+    if not force and lib == LIB and not _stale():
+        return lib
+
+    def compile_unit(unit):
+        name, src, extra = unit
+        obj = os.path.join(csrc, name + ".o")
+        cmd = [_nvcc(), *NVCC_FLAGS, *extra, "-c", os.path.join(csrc, src), "-o", obj]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
-        subprocess.run(cmd, check=True)
+        r = subprocess.run(cmd, capture_output=True, text=True)
+        return obj, r
+
+    jobs = max(1, min(len(UNITS), os.cpu_count() or 1))
+    with ThreadPoolExecutor(jobs) as ex:
+        results = list(ex.map(compile_unit, UNITS))
+    objs = []
+    failed = None
+    for obj, r in results:
+        if verbose or r.returncode:
+            sys.stderr.write(r.stdout + r.stderr)
+        if r.returncode and failed is None:
+            failed = r
         objs.append(obj)
-    cmd = [_nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-o", LIB, "-lcudart"]
+    if failed is not None:
+        for o in objs:
+            if os.path.exists(o):
+                os.remove(o)
+        raise subprocess.CalledProcessError(failed.returncode, failed.args, failed.stdout, failed.stderr)
+    cmd = [_nvcc(), "-shared", "-gencode", "arch=compute_100a,code=sm_100a", *objs, "-o", lib, "-lcudart"]
     subprocess.run(cmd, check=True)
     for o in objs:
         os.remove(o)
-    return LIB
+    return lib
 
 
 if __name__ == "__main__":

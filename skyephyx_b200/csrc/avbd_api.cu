@@ -8,6 +8,7 @@
 #include <cstdio>
 #include <cstdlib>
 #include <cstring>
+#include <limits>
 #include <map>
 #include <memory>
 #include <mutex>
@@ -18,6 +19,7 @@
 #include "../../include/avbd.h"
 #include "avbd_host.h"
 #include "avbd_step.cuh"
+#include "avbd_batch.h"
 
 using namespace avbd;
 
@@ -226,57 +228,9 @@ __global__ void k_collide(const __grid_constant__ World W, int a, int b, uint32_
 }
 
 // ===========================================================================
-// Batched path: one persistent kernel per step; each CTA pulls scenes from a
-// size-ordered queue and runs a scene's whole step.
+// Batched path: the persistent kernel builds live in their own translation
+// units (avbd_batch_v.cu, compiled once per build); this table indexes them.
 // ===========================================================================
-// MAXT is the largest CTA the build serves and MINB sets its register budget
-// (about 65536 / (MAXT * MINB) per thread).  The 256-thread builds keep a
-// step in about 156 (MINB 1), 128, 80 or 64 registers; the 512- and
-// 1024-thread builds give a large scene more lanes.  The autotuner picks one.
-//
-// A CTA starts as one team pulling scenes from the queue (largest first).  A
-// scene whose work (bodies + tets) is at most team_work per lane of half the
-// team is run by the lower half while the upper half, now a team of its own,
-// pulls the next scene; teams keep splitting this way down to
-// Team::min_size(), so small scenes run several to a CTA without waiting on
-// each other's barriers.
-__device__ __forceinline__ bool scene_fits_half(const World& W, int scene, int team_size) {
-    const SceneDesc& d = W.scenes[scene];
-    const int work = d.ntet > 0 ? W.fem_team_work : W.team_work;
-    if (work <= 0 || team_size / 2 < Team::min_size()) return false;
-    return (long long)(d.nbody + d.ntet) <= (long long)work * (team_size / 2);
-}
-
-template <int MAXT, int MINB>
-__global__ void __launch_bounds__(MAXT, MINB) k_batch_step(const __grid_constant__ World W, const int* order,
-                                                             const int* nlive_ptr, int* queue) {
-    __shared__ TeamShared s_team[kMaxTeams];
-    extern __shared__ float4 s_stage[];
-    const int nlive = *nlive_ptr;   // live scenes, read from device memory so the graph stays replayable
-    Team T = Team::cta(s_team, s_stage, W.stage_bodies);
-    int scene = -1;
-    for (;;) {
-        if (scene < 0) {
-            if (T.rank == 0) T.sh->q = atomicAdd(queue, 1);
-            T.sync();
-            const int q = T.sh->q;
-            T.sync();
-            if (q >= nlive) break;
-            scene = order[q];
-        }
-        if (scene_fits_half(W, scene, T.size)) {
-            const bool lower = T.rank < T.size / 2;
-            T = T.half(lower, s_team);
-            if (!lower) scene = -1;
-            continue;
-        }
-        scene_step(W, scene, T);
-        T.sync();
-        scene = -1;
-    }
-}
-
-using BatchKernel = void (*)(World, const int*, const int*, int*);
 struct BatchVariant {
     BatchKernel fn;
     int max_threads;
@@ -284,9 +238,9 @@ struct BatchVariant {
 // Index = register variant of avbd_batch_set_kernel.
 const BatchVariant kBatchVariants[] = {
     {nullptr, 0},
-    {k_batch_step<256, 1>, 256}, {k_batch_step<256, 2>, 256}, {k_batch_step<256, 3>, 256},
-    {k_batch_step<256, 4>, 256}, {k_batch_step<512, 1>, 512}, {k_batch_step<512, 2>, 512},
-    {k_batch_step<1024, 1>, 1024},
+    {batch_kernel_v1(), 256}, {batch_kernel_v2(), 256}, {batch_kernel_v3(), 256},
+    {batch_kernel_v4(), 256}, {batch_kernel_v5(), 512}, {batch_kernel_v6(), 512},
+    {batch_kernel_v7(), 1024},
 };
 constexpr int kNumBatchVariants = 7;
 
@@ -750,6 +704,7 @@ struct AvbdWorld {
     HostScene h;
     bool uploaded = false;
     bool stopped = false;
+    int stop_status = AVBD_STATUS_OK;   // EXPLODED or NAN once stopped
     Pools P;
     std::vector<SceneDesc> descs;
     int group = 0;   // lanes per body in the primal (0 = by scene kind)
@@ -832,7 +787,7 @@ float ev_ms(cudaEvent_t a, cudaEvent_t b) {
 }
 
 int world_step(AvbdWorld* w) {
-    if (w->stopped) return AVBD_STATUS_EXPLODED;
+    if (w->stopped) return w->stop_status;
     if (!w->uploaded) {
         int r = upload(w);
         if (r) return r;
@@ -920,6 +875,7 @@ int world_step(AvbdWorld* w) {
     else if (w->st.flags & 2) status = AVBD_STATUS_NAN;
     if (status != AVBD_STATUS_OK) {
         w->stopped = true;
+        w->stop_status = status;
         cudaStreamSynchronize(s);
         return status;
     }
@@ -990,6 +946,7 @@ struct AvbdBatch {
     // avbd_batch_prepare, copied to the pools by the next step.
     std::unique_ptr<StagedSink> upload;
     bool upload_pending = false;
+    bool upload_pinned = false;   // the staging buffers are page-locked
     int64_t uploaded_bytes = 0;   // host-to-device bytes of the last staged upload
 };
 
@@ -1109,7 +1066,7 @@ void batch_sync_order(AvbdBatch* b) {
 // Reserves fresh pools for every staged scene, places them, and stages them
 // into page-locked host buffers from all host threads (their ranges are
 // disjoint); the copy waits for batch_flush.
-int batch_stage(AvbdBatch* b) {
+int batch_stage(AvbdBatch* b, bool pin) {
     int64_t nb = 0, nf = 0, nt = 0, nr = 0, nsinc = 0, nsp = 0;
     for (size_t i = 0; i < b->scenes.size(); ++i) {
         if (b->state[i] != 2) continue;
@@ -1141,7 +1098,8 @@ int batch_stage(AvbdBatch* b) {
     work();
     for (auto& th : pool) th.join();
     if (staged.overflow) return AVBD_ERR_STATE;
-    staged.lock();
+    if (pin) staged.lock();
+    b->upload_pinned = pin;
     for (int i : slots) {
         b->state[i] = 1;
         if ((int)b->steps_due.size() <= i) b->steps_due.resize(i + 1, 0);
@@ -1159,6 +1117,10 @@ int batch_flush(AvbdBatch* b) {
     b->upload_pending = false;
     if (!b->upload->flush()) return AVBD_ERR_STATE;
     b->uploaded_bytes = b->upload->copied;
+    // pageable staging is not kept; page-locked staging (avbd_batch_prepare)
+    // is held until the batch is destroyed, since unpinning it costs about as
+    // much as the copy
+    if (!b->upload_pinned) b->upload.reset();
     return cudaGetLastError() == cudaSuccess ? 0 : AVBD_ERR_CUDA;
 }
 
@@ -1694,7 +1656,32 @@ int32_t avbd_get_state(AvbdWorld* w, float* pos, float* quat, float* vel, float*
     if (fetch(W.pos, pos, 3, false) || fetch(W.rot, quat, 4, true) || fetch(W.vel, vel, 3, false) ||
         fetch(W.omega, omega, 3, false))
         return AVBD_ERR_CUDA;
+    // a removed body (RemoveBody or out of bounds) has no state: it reads NaN
+    std::vector<int> fl(n);
+    if (n > 0 && cudaMemcpy(fl.data(), W.flags, n * sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+        return AVBD_ERR_CUDA;
+    const float nan = std::numeric_limits<float>::quiet_NaN();
+    for (int i = 0; i < n; ++i) {
+        if (!(fl[i] & kBodyRemoved)) continue;
+        for (int k = 0; k < 3; ++k) {
+            if (pos) pos[3 * i + k] = nan;
+            if (vel) vel[3 * i + k] = nan;
+            if (omega) omega[3 * i + k] = nan;
+        }
+        if (quat) for (int k = 0; k < 4; ++k) quat[4 * i + k] = nan;
+    }
     return n;
+}
+
+int32_t avbd_force_live(AvbdWorld* w, int32_t force) {
+    if (!w || force < 0 || force >= w->h.nforce()) return AVBD_ERR_INVALID;
+    int t = w->h.ftype[force];
+    if (w->uploaded) {
+        cudaSetDevice(w->device);
+        if (cudaMemcpy(&t, w->P.W.ftype + force, sizeof(int), cudaMemcpyDeviceToHost) != cudaSuccess)
+            return AVBD_ERR_CUDA;
+    }
+    return (t & (kForceDisabled | kForceRemoved)) ? 0 : 1;
 }
 
 int32_t avbd_set_state(AvbdWorld* w, const float* pos, const float* quat, const float* vel, const float* omega) {
@@ -1868,8 +1855,19 @@ int32_t avbd_batch_reserve(AvbdBatch* b, int64_t bodies, int64_t forces, int64_t
     return 0;
 }
 
+// Scenes staged by avbd_batch_prepare reach the device with the first step;
+// every entry point that reads device state or hands out pool space first
+// completes that copy, so it never acts on unwritten memory and a later copy
+// never overwrites a range given to another scene.
+static int batch_settle(AvbdBatch* b) {
+    if (!b->upload_pending) return 0;
+    if (cudaSetDevice(b->device) != cudaSuccess) return AVBD_ERR_CUDA;
+    return batch_flush(b);
+}
+
 int32_t avbd_batch_add_scene(AvbdBatch* b, const AvbdWorld* w) {
     if (!b || !w) return AVBD_ERR_INVALID;
+    if (int r = batch_settle(b)) return r;
     int slot = -1;
     for (size_t i = 0; i < b->state.size(); ++i)
         if (b->state[i] == 0) { slot = (int)i; break; }
@@ -1902,6 +1900,7 @@ int32_t avbd_batch_add_scene(AvbdBatch* b, const AvbdWorld* w) {
 
 int32_t avbd_batch_remove_scene(AvbdBatch* b, int32_t scene) {
     if (!b || scene < 0 || scene >= (int)b->state.size() || b->state[scene] == 0) return AVBD_ERR_INVALID;
+    if (int r = batch_settle(b)) return r;
     if (b->state[scene] == 1) {
         b->A.release(b->regions[scene]);
         b->order_dirty = true;
@@ -1916,7 +1915,7 @@ int32_t avbd_batch_remove_scene(AvbdBatch* b, int32_t scene) {
 int32_t avbd_batch_prepare(AvbdBatch* b) {
     if (!b) return AVBD_ERR_INVALID;
     if (b->reserved) return 0;
-    int r = batch_stage(b);
+    int r = batch_stage(b, true);
     if (r) return r;
     cudaSetDevice(b->device);
     if (!b->grid) batch_launch_shape(b);
@@ -1926,7 +1925,7 @@ int32_t avbd_batch_prepare(AvbdBatch* b) {
 int32_t avbd_batch_step(AvbdBatch* b, int32_t steps) {
     if (!b || steps < 0) return AVBD_ERR_INVALID;
     int r;
-    if (!b->reserved && (r = batch_stage(b))) return r;
+    if (!b->reserved && (r = batch_stage(b, false))) return r;
     cudaSetDevice(b->device);
     if ((r = batch_flush(b))) return r;
     batch_sync_order(b);
@@ -1961,6 +1960,7 @@ static bool live_slot(const AvbdBatch* b, int scene) {
 int32_t avbd_batch_scene_status(AvbdBatch* b, int32_t scene) {
     if (!b || scene < 0 || scene >= (int)b->state.size() || b->state[scene] == 0) return AVBD_ERR_INVALID;
     if (b->state[scene] == 2) return AVBD_STATUS_OK;
+    if (int r = batch_settle(b)) return r;
     cudaSetDevice(b->device);
     SceneState st;
     if (cudaMemcpy(&st, b->P.d_sstate + scene, sizeof(SceneState), cudaMemcpyDeviceToHost) != cudaSuccess)
@@ -1971,6 +1971,7 @@ int32_t avbd_batch_scene_status(AvbdBatch* b, int32_t scene) {
 int32_t avbd_batch_scene_info(AvbdBatch* b, int32_t scene, int32_t out[6]) {
     if (!b || !out || scene < 0 || scene >= (int)b->state.size() || b->state[scene] == 0) return AVBD_ERR_INVALID;
     if (b->state[scene] == 2) { for (int i = 0; i < 6; ++i) out[i] = 0; return 0; }
+    if (int r = batch_settle(b)) return r;
     cudaSetDevice(b->device);
     SceneState st;
     if (cudaMemcpy(&st, b->P.d_sstate + scene, sizeof(SceneState), cudaMemcpyDeviceToHost) != cudaSuccess)
@@ -1995,6 +1996,7 @@ int64_t avbd_batch_dynamic_bodies(const AvbdBatch* b) {
 
 int32_t avbd_batch_get_state(AvbdBatch* b, int32_t scene, float* pos, float* quat, float* vel, float* omega) {
     if (!live_slot(b, scene)) return AVBD_ERR_INVALID;
+    if (int r = batch_settle(b)) return r;
     const int n = b->bodies[scene];
     cudaSetDevice(b->device);
     const int b0 = b->descs[scene].body0;
@@ -2018,6 +2020,7 @@ int32_t avbd_batch_get_state(AvbdBatch* b, int32_t scene, float* pos, float* qua
 
 int32_t avbd_batch_get_all_poses(AvbdBatch* b, float* pos, float* quat, int64_t max_bodies) {
     if (!b || !b->reserved) return AVBD_ERR_STATE;
+    if (int r = batch_settle(b)) return r;
     cudaSetDevice(b->device);
     const int n = b->P.nb;
     if (n > max_bodies) return AVBD_ERR_INVALID;
@@ -2150,9 +2153,35 @@ struct NoAllocScratch {
 // Shared by every call on a device; it keeps the last call's contents.
 static __device__ __align__(256) NoAllocScratch g_noalloc_scratch;
 
-// Device address of g_noalloc_scratch per device, looked up once per device.
+// Device address of g_noalloc_scratch per device, looked up on the first
+// call on that device; the lookup is serialised so concurrent first calls
+// from several host threads do not race on the cache.
 constexpr int kNoAllocMaxDevices = 64;
-NoAllocScratch* g_noalloc_ptr[kNoAllocMaxDevices] = {};
+std::atomic<NoAllocScratch*> g_noalloc_ptr[kNoAllocMaxDevices] = {};
+std::mutex g_noalloc_lookup;
+
+NoAllocScratch* noalloc_scratch(int device) {
+    NoAllocScratch* s = g_noalloc_ptr[device].load(std::memory_order_acquire);
+    if (s) return s;
+    std::lock_guard<std::mutex> lock(g_noalloc_lookup);
+    s = g_noalloc_ptr[device].load(std::memory_order_relaxed);
+    if (!s) {
+        // with `device` current: the host name g_noalloc_scratch is only a
+        // stand-in, the kernel needs the address on that device
+        void* p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return nullptr;
+        s = static_cast<NoAllocScratch*>(p);
+        g_noalloc_ptr[device].store(s, std::memory_order_release);
+    }
+    return s;
+}
+
+// Puts back the caller's current device when the call returns.
+struct DeviceGuard {
+    int prev = -1;
+    DeviceGuard() { if (cudaGetDevice(&prev) != cudaSuccess) prev = -1; }
+    ~DeviceGuard() { if (prev >= 0) cudaSetDevice(prev); }
+};
 
 __global__ void k_collide_pairs_noalloc(const __grid_constant__ World W, NoAllocScratch* s, int n, int nbody) {
     for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
@@ -2197,16 +2226,11 @@ extern "C" int32_t avbd_collide_noalloc(AvbdWorld* w, int32_t n, const int32_t* 
     }
     if (!w->uploaded) return AVBD_ERR_STATE;   // the world must already live on the device
     if (w->device < 0 || w->device >= kNoAllocMaxDevices) return AVBD_ERR_INVALID;
+    DeviceGuard keep_device;
     if (cudaSetDevice(w->device) != cudaSuccess) return AVBD_ERR_CUDA;
-    if (!g_noalloc_ptr[w->device]) {
-        // one-time set-up on this device (with the device current): the host
-        // name g_noalloc_scratch is only a stand-in, the kernel needs this address
-        void* p = nullptr;
-        if (cudaGetSymbolAddress(&p, g_noalloc_scratch) != cudaSuccess || !p) return AVBD_ERR_CUDA;
-        g_noalloc_ptr[w->device] = static_cast<NoAllocScratch*>(p);
-    }
+    NoAllocScratch* s = noalloc_scratch(w->device);
+    if (!s) return AVBD_ERR_CUDA;
     if (n == 0) return 0;
-    NoAllocScratch* s = g_noalloc_ptr[w->device];
     cudaStream_t st = w->stream;
     if (cudaMemcpyAsync(s->body_a, body_a, n * sizeof(int32_t), cudaMemcpyHostToDevice, st) != cudaSuccess ||
         cudaMemcpyAsync(s->body_b, body_b, n * sizeof(int32_t), cudaMemcpyHostToDevice, st) != cudaSuccess)
@@ -2222,18 +2246,3 @@ extern "C" int32_t avbd_collide_noalloc(AvbdWorld* w, int32_t n, const int32_t* 
         if (counts[i] < 0) return AVBD_ERR_INVALID;
     return 0;
 }
-
-#ifdef AVBD_PHASE_TIMING
-// Development builds only: read and reset the per-phase cycle counters.
-extern "C" int32_t avbd_debug_phase_cycles(unsigned long long* phases, unsigned long long* scenes, int32_t nscenes,
-                                           int32_t reset) {
-    if (phases) cudaMemcpyFromSymbol(phases, g_phase_cycles, sizeof(unsigned long long) * 32);
-    if (scenes && nscenes > 0)
-        cudaMemcpyFromSymbol(scenes, g_scene_cycles, sizeof(unsigned long long) * std::min(nscenes, 1 << 16));
-    if (reset) {
-        static unsigned long long zeros[32] = {};
-        cudaMemcpyToSymbol(g_phase_cycles, zeros, sizeof(zeros));
-    }
-    return 0;
-}
-#endif

@@ -861,9 +861,16 @@ AVBD_HD void primal_apply(const World& W, int b, const float (&x)[6]) {
     W.dang[b] = f4(rotation_difference(nrot, q4(W.lrot[b])));
 }
 
+// A particle has no rotational inertia (solver.cpp:119-131): whenever force
+// rows reach its rotational block, that block holds contact torques alone and
+// is close to singular, so the solve follows the reference's factorisation
+// step for step (symmetric pivoting on the largest diagonal, the pivot rule
+// of the Eigen LDLT it calls at solver.cpp:437-438) instead of the unpivoted
+// shortcut, whose different elimination order rounds differently.
 AVBD_HD void primal_finish(const World& W, int b, Sys6& s) {
     float x[6];
-    ldlt_solve6(s, x);
+    if ((W.flags[b] & kBodyParticle) && !sys_rotation_free(s)) ldlt_solve<6, 6>(s.a, s.r, x);
+    else ldlt_solve6(s, x);
     primal_apply(W, b, x);
 }
 

@@ -6,27 +6,6 @@
 #pragma once
 #include "avbd_phases.cuh"
 
-// Optional per-phase cycle counters (development builds with -DAVBD_PHASE_TIMING
-// only; the hooks compile to nothing otherwise).
-#ifdef AVBD_PHASE_TIMING
-__device__ unsigned long long g_phase_cycles[2 * 16];
-__device__ unsigned long long g_scene_cycles[1 << 16];
-#define AVBD_PHASE_BEGIN(kind) long long _avbd_t0 = clock64(), _avbd_s0 = _avbd_t0; const int _avbd_kind = (kind);
-// (team time is counted in 256-thread CTA equivalents: cycles x team size / 256)
-#define AVBD_PHASE(k)                                                                               \
-    if (T.rank == 0) {                                                                              \
-        long long _t = clock64();                                                                   \
-        atomicAdd(&g_phase_cycles[_avbd_kind * 16 + (k)], (unsigned long long)((_t - _avbd_t0) * T.size / 256)); \
-        _avbd_t0 = _t;                                                                              \
-    }
-#define AVBD_PHASE_END(scene) \
-    if (T.rank == 0 && (scene) < (1 << 16)) g_scene_cycles[(scene)] = (unsigned long long)((clock64() - _avbd_s0) * T.size / 256);
-#else
-#define AVBD_PHASE_BEGIN(kind)
-#define AVBD_PHASE(k)
-#define AVBD_PHASE_END(scene)
-#endif
-
 namespace avbd {
 
 constexpr unsigned kFull = 0xffffffffu;
@@ -93,7 +72,7 @@ struct Team {
 
 // Exclusive scan of in[0, n) into out[0, n) by one team; returns the total.
 // in and out may alias.
-__device__ int block_exclusive_scan(const Team& T, const int* in, int* out, int n) {
+static __device__ int block_exclusive_scan(const Team& T, const int* in, int* out, int n) {
     const int lane = T.rank & 31, warp = T.rank >> 5, nwarps = T.size >> 5;
     if (T.rank == 0) T.sh->carry = 0;
     T.sync();
@@ -134,7 +113,7 @@ __device__ int block_exclusive_scan(const Team& T, const int* in, int* out, int 
 //   [static forces][manifolds as body B, by slot][manifolds as body A][energies]
 // which follows Mesh::forces then Mesh::energies (solver.cpp:395-435).
 // ---------------------------------------------------------------------------
-__device__ int owned_live(const World& W, int cur, int b, int base_slot) {
+static __device__ int owned_live(const World& W, int cur, int b, int base_slot) {
     const int c0 = W.cand_off[b] + base_slot, c1 = c0 + W.cand_cnt[b];
     int n = 0;
     for (int c = c0; c < c1; ++c) n += W.cn[cur][c] > 0 ? 1 : 0;
@@ -159,7 +138,7 @@ __device__ __forceinline__ void sort_manifold_entries(const World& W, int cur, u
 }
 
 // Returns false (and sets need_inc) when the scene's incidence region is too small.
-__device__ __noinline__ bool build_incidence(const Team& T, const World& W, const SceneDesc& sc, SceneState* st,
+static __device__ __noinline__ bool build_incidence(const Team& T, const World& W, const SceneDesc& sc, SceneState* st,
                                              int cur) {
     const int tid = T.rank, nt = T.size;
     const int b0 = sc.body0, b1 = sc.body0 + sc.nbody;
@@ -284,7 +263,7 @@ __device__ __forceinline__ void primal_group(const World& W, int cur, int b, flo
 
 // Sweeps the bodies list[0, n) with groups of G lanes of the calling team.
 template <int G>
-__device__ void primal_sweep_cta(const Team& T, const World& W, int cur, const int* list, int n, float alpha,
+static __device__ void primal_sweep_cta(const Team& T, const World& W, int cur, const int* list, int n, float alpha,
                                  bool write_stick) {
     const int lane = T.rank % G, gid = T.rank / G, ngroups = T.size / G;
     for (int base = 0; base < n; base += ngroups) {
@@ -295,7 +274,7 @@ __device__ void primal_sweep_cta(const Team& T, const World& W, int cur, const i
     }
 }
 
-__device__ __noinline__ void primal_sweep_cta_dispatch(const Team& T, const World& W, int cur, const int* list, int n,
+static __device__ __noinline__ void primal_sweep_cta_dispatch(const Team& T, const World& W, int cur, const int* list, int n,
                                                           float alpha, bool write_stick, int group) {
     switch (group) {
         case 32: primal_sweep_cta<32>(T, W, cur, list, n, alpha, write_stick); break;
@@ -326,7 +305,7 @@ __device__ __forceinline__ int tet_terms(const World& W, int b) { return W.sinc_
 // Any body of a flat-swept colour: inertia, force and manifold rows, then its
 // tet terms from slot q0 on (q0 < 0: terms evaluated here, the slots did not
 // hold them).  Out of line: the 6x6 system stays out of the sweep's registers.
-__device__ __noinline__ void flat_finish_body(const World& W, int cur, int b, int e0, int e1, int q0, float alpha,
+static __device__ __noinline__ void flat_finish_body(const World& W, int cur, int b, int e0, int e1, int q0, float alpha,
                                               bool write_stick, const float* sm, int nslots) {
     Sys6 s;
     sys_zero(s);
@@ -362,7 +341,7 @@ __device__ __forceinline__ float sys3_component(const Sys3& s, int k) {
 // rigid body, is finished by its first lane alone.  The loop bound is
 // uniform over each warp, so the shuffles run with the whole warp.
 template <int L>
-__device__ __noinline__ void flat_finish_split(const Team& T, const World& W, int cur, const int* list,
+static __device__ __noinline__ void flat_finish_split(const Team& T, const World& W, int cur, const int* list,
                                                   const int* tinc, int base, int v, int vend, float alpha,
                                                   bool write_stick, const float* sm, int nslots) {
     constexpr int G = 32 / L, C = 9 / L;
@@ -421,7 +400,7 @@ __device__ __noinline__ void flat_finish_split(const Team& T, const World& W, in
     }
 }
 
-__device__ __noinline__ void primal_sweep_flat(const Team& T, const World& W, int cur, const int* list,
+static __device__ __noinline__ void primal_sweep_flat(const Team& T, const World& W, int cur, const int* list,
                                                const int* tinc, size_t rec0, int c0, int c1, float alpha,
                                                bool write_stick) {
     float* sm = reinterpret_cast<float*>(T.stage);
@@ -488,7 +467,7 @@ __device__ __forceinline__ void primal_colour(const Team& T, const World& W, con
                                   sc.group);
 }
 
-__device__ __noinline__ bool colour_scene(const Team& T, const World& W, const SceneDesc& sc, SceneState* st,
+static __device__ __noinline__ bool colour_scene(const Team& T, const World& W, const SceneDesc& sc, SceneState* st,
                                           int scene, int cur);
 
 // Keeps the previous step's colouring when the contact graph is unchanged:
@@ -496,7 +475,7 @@ __device__ __noinline__ bool colour_scene(const Team& T, const World& W, const S
 // live last step, and no force or body removed since the colouring was made.
 // The colouring is a deterministic function of that graph, so reusing it is
 // exact.
-__device__ bool colour_scene_cached(const Team& T, const World& W, const SceneDesc& sc, SceneState* st, int scene,
+static __device__ bool colour_scene_cached(const Team& T, const World& W, const SceneDesc& sc, SceneState* st, int scene,
                                     int cur) {
     const int old = cur ^ 1;
     const bool reuse = st->colours_valid && st->nlive[cur] == st->nlive[old] && st->nmatched == st->nlive[cur] &&
@@ -545,7 +524,7 @@ __device__ __forceinline__ bool colour_before(const World& W, int pass, int u, i
 // takes the smallest colour its preceding neighbours do not use once they
 // are all coloured, which equals sequential greedy colouring in priority
 // order whatever the thread schedule.  False (status TIMEOUT) if it stalls.
-__device__ bool jp_pass(const Team& T, const World& W, const SceneDesc& sc, SceneState* st, int cur, int pass) {
+static __device__ bool jp_pass(const Team& T, const World& W, const SceneDesc& sc, SceneState* st, int cur, int pass) {
     int& s_remaining = T.sh->remaining;
     int& s_progress = T.sh->progress;
     int& s_maxc = T.sh->maxc;
@@ -599,7 +578,7 @@ __device__ bool jp_pass(const Team& T, const World& W, const SceneDesc& sc, Scen
 // Returns false (status TIMEOUT or CAPACITY set) if colouring could not finish.
 // The colour counts live in the team's stage (at least kMaxColours + 1 ints).
 // Priorities read W.cntB and W.bcur, free once the incidence is built.
-__device__ __noinline__ bool colour_scene(const Team& T, const World& W, const SceneDesc& sc, SceneState* st,
+static __device__ __noinline__ bool colour_scene(const Team& T, const World& W, const SceneDesc& sc, SceneState* st,
                                           int scene, int cur) {
     int& s_maxc = T.sh->maxc;
     int* s_count = reinterpret_cast<int*>(T.stage);
@@ -677,7 +656,7 @@ __device__ __noinline__ bool colour_scene(const Team& T, const World& W, const S
 
 // Phase loops of one scene kept out of line, so each gets its own register
 // allocation instead of the union of every inlined phase.
-__device__ __noinline__ void narrowphase_cta(const Team& T, const World& W, const SceneDesc& sc, SceneState* st,
+static __device__ __noinline__ void narrowphase_cta(const Team& T, const World& W, const SceneDesc& sc, SceneState* st,
                                              int cur, int ncand, int old_count) {
     for (int c = sc.cand0 + T.rank; c < sc.cand0 + ncand; c += T.size)
         narrowphase_slot(W, sc, st, c, cur, old_count);
@@ -685,7 +664,7 @@ __device__ __noinline__ void narrowphase_cta(const Team& T, const World& W, cons
 
 // Returns true if this thread saw a force fracture.  Manifolds come from the
 // step's live list (each manifold's dual is independent of the others).
-__device__ __noinline__ bool dual_cta(const Team& T, const World& W, const SceneDesc& sc, int cur, int nlive,
+static __device__ __noinline__ bool dual_cta(const Team& T, const World& W, const SceneDesc& sc, int cur, int nlive,
                                       bool last) {
     bool broke = false;
     for (int f = sc.force0 + T.rank; f < sc.force0 + sc.nforce; f += T.size)
@@ -790,7 +769,7 @@ __device__ __forceinline__ int grid_candidates(const World& W, const SceneDesc& 
     return n;
 }
 
-__device__ __noinline__ int broadphase_grid(const Team& T, const World& W, const SceneDesc& sc, int cur,
+static __device__ __noinline__ int broadphase_grid(const Team& T, const World& W, const SceneDesc& sc, int cur,
                                             const float4* sp) {
     const int tid = T.rank, nt = T.size, n = sc.nbody, b0 = sc.body0;
     int* red = T.sh->red;
@@ -906,7 +885,7 @@ __device__ __noinline__ int broadphase_grid(const Team& T, const World& W, const
 // ---------------------------------------------------------------------------
 // Whole step of one scene by one team (batched path).
 // ---------------------------------------------------------------------------
-__device__ void scene_step(const World& W, int scene, const Team& T) {
+static __device__ void scene_step(const World& W, int scene, const Team& T) {
     const SceneDesc sc = W.scenes[scene];
     SceneState* st = W.sstate + scene;
     const int tid = T.rank, nt = T.size;
@@ -914,7 +893,6 @@ __device__ void scene_step(const World& W, int scene, const Team& T) {
     if (st->status != kStatusOk && st->status != kStatusCapacity && st->status != kStatusTimeout) return;
     T.sync();
     if (tid == 0) { st->status = kStatusOk; st->need_cand = 0; st->need_k = 0; st->need_inc = 0; }
-    AVBD_PHASE_BEGIN(sc.ntet > 0 ? 1 : 0);
     const int old = st->cur, cur = old ^ 1;
     const int b0 = sc.body0, b1 = sc.body0 + sc.nbody;
     // 1. broadphase: count, scan, capacity check, write; positions and radii
@@ -955,7 +933,6 @@ __device__ void scene_step(const World& W, int scene, const Team& T) {
     }
     if (tid == 0) { st->kused[cur] = 0; st->nlive[cur] = 0; st->nmatched = 0; }
     T.sync();
-    AVBD_PHASE(0);
     // 2. narrowphase + manifold warm start into the other table
     const int old_count = st->ncand[old];
     narrowphase_cta(T, W, sc, st, cur, ncand, old_count);
@@ -969,7 +946,6 @@ __device__ void scene_step(const World& W, int scene, const Team& T) {
         return;
     }
     if (tid == 0) { st->ncand[cur] = ncand; st->cur = cur; }
-    AVBD_PHASE(1);
     // 2b. joints / springs warm start
     for (int f = sc.force0 + tid; f < sc.force0 + sc.nforce; f += nt)
         if (force_init(W, f)) atomicAdd(&st->topo, 1);
@@ -982,14 +958,11 @@ __device__ void scene_step(const World& W, int scene, const Team& T) {
         }
         return;
     }
-    AVBD_PHASE(2);
     // colouring
     if (!colour_scene_cached(T, W, sc, st, scene, cur)) return;
-    AVBD_PHASE(3);
     // 4. prediction
     for (int b = b0 + tid; b < b1; b += nt) predict_body(W, b);
     T.sync();
-    AVBD_PHASE(4);
     const int ncol = st->ncolours;
     const int nlive = st->nlive[cur];
     const int* cs = W.col_start + (size_t)scene * (kMaxColours + 1);
@@ -999,7 +972,6 @@ __device__ void scene_step(const World& W, int scene, const Team& T) {
             primal_colour(T, W, sc, cur, cs, c, W.P.alpha, false);
             T.sync();
         }
-        AVBD_PHASE(5);
         if (tid == 0) s_flags = 0;
         T.sync();
         if (dual_cta(T, W, sc, cur, nlive, it == W.P.num_iterations - 1)) s_flags = 1;
@@ -1012,7 +984,6 @@ __device__ void scene_step(const World& W, int scene, const Team& T) {
             for (int b = b0 + tid; b < b1; b += nt) W.reset_flag[b] = 0;
             T.sync();
         }
-        AVBD_PHASE(6);
     }
     // 6. velocities, explosion, out of bounds
     if (tid == 0) s_flags = 0;
@@ -1048,7 +1019,6 @@ __device__ void scene_step(const World& W, int scene, const Team& T) {
         T.sync();
     }
     if (tid == 0) st->step += 1;
-    AVBD_PHASE(7);
     // 7. post-stabilisation
     if (W.P.post_stabilization) {
         for (int c = 0; c < ncol; ++c) {
@@ -1056,8 +1026,6 @@ __device__ void scene_step(const World& W, int scene, const Team& T) {
             T.sync();
         }
     }
-    AVBD_PHASE(8);
-    AVBD_PHASE_END(scene);
 }
 
 }  // namespace avbd

@@ -33,6 +33,8 @@ class Request:
     dynamic: int = 0         # dynamic bodies (body-iterations per step / iterations)
     status: str = ""
     result: tuple = field(default=None, repr=False)   # (pos, quat) after the last step
+    sample: bool = False     # also keep the state after the request's first step (tolerance checks)
+    first: tuple = field(default=None, repr=False)    # (pos, quat) after the first step, for samples
 
 
 # Pool bytes per body of a typical scene (bodies, candidate pairs, contacts,
@@ -96,13 +98,15 @@ class Server:
         finished = []
         for slot, req in self.active.items():
             req.remaining -= 1
+            if req.sample and req.first is None:
+                req.first = tuple(a.copy() for a in self.batch.get_state(slot)[:2])
             if req.remaining <= 0:
                 finished.append(slot)
         for slot in finished:
             req = self.active.pop(slot)
             self.resident_dynamic -= req.dynamic
             req.status = self.batch.scene_status(slot)
-            if self.keep_results:
+            if self.keep_results or req.sample:
                 pos, quat = self.batch.get_state(slot)[:2]
                 req.result = (pos, quat)
             self.batch.remove_scene(slot)

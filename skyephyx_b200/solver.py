@@ -189,6 +189,10 @@ class Solver:
     def emergency_stop(self):
         return bool(self._lib.avbd_emergency_stop(self._h))
 
+    def force_live(self, force: int) -> bool:
+        """False once a fracture disabled the joint/spring or it left with a body."""
+        return bool(check(self._lib.avbd_force_live(self._h, int(force)), "force_live"))
+
     def get_state(self):
         n = self.num_bodies
         pos = np.zeros((n, 3), np.float32)

@@ -74,7 +74,8 @@ def run(name, build, coloured, steps=STEPS):
 
 def main():
     ap = argparse.ArgumentParser()
-    ap.add_argument("--ref", default="/root/reference")
+    ap.add_argument("--ref", default=None, help="SkyePhyX source tree (default: $SKYEPHYX_REF or the oracle "
+                                                 "Makefile's default)")
     args = ap.parse_args()
     from oracle import oracle
     oracle.build(args.ref)

@@ -8,6 +8,7 @@ import numpy as np
 import pytest
 
 from skyephyx_b200 import scenes
+from conftest import rot_err
 
 pytestmark = pytest.mark.gpu
 
@@ -260,3 +261,83 @@ def test_prepare_then_step_equals_step():
         runs.append([b.get_state(i)[:2] for i in range(len(builders))])
     for a, c in zip(*runs):
         assert same(a, c)
+
+
+def test_prepare_then_remove_and_add_admits_the_new_scene():
+    """Scenes staged by prepare() reach the device before a remove/add pair
+    reuses their space: the newly admitted scene steps as it does alone."""
+    from skyephyx_b200 import Batch
+    builders = mix_builders()
+    b = Batch()
+    keep = [staged(f) for f in builders]
+    for w in keep:
+        b.add_scene(w)
+    b.prepare()
+    b.remove_scene(2)
+    newcomer = lambda s: scenes.rigid_pile(s, 30, scenes.rng_for(4, 77), stack=True)
+    slot = b.add_scene(staged(newcomer))
+    assert b.scene_status(slot) == "ok"
+    assert b.step(3) == "ok"
+    ref = Batch()
+    ref.add_scene(staged(newcomer))
+    assert ref.step(3) == "ok"
+    assert same(b.get_state(slot)[:2], ref.get_state(0)[:2])
+    # the other scenes are the ones staged before the swap
+    alone = Batch()
+    alone.add_scene(staged(builders[0]))
+    assert alone.step(3) == "ok"
+    assert same(b.get_state(0)[:2], alone.get_state(0)[:2])
+
+
+def headline_slice(n_sample=256):
+    """A slice of the 4,096-scene batched mix: every 16th scene plus the eight
+    largest rigid and the eight largest FEM scenes."""
+    specs = scenes.batch_mix_specs()
+    rigid = sorted((i for i, sp in enumerate(specs) if sp[0] != "fem"), key=lambda i: -specs[i][1])[:8]
+    fem = sorted((i for i, sp in enumerate(specs) if sp[0] == "fem"), key=lambda i: -specs[i][1])[:8]
+    picks = sorted(set(range(0, len(specs), len(specs) // n_sample)) | set(rigid) | set(fem))
+    return [specs[i] for i in picks]
+
+
+def test_headline_launch_matches_oracle(oracle_mod):
+    """The launch the benchmark runs the 4,096-scene mix with (the autotuned
+    kernel build, lanes per body, flat FEM sweep, team split and grid
+    threshold for this mix) on a 270-scene slice that holds the mix's largest
+    scenes: after one step every scene's positions and rotations are within
+    1e-4 of the colour-ordered oracle, and its contact-point and colour
+    counts are equal."""
+    import os
+    from skyephyx_b200 import Batch, autotune
+    specs = headline_slice()
+    full = scenes.batch_mix_specs()
+    nfem = sum(1 for sp in full if sp[0] == "fem")
+    # the signature of the full mix (4,096 scenes, 25% FEM, ~512 bodies each)
+    cfg = autotune.lookup(autotune.signature(len(full), nfem, 512 * len(full)))
+    b = Batch()
+    keep = []
+    for sp in specs:
+        w = staged(lambda s: scenes.build_spec(s, sp))
+        keep.append(w)
+        b.add_scene(w)
+    autotune.apply(b, cfg)
+    assert b.step(1) == "ok"
+    orcs = []
+    for sp in specs:
+        o = oracle_mod.OracleSolver()
+        scenes.build_spec(o, sp)
+        orcs.append(o)
+    oracle_mod.step_many(orcs, 1, os.cpu_count() or 8, coloured=True)
+    worst_p = worst_r = 0.0
+    for i, (sp, o) in enumerate(zip(specs, orcs)):
+        info = b.scene_info(i)
+        assert info["status"] == 0, f"{sp}: {info}"
+        pb, qb = b.get_state(i)[:2]
+        po, qo = o.get_state()[:2]
+        dp = float(np.abs(pb - po).max(initial=0.0))
+        dr = float(rot_err(qb, qo).max(initial=0.0))
+        worst_p, worst_r = max(worst_p, dp), max(worst_r, dr)
+        assert dp <= 1e-4 and dr <= 1e-4, f"{sp}: |dpos| {dp:.3g} m, |drot| {dr:.3g} rad"
+        points = sum(len(v[0]) for v in o.contacts().values())
+        assert info["contacts"] == points, f"{sp}: {info['contacts']} contact points vs {points}"
+        assert info["colours"] == o.colours()[1], f"{sp}: colours"
+    print(f"headline slice: {len(specs)} scenes, max |dpos| {worst_p:.3g} m, max |drot| {worst_r:.3g} rad")

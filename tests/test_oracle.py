@@ -139,3 +139,55 @@ def test_stvk_tet_oracle_is_sane(oracle_mod):
     for _ in range(60):
         big.step_coloured()
     assert np.isfinite(big.get_state()[0]).all()
+
+
+FP64_SCENES = ["pyramid", "joint_playground", "soft_beam", "cloth", "mixed_300"]
+
+
+@pytest.mark.parametrize("name", FP64_SCENES)
+def test_fp64_oracle_agrees_with_fp32(oracle_mod, name):
+    """The FP64 build (the reference's code carried out in double) is the
+    FP32 oracle up to rounding: after one colour-ordered step the poses agree
+    to 2e-6 and the contact manifolds and colours are the same."""
+    import sys
+    sys.path.insert(0, os.path.join(HERE, "golden"))
+    from make_golden import golden_scenes
+    build = golden_scenes()[name]
+    a = oracle_mod.OracleSolver()
+    b = oracle_mod.OracleSolver(f64=True)
+    build(a)
+    build(b)
+    assert a.step_coloured() == 0 and b.step_coloured() == 0
+    pa, qa = a.get_state()[:2]
+    pb, qb = b.get_state()[:2]
+    assert pb.dtype == np.float64
+    assert np.abs(pa - pb).max() <= 2e-6
+    assert np.abs(qa - qb).max() <= 2e-6
+    assert {k: v[0] for k, v in a.contacts().items()} == {k: v[0] for k, v in b.contacts().items()}
+    assert a.colours()[1] == b.colours()[1]
+
+
+def test_metrics_measure_the_state(oracle_mod):
+    """orc_metrics: a resting pyramid has only gravitational energy (m g y)
+    and no violation; lifting one box by 1 m adds m g; a joint pulled apart
+    reports its positional violation."""
+    from skyephyx_b200 import scenes
+    o = oracle_mod.OracleSolver()
+    scenes.pyramid_wall(o, rows=3)
+    m = o.metrics()
+    masses = 1000.0  # unit cubes of density 1000
+    ys = o.get_state()[0][1:, 1]
+    assert m["max_violation"] == 0.0 and m["kinetic_j"] == 0.0 and m["elastic_j"] == 0.0
+    assert abs(m["potential_j"] - masses * 9.81 * float(np.sum(ys))) < 1e-3 * m["potential_j"]
+    p = o.get_state()[0].copy()
+    p[1, 1] += 1.0
+    o.set_state(pos=p)
+    assert abs(o.metrics()["potential_j"] - m["potential_j"] - masses * 9.81) < 1e-2
+    j = oracle_mod.OracleSolver()
+    b = j.add_body(scenes.CUBE, 1000.0, 0.5, (0.0, 5.0, 0.0), (1, 1, 1))
+    j.add_joint(-1, (0.0, 5.5, 0.0), b, (0.0, 0.5, 0.0))
+    assert j.metrics()["max_violation"] < 1e-6
+    p = j.get_state()[0].copy()
+    p[b, 1] -= 0.25
+    j.set_state(pos=p)
+    assert abs(j.metrics()["max_violation"] - 0.25) < 1e-5
