@@ -304,6 +304,66 @@ int32_t avbd_set_group(AvbdWorld* w, int32_t group);
 /* Device time of the last avbd_batch_step call in ms. */
 float avbd_batch_last_ms(const AvbdBatch* b);
 
+/* ---------------------------------------------------------------------------
+ * Serving: continuous batching of scene-simulation requests (no reference
+ * counterpart).  Each request is a staged scene and a step count.  A tick
+ * admits the requests that have arrived, in arrival order, as long as their
+ * scene fits the free pool space (HBM-budget admission; one that does not
+ * fit waits for space), advances every resident scene one step with one
+ * graph launch, and retires the scenes that took their last step, so their
+ * space goes to the next admissions.  avbd_server_tick returns while the
+ * step runs on the GPU: the next tick stages its newcomers meanwhile and then
+ * waits for it.  Not thread-safe per server.
+ * ------------------------------------------------------------------------- */
+typedef struct AvbdServer AvbdServer;
+
+#define AVBD_SERVE_KEEP_RESULT 1   /* keep the poses after the last step (avbd_server_result) */
+#define AVBD_SERVE_KEEP_FIRST  2   /* keep the poses after the first step too (tolerance checks) */
+
+typedef struct AvbdServedRequest {
+    int32_t request;     /* id returned by avbd_server_submit */
+    int32_t status;      /* AVBD_STATUS_* of the scene after its last step */
+    int32_t steps;
+    int32_t bodies;
+    double arrival_s;    /* the times the caller passed: arrival, and the ticks that */
+    double admitted_s;   /* admitted it and that found its last step complete */
+    double finished_s;
+} AvbdServedRequest;
+
+typedef struct AvbdServerStats {
+    int64_t submitted, admitted, completed, ticks;
+    int64_t body_iterations;   /* dynamic bodies x iterations over the steps launched */
+    int64_t uploaded_bytes;    /* host-to-device bytes of admitted scenes */
+    int64_t pending, active, resident_dynamic;
+} AvbdServerStats;
+
+/* Pools for `bodies` bodies (a quarter as many joints+springs and
+ * triangles, two tets per body) and `max_scenes` resident scenes. */
+int32_t avbd_server_create(const AvbdParams* params, int32_t device, int64_t bodies, int32_t max_scenes,
+                           AvbdServer** out);
+int32_t avbd_server_destroy(AvbdServer* s);
+/* The server's batch, for the launch knobs (avbd_batch_set_*) before the first tick. */
+AvbdBatch* avbd_server_batch(AvbdServer* s);
+/* Copies the scene staged in `scene` (built, never stepped) as a request of
+ * `steps` steps arriving at `arrival_s` (the caller's clock, as passed to
+ * avbd_server_tick); flags: AVBD_SERVE_KEEP_*.  Returns the request id. */
+int32_t avbd_server_submit(AvbdServer* s, const AvbdWorld* scene, int32_t steps, double arrival_s, int32_t flags);
+/* One tick at the caller's time now_s; returns the scenes the launched step
+ * advances (0 when nothing is resident). */
+int32_t avbd_server_tick(AvbdServer* s, double now_s);
+/* Waits for the step in flight and retires the scenes it finished. */
+int32_t avbd_server_drain(AvbdServer* s, double now_s);
+/* Takes the next finished request: 1 when one was written to out, 0 when none. */
+int32_t avbd_server_poll(AvbdServer* s, AvbdServedRequest* out);
+/* Kept poses of a finished request into host buffers (pos n*3, quat n*4
+ * w x y z; any may be NULL).  Returns the body count, AVBD_ERR_STATE when
+ * the request is not finished or a requested result was not kept. */
+int32_t avbd_server_result(AvbdServer* s, int32_t request, float* pos, float* quat_wxyz, float* first_pos,
+                           float* first_quat_wxyz);
+/* Frees the kept poses of a request. */
+int32_t avbd_server_release(AvbdServer* s, int32_t request);
+int32_t avbd_server_stats(const AvbdServer* s, AvbdServerStats* out);
+
 #ifdef __cplusplus
 }
 #endif

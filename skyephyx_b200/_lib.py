@@ -33,6 +33,17 @@ class AvbdParams(C.Structure):
     ]
 
 
+class AvbdServedRequest(C.Structure):
+    """AvbdServedRequest (include/avbd.h): one finished served request."""
+    _fields_ = [("request", C.c_int32), ("status", C.c_int32), ("steps", C.c_int32), ("bodies", C.c_int32),
+                ("arrival_s", C.c_double), ("admitted_s", C.c_double), ("finished_s", C.c_double)]
+
+
+class AvbdServerStats(C.Structure):
+    _fields_ = [(n, C.c_int64) for n in ("submitted", "admitted", "completed", "ticks", "body_iterations",
+                                         "uploaded_bytes", "pending", "active", "resident_dynamic")]
+
+
 class AvbdTimings(C.Structure):
     _fields_ = [(n, C.c_float) for n in ("broad_phase_ms", "warmstart_ms", "colouring_ms", "prediction_ms",
                                          "primal_dual_ms", "velocity_update_ms", "post_stab_ms",
@@ -113,6 +124,16 @@ SIGNATURES = [
     ("avbd_batch_last_ms", [_V], C.c_float),
     ("avbd_batch_set_groups", [_V, C.c_int32, C.c_int32], C.c_int32),
     ("avbd_set_group", [_V, C.c_int32], C.c_int32),
+    ("avbd_server_create", [C.POINTER(AvbdParams), C.c_int32, C.c_int64, C.c_int32, C.POINTER(_V)], C.c_int32),
+    ("avbd_server_destroy", [_V], C.c_int32),
+    ("avbd_server_batch", [_V], _V),
+    ("avbd_server_submit", [_V, _V, C.c_int32, C.c_double, C.c_int32], C.c_int32),
+    ("avbd_server_tick", [_V, C.c_double], C.c_int32),
+    ("avbd_server_drain", [_V, C.c_double], C.c_int32),
+    ("avbd_server_poll", [_V, C.POINTER(AvbdServedRequest)], C.c_int32),
+    ("avbd_server_result", [_V, C.c_int32, _F, _F, _F, _F], C.c_int32),
+    ("avbd_server_release", [_V, C.c_int32], C.c_int32),
+    ("avbd_server_stats", [_V, C.POINTER(AvbdServerStats)], C.c_int32),
 ]
 
 

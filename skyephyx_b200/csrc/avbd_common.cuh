@@ -52,6 +52,8 @@ constexpr int kMaxContacts = 8;       // Manifold::contactPoints[8] (force.hpp:1
 constexpr int kMaxColours = 1024;     // colour slots per scene
 constexpr int kColourWorkBuckets = 16; // work classes used to order bodies within a colour
 constexpr int kGroupFlat = 64;         // SceneDesc::group of scenes swept term-per-lane (AVBD_GROUP_FLAT)
+constexpr int kStagedBodies = 2560;    // batched kernel: shared-memory stage of a 256-thread CTA in float4 (40 KB);
+                                       // smaller CTAs get proportionally less
 
 // tet energy models
 constexpr int kTetNeoHookean = 0;      // NeoHookeanFEM (neohookeanfem.cpp)

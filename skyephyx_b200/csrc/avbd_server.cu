@@ -1,0 +1,414 @@
+// Continuous-batching server of scene-simulation requests (avbd_server_* in
+// include/avbd.h).  No counterpart in the reference, whose caller steps one
+// Solver per frame (GameManager.cpp:68-83).
+//
+// Every admitted scene stays resident in one AvbdBatch and all resident
+// scenes advance one step per tick through the batch's CUDA graph (one
+// persistent-kernel launch).  A tick is pipelined with the step in flight:
+//
+//   1. newcomers whose arrival time has passed are placed in the pools (first
+//      fit, in arrival order; a scene that does not fit waits) and staged
+//      into a page-locked arena, while the previous step still runs;
+//   2. the host waits for that step, which also brought back the poses of
+//      the scenes it finished (and of sampled scenes after their first step);
+//      those scenes retire: their results are kept, their pool space is
+//      freed for the next admissions;
+//   3. the newcomers' copies, the live-scene order and the next step are
+//      issued on the stream, followed by the readback of the scenes that step
+//      will finish; the call returns while the GPU steps.
+//
+// A scene's arithmetic does not depend on what else is resident, so a served
+// result is the one the scene gets alone (tested).
+#include <cuda_runtime.h>
+
+#include <algorithm>
+#include <deque>
+#include <new>
+#include <vector>
+
+#include "avbd_pools.h"
+
+using namespace avbd;
+using namespace avbd::host;
+
+namespace {
+
+struct ServedRequest {
+    int id = -1;
+    int slot = -1;
+    int steps = 0;          // steps asked for
+    int taken = 0;          // steps issued so far
+    int flags = 0;          // AVBD_SERVE_KEEP_*
+    int status = AVBD_STATUS_OK;
+    int nbody = 0;
+    int64_t dynamic = 0;
+    double arrival = 0.0, admitted = -1.0, finished = -1.0;
+    HostScene scene;        // the staged scene until it is admitted
+    std::vector<float4> first_pos, first_rot, pos, rot;   // kept results (x y z / x y z w)
+};
+
+// One pose readback enqueued after a step: `n` float4 of pos and of rot into
+// the readback arena at `off`, plus the scene's state word.
+struct Readback {
+    int req;
+    bool final;             // the request's last step (else its first-step sample)
+    size_t off;
+    int n;
+    int state_off;
+};
+
+}  // namespace
+
+struct AvbdServer {
+    AvbdBatch* b = nullptr;
+    std::vector<ServedRequest> reqs;    // by request id
+    std::deque<int> pending;            // request ids waiting for admission, arrival order
+    std::vector<int> slot_req;          // request id of each batch slot (-1 free)
+    std::deque<int> finished;           // request ids ready for avbd_server_poll
+    ArenaSink arena[2];                 // upload staging, alternating per tick
+    int arena_cur = 0;
+    float4* rb = nullptr;               // page-locked readback arena
+    size_t rb_cap = 0;
+    SceneState* rb_state = nullptr;     // page-locked scene states of the readbacks
+    int rb_state_cap = 0;
+    std::vector<Readback> rb_list;      // readbacks of the step in flight
+    int* order_host = nullptr;          // page-locked live-slot order
+    int order_cap = 0;
+    cudaEvent_t step_done = nullptr;
+    bool in_flight = false;
+    int64_t resident_dynamic = 0;
+    AvbdServerStats stats{};
+};
+
+namespace {
+
+int grow_pinned(void** p, size_t bytes) {
+    if (*p) cudaFreeHost(*p);
+    *p = nullptr;
+    if (cudaHostAlloc(p, bytes, cudaHostAllocDefault) != cudaSuccess) return AVBD_ERR_NOMEM;
+    return 0;
+}
+
+// Places a newcomer in the pools and stages its upload; false if it does not fit.
+bool server_admit(AvbdServer* s, int rid, double now) {
+    AvbdBatch* b = s->b;
+    ServedRequest& r = s->reqs[rid];
+    int slot = -1;
+    for (size_t i = 0; i < b->state.size(); ++i)
+        if (b->state[i] == 0 && s->slot_req[i] < 0) { slot = (int)i; break; }
+    if (slot < 0) {
+        if ((int)b->state.size() >= b->P.ns) return false;
+        slot = (int)b->state.size();
+        b->scenes.emplace_back();
+        b->state.push_back(0);
+        b->regions.emplace_back();
+        b->descs.emplace_back();
+        b->bodies.push_back(0);
+        b->dynamic.push_back(0);
+        s->slot_req.push_back(-1);
+    }
+    const HostScene& h = r.scene;
+    int cc, kc, nsinc, nsp;
+    scene_caps(h, cc, kc);
+    static_counts(h, nsinc, nsp);
+    Region reg;
+    if (!place_scene(b->A, h, cc, kc, nsinc, nsp, reg)) return false;
+    b->regions[slot] = reg;
+    upload_scene(b->P, h, static_incidence(h, reg), reg, scene_group(h, b->group_rigid, b->group_fem), slot,
+                 b->descs[slot], s->arena[s->arena_cur]);
+    b->state[slot] = 1;
+    b->bodies[slot] = h.nbody();
+    b->dynamic[slot] = h.ndynamic();
+    if ((int)b->steps_due.size() <= slot) b->steps_due.resize(slot + 1, 0);
+    b->steps_due[slot] = 0;
+    b->order_dirty = true;
+    s->slot_req[slot] = rid;
+    r.slot = slot;
+    r.admitted = now;
+    r.scene = HostScene();   // the device holds it now
+    s->resident_dynamic += r.dynamic;
+    s->stats.admitted += 1;
+    return true;
+}
+
+// Completes the step in flight: waits for it, files the readbacks it
+// brought, retires the scenes it finished.
+int server_complete(AvbdServer* s, double now) {
+    if (!s->in_flight) return 0;
+    AvbdBatch* b = s->b;
+    if (cudaEventSynchronize(s->step_done) != cudaSuccess) return AVBD_ERR_CUDA;
+    s->in_flight = false;
+    // scenes a full table stopped grow and catch up before anything reads them
+    if (int r = batch_fix_capacity(b)) return r;
+    bool refetch = false;
+    for (const Readback& rb : s->rb_list)
+        if (s->rb_state[rb.state_off].status == kStatusCapacity) refetch = true;
+    if (refetch) {
+        // a scene the catch-up re-ran: read its poses again now
+        for (const Readback& rb : s->rb_list) {
+            const ServedRequest& r = s->reqs[rb.req];
+            const SceneDesc& d = b->descs[r.slot];
+            cudaMemcpyAsync(s->rb + rb.off, b->P.W.pos + d.body0, rb.n * sizeof(float4), cudaMemcpyDeviceToHost,
+                            b->stream);
+            cudaMemcpyAsync(s->rb + rb.off + rb.n, b->P.W.rot + d.body0, rb.n * sizeof(float4),
+                            cudaMemcpyDeviceToHost, b->stream);
+            cudaMemcpyAsync(s->rb_state + rb.state_off, b->P.d_sstate + r.slot, sizeof(SceneState),
+                            cudaMemcpyDeviceToHost, b->stream);
+        }
+        if (cudaStreamSynchronize(b->stream) != cudaSuccess) return AVBD_ERR_CUDA;
+    }
+    for (const Readback& rb : s->rb_list) {
+        ServedRequest& r = s->reqs[rb.req];
+        const float4* p = s->rb + rb.off;
+        if (!rb.final) {
+            r.first_pos.assign(p, p + rb.n);
+            r.first_rot.assign(p + rb.n, p + 2 * rb.n);
+            continue;
+        }
+        r.status = s->rb_state[rb.state_off].status;
+        if (r.flags & AVBD_SERVE_KEEP_RESULT) {
+            r.pos.assign(p, p + rb.n);
+            r.rot.assign(p + rb.n, p + 2 * rb.n);
+        }
+        // retire: the slot and its pool ranges go back to the allocator
+        b->A.release(b->regions[r.slot]);
+        b->state[r.slot] = 0;
+        b->bodies[r.slot] = 0;
+        b->dynamic[r.slot] = 0;
+        b->order_dirty = true;
+        s->slot_req[r.slot] = -1;
+        s->resident_dynamic -= r.dynamic;
+        r.finished = now;
+        s->finished.push_back(r.id);
+        s->stats.completed += 1;
+    }
+    s->rb_list.clear();
+    return 0;
+}
+
+// Issues the order list (page-locked copy) when the live set changed.
+int server_sync_order(AvbdServer* s) {
+    AvbdBatch* b = s->b;
+    if (!b->order_dirty) return 0;
+    std::vector<int> order;
+    order.reserve(b->state.size());
+    for (size_t i = 0; i < b->state.size(); ++i)
+        if (b->state[i] == 1) order.push_back((int)i);
+    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
+        const SceneDesc& a = b->descs[x];
+        const SceneDesc& c = b->descs[y];
+        return (a.nbody + a.ntet) > (c.nbody + c.ntet);
+    });
+    const int n = (int)order.size();
+    if (n + 1 > s->order_cap) {
+        if (grow_pinned(reinterpret_cast<void**>(&s->order_host), (size_t)(n + 1 + 1024) * sizeof(int)))
+            return AVBD_ERR_NOMEM;
+        s->order_cap = n + 1 + 1024;
+    }
+    std::copy(order.begin(), order.end(), s->order_host + 1);
+    s->order_host[0] = n;
+    b->nlive = n;
+    if (n) cudaMemcpyAsync(b->d_order, s->order_host + 1, n * sizeof(int), cudaMemcpyHostToDevice, b->stream);
+    cudaMemcpyAsync(b->d_nlive, s->order_host, sizeof(int), cudaMemcpyHostToDevice, b->stream);
+    b->order_dirty = false;
+    return 0;
+}
+
+}  // namespace
+
+extern "C" {
+
+int32_t avbd_server_create(const AvbdParams* params, int32_t device, int64_t bodies, int32_t max_scenes,
+                           AvbdServer** out) {
+    if (!out || bodies < 1 || max_scenes < 1) return AVBD_ERR_INVALID;
+    AvbdBatch* b = nullptr;
+    int r = avbd_batch_create(params, device, &b);
+    if (r) return r;
+    AvbdServer* s = new (std::nothrow) AvbdServer();
+    if (!s) {
+        avbd_batch_destroy(b);
+        return AVBD_ERR_NOMEM;
+    }
+    s->b = b;
+    // pools: the body budget, a quarter as many forces and triangles, two tets per body
+    r = avbd_batch_reserve(b, bodies, bodies / 4, 2 * bodies, bodies / 4, max_scenes);
+    if (!r && cudaEventCreateWithFlags(&s->step_done, cudaEventDisableTiming) != cudaSuccess) r = AVBD_ERR_CUDA;
+    if (r) {
+        avbd_server_destroy(s);
+        return r;
+    }
+    *out = s;
+    return 0;
+}
+
+int32_t avbd_server_destroy(AvbdServer* s) {
+    if (!s) return AVBD_ERR_INVALID;
+    if (s->b) {
+        cudaSetDevice(s->b->device);
+        if (s->b->stream) cudaStreamSynchronize(s->b->stream);
+    }
+    if (s->step_done) cudaEventDestroy(s->step_done);
+    if (s->rb) cudaFreeHost(s->rb);
+    if (s->rb_state) cudaFreeHost(s->rb_state);
+    if (s->order_host) cudaFreeHost(s->order_host);
+    s->arena[0].release();
+    s->arena[1].release();
+    if (s->b) avbd_batch_destroy(s->b);
+    delete s;
+    return 0;
+}
+
+AvbdBatch* avbd_server_batch(AvbdServer* s) { return s ? s->b : nullptr; }
+
+int32_t avbd_server_submit(AvbdServer* s, const AvbdWorld* scene, int32_t steps, double arrival_s, int32_t flags) {
+    if (!s || !scene || steps < 1) return AVBD_ERR_INVALID;
+    ServedRequest r;
+    r.id = (int)s->reqs.size();
+    r.steps = steps;
+    r.flags = flags;
+    r.arrival = arrival_s;
+    r.scene = scene->h;
+    r.nbody = r.scene.nbody();
+    r.dynamic = r.scene.ndynamic();
+    s->reqs.push_back(std::move(r));
+    // arrival order: requests are usually submitted in order; keep the queue sorted
+    auto it = s->pending.end();
+    while (it != s->pending.begin() && s->reqs[*(it - 1)].arrival > arrival_s) --it;
+    s->pending.insert(it, s->reqs.back().id);
+    s->stats.submitted += 1;
+    return s->reqs.back().id;
+}
+
+int32_t avbd_server_tick(AvbdServer* s, double now_s) {
+    if (!s) return AVBD_ERR_INVALID;
+    AvbdBatch* b = s->b;
+    if (cudaSetDevice(b->device) != cudaSuccess) return AVBD_ERR_CUDA;
+    if (!b->grid && batch_launch_shape(b)) return AVBD_ERR_CUDA;
+    // 1. admissions staged while the previous step runs
+    s->arena_cur ^= 1;
+    ArenaSink& arena = s->arena[s->arena_cur];
+    arena.clear();
+    int admitted = 0;
+    while (!s->pending.empty() && s->reqs[s->pending.front()].arrival <= now_s) {
+        if (!server_admit(s, s->pending.front(), now_s)) break;   // no room: wait in arrival order
+        s->pending.pop_front();
+        ++admitted;
+    }
+    if (arena.overflow) return AVBD_ERR_NOMEM;
+    // 2. the step in flight and its readbacks
+    if (int r = server_complete(s, now_s)) return r;
+    // 3. uploads, order, next step, readbacks of the scenes it finishes
+    s->stats.uploaded_bytes += arena.issue(b->stream);
+    if (int r = server_sync_order(s)) return r;
+    if (b->nlive == 0) return 0;
+    b->P.W.P = to_params(b->params);
+    if (!b->graph && batch_build_graph(b)) return AVBD_ERR_CUDA;
+    cudaMemsetAsync(b->d_fail, 0, sizeof(int), b->stream);
+    if (cudaGraphLaunch(b->graph, b->stream) != cudaSuccess) return AVBD_ERR_CUDA;
+    s->stats.ticks += 1;
+    s->stats.body_iterations += s->resident_dynamic * b->params.num_iterations;
+    size_t need = 0;
+    int nstate = 0;
+    for (size_t slot = 0; slot < s->slot_req.size(); ++slot) {
+        const int rid = s->slot_req[slot];
+        if (rid < 0 || b->state[slot] != 1) continue;
+        ServedRequest& r = s->reqs[rid];
+        r.taken += 1;
+        b->steps_due[slot] += 1;
+        const bool final = r.taken >= r.steps;
+        const bool first = r.taken == 1 && (r.flags & AVBD_SERVE_KEEP_FIRST);
+        if (final || first) {
+            s->rb_list.push_back({rid, final, need, r.nbody, nstate});
+            need += 2 * (size_t)r.nbody;
+            ++nstate;
+            if (final && first) {   // a one-step request: the same poses serve both
+                s->rb_list.push_back({rid, false, need - 2 * (size_t)r.nbody, r.nbody, nstate - 1});
+            }
+        }
+    }
+    if (need > s->rb_cap) {
+        if (grow_pinned(reinterpret_cast<void**>(&s->rb), (need + need / 2) * sizeof(float4))) return AVBD_ERR_NOMEM;
+        s->rb_cap = need + need / 2;
+    }
+    if (nstate > s->rb_state_cap) {
+        if (grow_pinned(reinterpret_cast<void**>(&s->rb_state), (size_t)(nstate + 256) * sizeof(SceneState)))
+            return AVBD_ERR_NOMEM;
+        s->rb_state_cap = nstate + 256;
+    }
+    for (const Readback& rb : s->rb_list) {
+        const ServedRequest& r = s->reqs[rb.req];
+        const SceneDesc& d = b->descs[r.slot];
+        if (!rb.final && r.taken >= r.steps) continue;   // shares the final readback
+        cudaMemcpyAsync(s->rb + rb.off, b->P.W.pos + d.body0, rb.n * sizeof(float4), cudaMemcpyDeviceToHost,
+                        b->stream);
+        cudaMemcpyAsync(s->rb + rb.off + rb.n, b->P.W.rot + d.body0, rb.n * sizeof(float4), cudaMemcpyDeviceToHost,
+                        b->stream);
+        cudaMemcpyAsync(s->rb_state + rb.state_off, b->P.d_sstate + r.slot, sizeof(SceneState),
+                        cudaMemcpyDeviceToHost, b->stream);
+    }
+    if (cudaEventRecord(s->step_done, b->stream) != cudaSuccess) return AVBD_ERR_CUDA;
+    s->in_flight = true;
+    return b->nlive;
+}
+
+int32_t avbd_server_drain(AvbdServer* s, double now_s) {
+    if (!s) return AVBD_ERR_INVALID;
+    if (cudaSetDevice(s->b->device) != cudaSuccess) return AVBD_ERR_CUDA;
+    return server_complete(s, now_s);
+}
+
+int32_t avbd_server_poll(AvbdServer* s, AvbdServedRequest* out) {
+    if (!s || !out) return AVBD_ERR_INVALID;
+    if (s->finished.empty()) return 0;
+    const ServedRequest& r = s->reqs[s->finished.front()];
+    s->finished.pop_front();
+    out->request = r.id;
+    out->status = r.status;
+    out->steps = r.steps;
+    out->bodies = r.nbody;
+    out->arrival_s = r.arrival;
+    out->admitted_s = r.admitted;
+    out->finished_s = r.finished;
+    return 1;
+}
+
+int32_t avbd_server_result(AvbdServer* s, int32_t request, float* pos, float* quat_wxyz, float* first_pos,
+                           float* first_quat_wxyz) {
+    if (!s || request < 0 || request >= (int)s->reqs.size()) return AVBD_ERR_INVALID;
+    const ServedRequest& r = s->reqs[request];
+    if (r.finished < 0.0) return AVBD_ERR_STATE;
+    auto put = [](const std::vector<float4>& p, const std::vector<float4>& q, float* pd, float* qd) {
+        for (size_t i = 0; i < p.size(); ++i) {
+            if (pd) { pd[3 * i] = p[i].x; pd[3 * i + 1] = p[i].y; pd[3 * i + 2] = p[i].z; }
+            if (qd) { qd[4 * i] = q[i].w; qd[4 * i + 1] = q[i].x; qd[4 * i + 2] = q[i].y; qd[4 * i + 3] = q[i].z; }
+        }
+    };
+    if ((pos || quat_wxyz) && r.pos.empty()) return AVBD_ERR_STATE;
+    if ((first_pos || first_quat_wxyz) && r.first_pos.empty()) return AVBD_ERR_STATE;
+    put(r.pos, r.rot, pos, quat_wxyz);
+    put(r.first_pos, r.first_rot, first_pos, first_quat_wxyz);
+    return r.nbody;
+}
+
+int32_t avbd_server_release(AvbdServer* s, int32_t request) {
+    if (!s || request < 0 || request >= (int)s->reqs.size()) return AVBD_ERR_INVALID;
+    ServedRequest& r = s->reqs[request];
+    std::vector<float4>().swap(r.pos);
+    std::vector<float4>().swap(r.rot);
+    std::vector<float4>().swap(r.first_pos);
+    std::vector<float4>().swap(r.first_rot);
+    return 0;
+}
+
+int32_t avbd_server_stats(const AvbdServer* s, AvbdServerStats* out) {
+    if (!s || !out) return AVBD_ERR_INVALID;
+    *out = s->stats;
+    out->pending = (int64_t)s->pending.size();
+    int64_t active = 0;
+    for (int rid : s->slot_req) active += rid >= 0 ? 1 : 0;
+    out->active = active;
+    out->resident_dynamic = s->resident_dynamic;
+    return 0;
+}
+
+}  // extern "C"

@@ -9,7 +9,6 @@
 namespace avbd {
 
 constexpr unsigned kFull = 0xffffffffu;
-constexpr int kStagedBodies = 2560;   // stage of a 256-thread CTA (40 KB); smaller CTAs get proportionally less
 constexpr int kMaxTeams = 8;          // teams a CTA may split into
 
 // Scalars a team shares through shared memory.

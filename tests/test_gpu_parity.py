@@ -62,10 +62,10 @@ def test_one_step_parity(oracle_mod, Solver, name):
     assert rot_err(qo, qg).max(initial=0.0) <= ROT_TOL
 
 
-# Particle orientations of the full-size 0.05 m block: the reference itself
-# moves them by up to 5.5e-4 rad (10 iterations) when Young's modulus or the
-# particle mass changes by one float32 ulp, with the same contact set (its
-# positions move by up to 5.5e-5 m).  A particle has no rotational inertia
+# Particle orientations of the full-size 0.05 m block: at 20 iterations the
+# reference itself moves them by up to 9.9e-4 rad (20 particles beyond 1e-4
+# rad) when Young's modulus changes by one float32 ulp, with the same
+# contact set (its positions move by up to 7.7e-5 m).  A particle has no rotational inertia
 # (solver.cpp:119-131): its rotational block is contact torques alone and
 # close to singular, so rounding-level differences anywhere in the step
 # reach these orientations amplified.
@@ -253,21 +253,22 @@ def test_cpp_facade_matches_python(Solver, tmp_path):
 
 
 def test_remove_body_mid_run(Solver):
-    """RemoveBody after the first steps: the body stops (its pose is kept),
-    its manifolds go, and the rest of the scene steps on."""
+    """RemoveBody after the first steps: the body leaves (its state reads
+    NaN), its manifolds go, and the rest of the scene steps on."""
     g = Solver()
     scenes.level_pyramid(g)
     for _ in range(3):
         assert g.step() == "ok"
     top = g.num_bodies - 1
     g.remove_body(top)
-    kept = g.get_state()[0][top].copy()
+    assert np.isnan(g.get_state()[0][top]).all()
     for _ in range(5):
         assert g.step() == "ok"
     p = g.get_state()[0]
-    assert np.array_equal(p[top], kept)
+    assert np.isnan(p[top]).all()
     assert all(top not in pair for pair in g.contacts())
-    assert np.isfinite(p).all()
+    keep = np.arange(len(p)) != top
+    assert np.isfinite(p[keep]).all()
 
 
 @pytest.mark.parametrize("name", ["pyramid", "joint_playground", "soft_beam"])

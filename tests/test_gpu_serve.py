@@ -89,3 +89,26 @@ def test_served_results_equal_alone():
         assert same(req.result, alone(f, steps)), f"request {req.rid}"
     st = srv.latency_stats()
     assert st["completed"] == len(arrivals) and st["p99_s"] >= st["p50_s"] > 0
+
+
+def test_server_admits_by_pool_space_and_keeps_samples():
+    """A server whose pools hold two of three equal requests: the third waits
+    for a retirement, every result equals the scene alone, and a sampled
+    request's first-step poses equal one step alone."""
+    from skyephyx_b200.serve import Request, Server
+    build = lambda s: scenes.rigid_pile(s, 400, scenes.rng_for(4, 21), stack=False)
+    srv = Server(budget_bytes=1000 * 9000, max_scenes=8)   # about 1,000 bodies of pool space
+    steps = [4, 6, 5]
+    for i, n in enumerate(steps):
+        srv.submit(Request(rid=i, scene=staged(build), steps=n, arrival=0.0, sample=(i == 2)))
+    srv.start()
+    srv.run()
+    done = {r.rid: r for r in srv.done}
+    assert sorted(done) == [0, 1, 2]
+    assert done[2].admitted >= min(done[0].finished, done[1].finished)
+    for i, n in enumerate(steps):
+        assert done[i].status == "ok"
+        assert same(done[i].result, alone(build, n)), f"request {i}"
+    assert same(done[2].first, alone(build, 1))
+    st = srv.stats()
+    assert st["completed"] == 3 and st["pending"] == 0 and st["active"] == 0
