@@ -134,6 +134,13 @@ int32_t avbd_make_tet_volume(AvbdWorld* w, float ox, float oy, float oz, int32_t
                              float cell_size, float youngs_modulus, float poisson_ratio, float particle_mass,
                              float friction, int32_t pin_min_x);
 
+/* GeometryHelpers::makeTetSphere (geometry.cpp:106-232): a centre particle
+ * and N = round(res) concentric shells of 6N x 3N ring particles plus poles,
+ * filled with Neo-Hookean tets (the innermost shell fanned to the centre,
+ * prisms of 3 tets between shells).  Returns the id of the first particle. */
+int32_t avbd_make_tet_sphere(AvbdWorld* w, float cx, float cy, float cz, float radius, float res,
+                             float youngs_modulus, float poisson_ratio, float particle_mass, float friction);
+
 /* Solver::RemoveBody (solver.hpp:49, solver.cpp:104-115) and Mesh::~Mesh (geometry.cpp:11-25):
  * the body and every force and energy on it stop taking part.  Ids stay
  * stable (the reference swap-removes and renumbers).  Valid before or after
@@ -181,6 +188,30 @@ int32_t avbd_set_state(AvbdWorld* w, const float* pos, const float* quat_wxyz, c
 int64_t avbd_snapshot_bytes(const AvbdWorld* w);
 int32_t avbd_snapshot(AvbdWorld* w, void* dst, int64_t bytes);
 int32_t avbd_restore(AvbdWorld* w, const void* src, int64_t bytes);
+
+/* Mesh::color (AddBody's color argument, solver.cpp:50); default white.
+ * Read only by the instance export. */
+int32_t avbd_set_body_color(AvbdWorld* w, int32_t body, const float rgb[3]);
+
+/* The renderer's GPUInstanceData (RenderEngine.hpp:43-49), 128 bytes:
+ * model matrix (column-major 4x4: rotation x scale, position), normal matrix
+ * (the inverse transpose of its 3x3 block, three columns padded to four
+ * floats) and colour (r, g, b, 1). */
+typedef struct AvbdInstance {
+    float model[16];
+    float normal[12];
+    float color[4];
+} AvbdInstance;
+
+/* Headless pose export (RenderEngine::UpdateInstanceBuffer,
+ * RenderEngine.cpp:951-1000, without a graphics API): one AvbdInstance per
+ * live body, grouped by model type (cube, sphere, pyramid) and by body id
+ * within a type, as the renderer packs its per-model batches.  dst is device
+ * memory an external renderer can read (written in place by a kernel) or
+ * host memory (copied).  first/count per model may be NULL.  Returns the
+ * instances written, AVBD_ERR_INVALID when capacity is too small. */
+int32_t avbd_export_instances(AvbdWorld* w, AvbdInstance* dst, int32_t capacity, int32_t first_per_model[3],
+                              int32_t count_per_model[3]);
 
 /* Live contact manifolds after the last step (parity introspection).
  * Returns the count; fills up to max entries: pairs (A,B) body ids, counts,
@@ -265,6 +296,9 @@ int32_t avbd_batch_get_state(AvbdBatch* b, int32_t scene, float* pos, float* qua
  * host buffers of max_bodies float4; a scene's bodies start at
  * avbd_batch_scene_body_offset(). */
 int32_t avbd_batch_get_all_poses(AvbdBatch* b, float* pos, float* quat_xyzw, int64_t max_bodies);
+/* avbd_export_instances for one scene of a batch. */
+int32_t avbd_batch_export_instances(AvbdBatch* b, int32_t scene, AvbdInstance* dst, int32_t capacity,
+                                    int32_t first_per_model[3], int32_t count_per_model[3]);
 /* Device bytes a scene staged in `w` needs inside a batch (admission control). */
 int64_t avbd_scene_footprint_bytes(const AvbdWorld* w);
 /* Per-scene counters after the last step: status, colours, candidate pairs,
@@ -338,11 +372,13 @@ typedef struct AvbdServerStats {
 } AvbdServerStats;
 
 /* Pools for `bodies` bodies (a quarter as many joints+springs and
- * triangles, two tets per body) and `max_scenes` resident scenes. */
+ * triangles, two tets per body) and `max_scenes` resident scenes, reserved
+ * at the first tick. */
 int32_t avbd_server_create(const AvbdParams* params, int32_t device, int64_t bodies, int32_t max_scenes,
                            AvbdServer** out);
 int32_t avbd_server_destroy(AvbdServer* s);
-/* The server's batch, for the launch knobs (avbd_batch_set_*) before the first tick. */
+/* The server's batch, for the launch knobs (avbd_batch_set_*) before the
+ * first tick; the server drives it (do not step or add scenes directly). */
 AvbdBatch* avbd_server_batch(AvbdServer* s);
 /* Copies the scene staged in `scene` (built, never stepped) as a request of
  * `steps` steps arriving at `arrival_s` (the caller's clock, as passed to

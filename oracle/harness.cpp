@@ -636,6 +636,21 @@ int orc_make_tet_volume(void* h, float ox, float oy, float oz, int nx, int ny, i
     return first;
 }
 
+// GeometryHelpers::makeTetSphere (geometry.cpp:106-232), the reference's own.
+int orc_make_tet_sphere(void* h, float cx, float cy, float cz, float radius, float res, float E, float nu,
+                        float particle_mass, float friction) {
+    Orc* o = static_cast<Orc*>(h);
+    const size_t b0 = o->solver.solverBodies.size();
+    const size_t e0 = o->solver.solverEnergies.size();
+    GeometryHelpers::makeTetSphere(&o->solver, cx, cy, cz, radius, res, E, nu, Eigen::Vector3f(1, 1, 1),
+                                   particle_mass, friction);
+    const int first = (int)o->bodies.size();
+    for (size_t i = b0; i < o->solver.solverBodies.size(); ++i) o->bodies.push_back(o->solver.solverBodies[i].get());
+    for (size_t i = e0; i < o->solver.solverEnergies.size(); ++i)
+        o->energies.push_back(o->solver.solverEnergies[i].get());
+    return first;
+}
+
 // makeTetVolume's particles and tets (geometry.cpp:30-94) with StVK tets: the
 // reference builds the volume with Neo-Hookean tets, which are then replaced,
 // in creation order, by StVK tets on the same bodies.

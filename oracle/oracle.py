@@ -77,6 +77,7 @@ def _lib(kind: str = "parity"):
         "orc_make_stvk_tet_volume": ([vp, real, real, real, C.c_int, C.c_int, C.c_int, real,
                                       real, real, real, real, C.c_int], C.c_int),
         "orc_add_stvk_tet": ([vp, ip, real, real], C.c_int),
+        "orc_make_tet_sphere": ([vp, real, real, real, real, real, real, real, real, real], C.c_int),
         "orc_step": ([vp], C.c_int),
         "orc_step_coloured": ([vp, C.c_int], C.c_int),
         "orc_step_many": ([C.POINTER(vp), C.c_int, C.c_int, C.c_int, C.c_int], C.c_double),
@@ -210,6 +211,10 @@ class OracleSolver:
         return self._lib.orc_make_tet_volume(self._h, _r(ox), _r(oy), _r(oz), int(nx), int(ny), int(nz),
                                              _r(cell), _r(E), _r(nu), _r(particle_mass),
                                              _r(friction), int(bool(pin_min_x)))
+
+    def make_tet_sphere(self, cx, cy, cz, radius, res, E, nu, particle_mass=1.0, friction=0.5):
+        return self._lib.orc_make_tet_sphere(self._h, _r(cx), _r(cy), _r(cz), _r(radius), _r(res), _r(E), _r(nu),
+                                             _r(particle_mass), _r(friction))
 
     # ---- stepping ----
     def step(self):

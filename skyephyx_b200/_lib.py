@@ -78,6 +78,11 @@ SIGNATURES = [
     ("avbd_make_stvk_tet_volume", [_V, C.c_float, C.c_float, C.c_float, C.c_int32, C.c_int32, C.c_int32, C.c_float,
                               C.c_float, C.c_float, C.c_float, C.c_float, C.c_int32], C.c_int32),
     ("avbd_add_stvk_tet", [_V, _I, C.c_float, C.c_float], C.c_int32),
+    ("avbd_set_body_color", [_V, C.c_int32, _F], C.c_int32),
+    ("avbd_export_instances", [_V, _V, C.c_int32, _I, _I], C.c_int32),
+    ("avbd_batch_export_instances", [_V, C.c_int32, _V, C.c_int32, _I, _I], C.c_int32),
+    ("avbd_make_tet_sphere", [_V, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float,
+                              C.c_float, C.c_float], C.c_int32),
     ("avbd_remove_body", [_V, C.c_int32], C.c_int32),
     ("avbd_remove_force", [_V, C.c_int32], C.c_int32),
     ("avbd_remove_neohookean_tet", [_V, C.c_int32], C.c_int32),

@@ -212,6 +212,65 @@ __global__ void k_remove_item(const __grid_constant__ World W, int kind, int idx
     W.sstate[0].topo += 1;
 }
 
+// Headless instance export (RenderEngine::UpdateInstanceBuffer,
+// RenderEngine.cpp:951-1000): one 128-byte record per live body, packed by
+// model type in ModelType order and by body id within a type, the order the
+// renderer's per-model batches take.  One CTA: per model, a chunked scan of
+// "live body of this model" gives each body its place.
+__global__ void __launch_bounds__(1024) k_export_instances(const __grid_constant__ World W, int body0, int nbody,
+                                                           AvbdInstance* dst, int cap, int* counts) {
+    __shared__ int s_warp[32];
+    __shared__ int s_base;
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5, nwarps = blockDim.x >> 5;
+    if (tid == 0) s_base = 0;
+    __syncthreads();
+    for (int m = 0; m < 3; ++m) {
+        if (tid == 0) counts[m] = s_base;   // first instance of this model (counts[3 + m]: how many)
+        const int start = s_base;
+        __syncthreads();
+        for (int c0 = 0; c0 < nbody; c0 += blockDim.x) {
+            const int i = c0 + tid;
+            bool take = false;
+            if (i < nbody) {
+                const int fl = W.flags[body0 + i];
+                take = !(fl & kBodyRemoved) && ((fl >> kBodyModelShift) & 15) == m;
+            }
+            const unsigned bal = __ballot_sync(0xffffffffu, take);
+            if (lane == 0) s_warp[warp] = __popc(bal);
+            __syncthreads();
+            int before = 0, total = 0;
+            for (int w = 0; w < nwarps; ++w) {
+                const int v = s_warp[w];
+                if (w < warp) before += v;
+                total += v;
+            }
+            const int k = s_base + before + __popc(bal & ((1u << lane) - 1u));
+            if (take && k < cap) {
+                const int b = body0 + i;
+                const Q4 q = q4(W.rot[b]);
+                const M3 R = rotmat(q);
+                const float4 s = W.scale[b], p = W.pos[b], col = W.color[b];
+                float4* out = reinterpret_cast<float4*>(dst + k);
+                // modelMatrix (column-major 4x4): R diag(s) | position
+                out[0] = make_float4(R.c[0].x * s.x, R.c[0].y * s.x, R.c[0].z * s.x, 0.f);
+                out[1] = make_float4(R.c[1].x * s.y, R.c[1].y * s.y, R.c[1].z * s.y, 0.f);
+                out[2] = make_float4(R.c[2].x * s.z, R.c[2].y * s.z, R.c[2].z * s.z, 0.f);
+                out[3] = make_float4(p.x, p.y, p.z, 1.f);
+                // normalMatrix: (R diag(s))^-T = R diag(1/s), columns padded to 4
+                out[4] = make_float4(R.c[0].x / s.x, R.c[0].y / s.x, R.c[0].z / s.x, 0.f);
+                out[5] = make_float4(R.c[1].x / s.y, R.c[1].y / s.y, R.c[1].z / s.y, 0.f);
+                out[6] = make_float4(R.c[2].x / s.z, R.c[2].y / s.z, R.c[2].z / s.z, 0.f);
+                out[7] = make_float4(col.x, col.y, col.z, 1.f);
+            }
+            __syncthreads();
+            if (tid == 0) s_base += total;
+            __syncthreads();
+        }
+        if (tid == 0) counts[3 + m] = s_base - start;
+        __syncthreads();
+    }
+}
+
 __global__ void k_collide(const __grid_constant__ World W, int a, int b, uint32_t* ids, float* data, int* n) {
     if (blockIdx.x != 0 || threadIdx.x != 0) return;
     Collision col;
@@ -231,6 +290,43 @@ __global__ void k_collide(const __grid_constant__ World W, int a, int b, uint32_
 
 }  // namespace
 
+namespace avbd {
+namespace host {
+
+int export_instances(const World& W, int body0, int nbody, AvbdInstance* dst, int32_t capacity,
+                     int32_t first_per_model[3], int32_t count_per_model[3], cudaStream_t st) {
+    if (!dst || capacity < 0) return AVBD_ERR_INVALID;
+    cudaPointerAttributes attr{};
+    const bool on_device = cudaPointerGetAttributes(&attr, dst) == cudaSuccess &&
+                           (attr.type == cudaMemoryTypeDevice || attr.type == cudaMemoryTypeManaged);
+    cudaGetLastError();
+    AvbdInstance* out = dst;
+    int* d_counts = nullptr;
+    if (cudaMalloc(&d_counts, 6 * sizeof(int)) != cudaSuccess) return AVBD_ERR_NOMEM;
+    if (!on_device && capacity > 0 &&
+        cudaMalloc(&out, (size_t)capacity * sizeof(AvbdInstance)) != cudaSuccess) {
+        cudaFree(d_counts);
+        return AVBD_ERR_NOMEM;
+    }
+    k_export_instances<<<1, 1024, 0, st>>>(W, body0, nbody, out, capacity, d_counts);
+    int counts[6] = {};
+    cudaMemcpyAsync(counts, d_counts, sizeof(counts), cudaMemcpyDeviceToHost, st);
+    cudaError_t e = cudaStreamSynchronize(st);
+    const int total = counts[3] + counts[4] + counts[5];
+    if (e == cudaSuccess && !on_device && capacity > 0)
+        e = cudaMemcpy(dst, out, (size_t)std::min(total, capacity) * sizeof(AvbdInstance), cudaMemcpyDeviceToHost);
+    if (!on_device && capacity > 0) cudaFree(out);
+    cudaFree(d_counts);
+    if (e != cudaSuccess) return AVBD_ERR_CUDA;
+    for (int m = 0; m < 3; ++m) {
+        if (first_per_model) first_per_model[m] = counts[m];
+        if (count_per_model) count_per_model[m] = counts[3 + m];
+    }
+    return total > capacity ? AVBD_ERR_INVALID : total;
+}
+
+}  // namespace host
+}  // namespace avbd
 
 namespace {
 
@@ -710,6 +806,37 @@ int32_t avbd_make_tet_volume(AvbdWorld* w, float ox, float oy, float oz, int32_t
     AVBD_STAGING_ONLY(w);
     int r = w->h.make_tet_volume(ox, oy, oz, nx, ny, nz, cell, E, nu, pm, friction, pin != 0);
     return r < 0 ? AVBD_ERR_INVALID : r;
+}
+
+int32_t avbd_set_body_color(AvbdWorld* w, int32_t body, const float rgb[3]) {
+    if (!w || !rgb || body < 0 || body >= w->h.nbody()) return AVBD_ERR_INVALID;
+    w->h.color[body] = make_float4(rgb[0], rgb[1], rgb[2], 1.f);
+    if (w->uploaded) {
+        cudaSetDevice(w->device);
+        if (cudaMemcpy(w->P.W.color + w->descs[0].body0 + body, &w->h.color[body], sizeof(float4),
+                       cudaMemcpyHostToDevice) != cudaSuccess)
+            return AVBD_ERR_CUDA;
+    }
+    return 0;
+}
+
+int32_t avbd_export_instances(AvbdWorld* w, AvbdInstance* dst, int32_t capacity, int32_t first_per_model[3],
+                              int32_t count_per_model[3]) {
+    if (!w) return AVBD_ERR_INVALID;
+    if (!w->uploaded) {
+        int r = upload(w);
+        if (r) return r;
+    }
+    if (cudaSetDevice(w->device) != cudaSuccess) return AVBD_ERR_CUDA;
+    return export_instances(w->P.W, w->descs[0].body0, w->h.nbody(), dst, capacity, first_per_model,
+                            count_per_model, w->stream);
+}
+
+int32_t avbd_make_tet_sphere(AvbdWorld* w, float cx, float cy, float cz, float radius, float res, float E, float nu,
+                             float pm, float friction) {
+    AVBD_STAGING_ONLY(w);
+    if (!(radius > 0.f) || !(res > 0.f) || res > 64.f) return AVBD_ERR_INVALID;
+    return w->h.make_tet_sphere(cx, cy, cz, radius, res, E, nu, pm, friction);
 }
 
 int32_t avbd_step(AvbdWorld* w) {

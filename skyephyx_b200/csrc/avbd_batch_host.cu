@@ -637,13 +637,22 @@ int32_t avbd_batch_get_all_poses(AvbdBatch* b, float* pos, float* quat, int64_t 
     return n;
 }
 
+int32_t avbd_batch_export_instances(AvbdBatch* b, int32_t scene, AvbdInstance* dst, int32_t capacity,
+                                    int32_t first_per_model[3], int32_t count_per_model[3]) {
+    if (!live_slot(b, scene)) return AVBD_ERR_INVALID;
+    if (int r = batch_settle(b)) return r;
+    if (cudaSetDevice(b->device) != cudaSuccess) return AVBD_ERR_CUDA;
+    return export_instances(b->P.W, b->descs[scene].body0, b->bodies[scene], dst, capacity, first_per_model,
+                            count_per_model, b->stream);
+}
+
 int32_t avbd_batch_scene_body_offset(const AvbdBatch* b, int32_t scene) {
     if (!live_slot(b, scene)) return AVBD_ERR_INVALID;
     return b->descs[scene].body0;
 }
 
 // Device bytes per unit of each pool (allocate_all / alloc_tables).
-constexpr int64_t kBytesPerBody = 15 * 16 + 18 * 4;        // float4 state + per-body ints
+constexpr int64_t kBytesPerBody = 16 * 16 + 18 * 4;        // float4 state + per-body ints
 constexpr int64_t kBytesPerCand = 2 * (8 + 4 + 4 + 4 + 4 + 4);  // two manifold tables
 constexpr int64_t kBytesPerContact = 2 * (4 + 9 * 16);      // two contact pools
 constexpr int64_t kBytesPerForce = 4 + 8 + 6 * 16 + 6 * 6 * 4;

@@ -70,6 +70,7 @@ constexpr int kBodyStatic = 1;
 constexpr int kBodyParticle = 2;
 constexpr int kBodyHasMass = 4;       // !isStatic && mass > 0 at the mass cache
 constexpr int kBodyRemoved = 8;
+constexpr int kBodyModelShift = 8;    // flags bits 8..11: the body's ModelType (geometry.hpp:17-22)
 
 // incidence entry kinds (top 3 bits) and roles (next 2 bits)
 constexpr uint32_t kEntForce = 0u;
@@ -170,6 +171,7 @@ struct World {
     float4* Mw1;        // world I (xy, xz, yz), unused
     int* flags;
     float* friction;
+    float4* color;      // Mesh::color (r g b 1): read only by the instance export
     int* colour;
     int* local;         // body index within its scene
     int* reset_flag;    // set by a fracturing force for the manifold reset pass

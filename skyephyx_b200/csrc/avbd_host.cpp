@@ -1,8 +1,10 @@
 // Host staging of scenes (see avbd_host.h).  Compiled with -ffp-contract=off.
 #include "avbd_host.h"
 
+#include <algorithm>
 #include <cmath>
 #include <cstring>
+#include <utility>
 
 namespace avbd {
 
@@ -82,8 +84,9 @@ int HostScene::add_body(int model, float density, float fr, const float* p, cons
     vel.push_back(mk4(v[0], v[1], v[2]));
     omega.push_back(mk4(w[0], w[1], w[2]));
     massI.push_back(mk4(mass, Ix, Iy, Iz));
-    flags.push_back(is_static ? kBodyStatic : 0);
+    flags.push_back((is_static ? kBodyStatic : 0) | ((model & 15) << kBodyModelShift));
     friction.push_back(fr);
+    color.push_back(mk4(1.f, 1.f, 1.f, 1.f));
     return (int)pos.size() - 1;
 }
 
@@ -272,6 +275,90 @@ int HostScene::make_tet_volume(float ox, float oy, float oz, int nx, int ny, int
                     else add_nh_tet(t, E, nu);
                 }
             }
+    return first;
+}
+
+int HostScene::make_tet_sphere(float cx, float cy, float cz, float radius, float res, float E, float nu,
+                               float pm, float fr) {
+    // GeometryHelpers::makeTetSphere (geometry.cpp:106-232): a centre
+    // particle, N concentric shells of 6N x 3N ring particles plus two poles,
+    // the innermost shell fanned to the centre, each outer shell joined to the
+    // one inside by triangular prisms of 3 tets; every tet's last two
+    // vertices swap when its rest volume would be negative.  Positions are
+    // formed with the reference's float operations, in its order.
+    const int N = std::max(1, (int)std::roundf(res));
+    const int nLon = 6 * N, nLat = 3 * N, nShells = N;
+    const int vps = 2 + nLat * nLon;
+    std::vector<int> pts(1 + (size_t)nShells * vps, -1);
+    auto sBase = [&](int sh) { return 1 + sh * vps; };
+    auto sSouth = [&](int sh) { return sBase(sh); };
+    auto sNorth = [&](int sh) { return sBase(sh) + 1; };
+    auto sV = [&](int sh, int j, int i) { return sBase(sh) + 2 + j * nLon + ((i % nLon + nLon) % nLon); };
+    const float zero[3] = {0.f, 0.f, 0.f};
+    auto makeP = [&](float x, float y, float z) {
+        const float p[3] = {x, y, z};
+        return add_particle(pm, fr, p, zero, false);
+    };
+    const int first = nbody();
+    pts[0] = makeP(cx, cy, cz);
+    const float pi = (float)M_PI;
+    for (int sh = 0; sh < nShells; sh++) {
+        const float r = radius * (sh + 1) / (float)nShells;
+        pts[sSouth(sh)] = makeP(cx, cy - r, cz);
+        pts[sNorth(sh)] = makeP(cx, cy + r, cz);
+        for (int j = 0; j < nLat; j++) {
+            const float theta = pi * (j + 1) / (float)(nLat + 1);
+            const float sinT = std::sin(theta), cosT = std::cos(theta);
+            for (int i = 0; i < nLon; i++) {
+                const float phi = 2.f * pi * i / (float)nLon;
+                pts[sV(sh, j, i)] = makeP(cx + r * sinT * std::cos(phi), cy + r * cosT, cz + r * sinT * std::sin(phi));
+            }
+        }
+    }
+    auto addTet = [&](int a, int b, int c, int d) {
+        const float4 pa = pos[a], pb = pos[b], pc = pos[c], pd = pos[d];
+        // columns b - a, c - a, d - a; determinant by the first column's cofactors
+        const float m00 = pb.x - pa.x, m10 = pb.y - pa.y, m20 = pb.z - pa.z;
+        const float m01 = pc.x - pa.x, m11 = pc.y - pa.y, m21 = pc.z - pa.z;
+        const float m02 = pd.x - pa.x, m12 = pd.y - pa.y, m22 = pd.z - pa.z;
+        const float det = m00 * (m11 * m22 - m12 * m21) - m10 * (m01 * m22 - m02 * m21) +
+                          m20 * (m01 * m12 - m02 * m11);
+        if (det < 0.f) std::swap(c, d);
+        const int v[4] = {a, b, c, d};
+        add_nh_tet(v, E, nu);
+    };
+    auto addPrism = [&](int P0, int P1, int P2, int Q0, int Q1, int Q2) {
+        addTet(P0, P1, P2, Q2);
+        addTet(P0, Q1, P1, Q2);
+        addTet(P0, Q0, Q1, Q2);
+    };
+    for (int sh = 0; sh < nShells; sh++) {
+        const bool fan = sh == 0;
+        const int sIn = sh - 1;
+        for (int i = 0; i < nLon; i++) {
+            const int i1 = (i + 1) % nLon;
+            if (fan) addTet(pts[0], pts[sNorth(sh)], pts[sV(sh, 0, i)], pts[sV(sh, 0, i1)]);
+            else addPrism(pts[sNorth(sIn)], pts[sV(sIn, 0, i)], pts[sV(sIn, 0, i1)], pts[sNorth(sh)],
+                          pts[sV(sh, 0, i)], pts[sV(sh, 0, i1)]);
+            const int jS = nLat - 1;
+            if (fan) addTet(pts[0], pts[sSouth(sh)], pts[sV(sh, jS, i)], pts[sV(sh, jS, i1)]);
+            else addPrism(pts[sSouth(sIn)], pts[sV(sIn, jS, i)], pts[sV(sIn, jS, i1)], pts[sSouth(sh)],
+                          pts[sV(sh, jS, i)], pts[sV(sh, jS, i1)]);
+        }
+        for (int j = 0; j < nLat - 1; j++)
+            for (int i = 0; i < nLon; i++) {
+                const int i1 = (i + 1) % nLon;
+                if (fan) {
+                    addTet(pts[0], pts[sV(sh, j, i)], pts[sV(sh, j, i1)], pts[sV(sh, j + 1, i1)]);
+                    addTet(pts[0], pts[sV(sh, j, i)], pts[sV(sh, j + 1, i1)], pts[sV(sh, j + 1, i)]);
+                } else {
+                    addPrism(pts[sV(sIn, j, i)], pts[sV(sIn, j, i1)], pts[sV(sIn, j + 1, i1)], pts[sV(sh, j, i)],
+                             pts[sV(sh, j, i1)], pts[sV(sh, j + 1, i1)]);
+                    addPrism(pts[sV(sIn, j, i)], pts[sV(sIn, j + 1, i1)], pts[sV(sIn, j + 1, i)], pts[sV(sh, j, i)],
+                             pts[sV(sh, j + 1, i1)], pts[sV(sh, j + 1, i)]);
+                }
+            }
+    }
     return first;
 }
 

@@ -17,7 +17,7 @@ namespace avbd {
 
 struct HostScene {
     // bodies
-    std::vector<float4> pos, rot, scale, vel, omega, massI;
+    std::vector<float4> pos, rot, scale, vel, omega, massI, color;
     std::vector<int> flags;
     std::vector<float> friction;
     // joints / springs
@@ -58,6 +58,8 @@ struct HostScene {
     int add_stvk_tri(const int* v, float E, float nu);
     int make_tet_volume(float ox, float oy, float oz, int nx, int ny, int nz, float cell, float E, float nu,
                         float particle_mass, float friction_, bool pin_min_x, int model = kTetNeoHookean);
+    int make_tet_sphere(float cx, float cy, float cz, float radius, float res, float E, float nu,
+                        float particle_mass, float friction_);
 
     // Static incidence (forces then energies per body) and joint/spring partner
     // lists.  Offsets are relative to the scene's own entry / partner arrays;

@@ -90,6 +90,7 @@ struct Pools {
         A(alloc(W.omega, nb)); A(alloc(W.pvel, nb)); A(alloc(W.dlin, nb)); A(alloc(W.dang, nb));
         A(alloc(W.massI, nb)); A(alloc(W.Mw0, nb)); A(alloc(W.Mw1, nb));
         A(alloc(W.flags, nb)); A(alloc(W.friction, nb)); A(alloc(W.colour, nb)); A(alloc(W.local, nb));
+        A(alloc(W.color, nb));
         A(alloc(W.reset_flag, nb));
         A(alloc_c(W.sinc_off, nb)); A(alloc_c(W.sinc_n, nb)); A(alloc_c(W.sinc_nf, nb)); A(alloc_c(W.sinc, nsinc));
         A(alloc_c(W.spartner_off, nb)); A(alloc_c(W.spartner_n, nb)); A(alloc_c(W.spartner, 2 * (size_t)nsp));
@@ -459,6 +460,7 @@ inline void upload_scene(Pools& P, const HostScene& h, const StaticInc& si, cons
     sink.put(W.pos, h.pos, d.body0); sink.put(W.rot, h.rot, d.body0); sink.put(W.scale, h.scale, d.body0);
     sink.put(W.vel, h.vel, d.body0); sink.put(W.omega, h.omega, d.body0); sink.put(W.massI, h.massI, d.body0);
     sink.put(W.flags, h.flags, d.body0); sink.put(W.friction, h.friction, d.body0);
+    sink.put(W.color, h.color, d.body0);
     sink.put(W.lpos, h.pos, d.body0); sink.put(W.lrot, h.rot, d.body0);
     sink.put(W.ipos, h.pos, d.body0); sink.put(W.irot, h.rot, d.body0);
     sink.zero(W.pvel, d.body0, d.nbody);
@@ -610,6 +612,10 @@ struct AvbdBatch {
 
 namespace avbd {
 namespace host {
+
+// Instance export of the bodies [body0, body0 + nbody) (avbd_api.cu).
+int export_instances(const World& W, int body0, int nbody, AvbdInstance* dst, int32_t capacity,
+                     int32_t first_per_model[3], int32_t count_per_model[3], cudaStream_t st);
 
 // Batch internals (avbd_batch_host.cu) used by the serving loop.
 int batch_stream(AvbdBatch* b);

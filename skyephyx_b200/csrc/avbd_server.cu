@@ -77,6 +77,8 @@ struct AvbdServer {
     cudaEvent_t step_done = nullptr;
     bool in_flight = false;
     int64_t resident_dynamic = 0;
+    int64_t pool_bodies = 0;            // pool capacity, reserved at the first tick
+    int max_scenes = 0;
     AvbdServerStats stats{};
 };
 
@@ -230,9 +232,9 @@ int32_t avbd_server_create(const AvbdParams* params, int32_t device, int64_t bod
         return AVBD_ERR_NOMEM;
     }
     s->b = b;
-    // pools: the body budget, a quarter as many forces and triangles, two tets per body
-    r = avbd_batch_reserve(b, bodies, bodies / 4, 2 * bodies, bodies / 4, max_scenes);
-    if (!r && cudaEventCreateWithFlags(&s->step_done, cudaEventDisableTiming) != cudaSuccess) r = AVBD_ERR_CUDA;
+    s->pool_bodies = bodies;
+    s->max_scenes = max_scenes;
+    if (cudaEventCreateWithFlags(&s->step_done, cudaEventDisableTiming) != cudaSuccess) r = AVBD_ERR_CUDA;
     if (r) {
         avbd_server_destroy(s);
         return r;
@@ -283,6 +285,11 @@ int32_t avbd_server_tick(AvbdServer* s, double now_s) {
     if (!s) return AVBD_ERR_INVALID;
     AvbdBatch* b = s->b;
     if (cudaSetDevice(b->device) != cudaSuccess) return AVBD_ERR_CUDA;
+    if (!b->reserved) {
+        // pools: the body budget, a quarter as many forces and triangles, two tets per body
+        const int64_t nb = s->pool_bodies;
+        if (int r = avbd_batch_reserve(b, nb, nb / 4, 2 * nb, nb / 4, s->max_scenes)) return r;
+    }
     if (!b->grid && batch_launch_shape(b)) return AVBD_ERR_CUDA;
     // 1. admissions staged while the previous step runs
     s->arena_cur ^= 1;

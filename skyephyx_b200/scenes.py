@@ -343,6 +343,33 @@ def level_cloth(s, E=8000.0, nu=0.3, particle_mass=1.0, N=10, M=15, spacing=1.5)
     return parts
 
 
+def level_soft_spheres(s, E=8000.0, nu=0.3, particle_mass=1.0):
+    """levels.h:412-440: a makeTetSphere ball (radius 3, res 2: 149 particles,
+    576 tets) dropped from 5 m above a static ground box."""
+    s.add_body(CUBE, 1.0, 0.5, v3(0.0, -10.0, 0.0), v3(40.0, 1.0, 20.0), is_static=True)
+    radius = 3.0
+    return s.make_tet_sphere(0.0, -9.5 + radius + 5.0, 0.0, radius, 2.0, E, nu, particle_mass)
+
+
+def level_safety_net(s, E=8000.0, nu=0.3, particle_mass=1.0, count=15, spacing=0.5):
+    """levels.h:493-547: a 15x15 StVK triangle net pinned at its four corners."""
+    sx = -(count - 1) * spacing * 0.5
+    sz = -(count - 1) * spacing * 0.5
+    parts = [0] * (count * count)
+    for j in range(count):
+        for i in range(count):
+            parts[i + j * count] = s.add_particle(particle_mass, 0.5, v3(sx + i * spacing, -10.0, sz + j * spacing))
+    for c in (0, count - 1, (count - 1) * count, count * count - 1):
+        s.set_static(parts[c], True)
+    for j in range(count - 1):
+        for i in range(count - 1):
+            v00, v10 = parts[i + j * count], parts[i + 1 + j * count]
+            v01, v11 = parts[i + (j + 1) * count], parts[i + 1 + (j + 1) * count]
+            s.add_stvk_tri((v00, v10, v11), E, nu)
+            s.add_stvk_tri((v00, v11, v01), E, nu)
+    return parts
+
+
 LEVELS = {
     "pyramid": level_pyramid,
     "mass_stack": level_mass_stack,
@@ -352,4 +379,6 @@ LEVELS = {
     "neohookean_tets": level_neohookean_tets,
     "soft_beam": level_soft_beam,
     "cloth": level_cloth,
+    "soft_spheres": level_soft_spheres,
+    "safety_net": level_safety_net,
 }

@@ -164,6 +164,34 @@ class Solver:
                                                     float(particle_mass), float(friction), int(bool(pin_min_x))),
                      "make_tet_volume")
 
+    def set_color(self, body, rgb):
+        """Mesh::color of a body (read only by the instance export)."""
+        c = _f(rgb, 3)
+        check(self._lib.avbd_set_body_color(self._h, int(body), _fp(c)), "set_body_color")
+
+    def export_instances(self, dst=None):
+        """Headless pose export in the renderer's 128-byte instance layout
+        (RenderEngine.cpp:951-1000).  dst: a device pointer (int) of room for
+        num_bodies records, or None for a host array of shape (n, 32) float32
+        (model matrix 16, normal matrix 12, colour 4).  Returns (array or
+        count, first index per model, count per model)."""
+        n = self.num_bodies
+        first = (C.c_int32 * 3)()
+        count = (C.c_int32 * 3)()
+        if dst is None:
+            out = np.zeros((n, 32), np.float32)
+            k = check(self._lib.avbd_export_instances(self._h, out.ctypes.data, n, first, count), "export_instances")
+            return out[:k], list(first), list(count)
+        k = check(self._lib.avbd_export_instances(self._h, C.c_void_p(int(dst)), n, first, count),
+                  "export_instances")
+        return k, list(first), list(count)
+
+    def make_tet_sphere(self, cx, cy, cz, radius, res, E, nu, particle_mass=1.0, friction=0.5):
+        """GeometryHelpers::makeTetSphere (geometry.cpp:106-232). Returns the first particle id."""
+        return check(self._lib.avbd_make_tet_sphere(self._h, float(cx), float(cy), float(cz), float(radius),
+                                                    float(res), float(E), float(nu), float(particle_mass),
+                                                    float(friction)), "make_tet_sphere")
+
     # ---- stepping ----
     def step(self):
         """Solver::Step(); returns the status name ('ok', 'exploded', ...)."""
