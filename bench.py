@@ -507,6 +507,7 @@ def serve_run(rate, window, warmup, cap_s, budget_gb, launch=None, seed_base=0x5
     (t0, s0), (t1, s1) = marks["w0"], marks.get("w1", (elapsed, srv.stats()))
     dt = max(t1 - t0, 1e-9)
     lat = srv.latency_stats(since=warmup, until=span)
+    waits = np.array([r.admitted - r.arrival for r in srv.done if warmup <= r.arrival < span])
     final = srv.stats()
     backlog = final["pending"] + final["active"]
     out = {"offered_rate": rate, "warmup_s": warmup, "window_s": window, "requests": len(arrivals),
@@ -515,7 +516,11 @@ def serve_run(rate, window, warmup, cap_s, budget_gb, launch=None, seed_base=0x5
            "scenes_per_s": (s1["completed"] - s0["completed"]) / dt,
            "ticks_per_s": (s1["ticks"] - s0["ticks"]) / dt, "resident_dynamic_at_window_end": s1["resident_dynamic"],
            "p50_s": lat.get("p50_s"), "p99_s": lat.get("p99_s"), "latency_requests": lat.get("completed", 0),
-           "keeps_up": backlog == 0 and elapsed <= span + 5.0, "budget_gb": budget_gb, "build_s": build_s,
+           "admission_wait_p50_s": float(np.percentile(waits, 50)) if waits.size else None,
+           "admission_wait_p99_s": float(np.percentile(waits, 99)) if waits.size else None,
+           # keeping up: every request done within the cap and none waited a second for admission
+           "keeps_up": bool(backlog == 0 and waits.size and np.percentile(waits, 99) < 1.0),
+           "budget_gb": budget_gb, "build_s": build_s,
            "elapsed_s": elapsed,
            "workload": "requests: box counts log-uniform 8-2048 in a container, one hinge link and one spring per "
                        "16 boxes, U{60..600} steps"}

@@ -296,6 +296,18 @@ int32_t avbd_batch_get_state(AvbdBatch* b, int32_t scene, float* pos, float* qua
  * host buffers of max_bodies float4; a scene's bodies start at
  * avbd_batch_scene_body_offset(). */
 int32_t avbd_batch_get_all_poses(AvbdBatch* b, float* pos, float* quat_xyzw, int64_t max_bodies);
+/* Snapshot of one live scene of a batch (no reference counterpart): every
+ * device value of the scene (bodies, forces, energies, both manifold tables
+ * and contacts, incidence, colours, counters).  dst may be host or device
+ * memory of avbd_batch_scene_snapshot_bytes() bytes.  avbd_batch_scene_restore
+ * admits a snapshot as a new scene of this batch (or of another batch of the
+ * same pools layout), wherever it fits, and returns its scene id; the scene
+ * then takes the steps it would have taken without the interruption, bit for
+ * bit (serving pre-emption: snapshot, remove, restore later).  NOMEM when it
+ * does not fit now. */
+int64_t avbd_batch_scene_snapshot_bytes(AvbdBatch* b, int32_t scene);
+int32_t avbd_batch_scene_snapshot(AvbdBatch* b, int32_t scene, void* dst, int64_t bytes);
+int32_t avbd_batch_scene_restore(AvbdBatch* b, const void* src, int64_t bytes);
 /* avbd_export_instances for one scene of a batch. */
 int32_t avbd_batch_export_instances(AvbdBatch* b, int32_t scene, AvbdInstance* dst, int32_t capacity,
                                     int32_t first_per_model[3], int32_t count_per_model[3]);

@@ -81,6 +81,9 @@ SIGNATURES = [
     ("avbd_set_body_color", [_V, C.c_int32, _F], C.c_int32),
     ("avbd_export_instances", [_V, _V, C.c_int32, _I, _I], C.c_int32),
     ("avbd_batch_export_instances", [_V, C.c_int32, _V, C.c_int32, _I, _I], C.c_int32),
+    ("avbd_batch_scene_snapshot_bytes", [_V, C.c_int32], C.c_int64),
+    ("avbd_batch_scene_snapshot", [_V, C.c_int32, _V, C.c_int64], C.c_int32),
+    ("avbd_batch_scene_restore", [_V, _V, C.c_int64], C.c_int32),
     ("avbd_make_tet_sphere", [_V, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float, C.c_float,
                               C.c_float, C.c_float], C.c_int32),
     ("avbd_remove_body", [_V, C.c_int32], C.c_int32),

@@ -20,7 +20,8 @@ CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libavbd.so")
 # (object name, source, extra flags)
 UNITS = [("avbd_api", "avbd_api.cu", []), ("avbd_batch_host", "avbd_batch_host.cu", []),
-         ("avbd_server", "avbd_server.cu", []), ("avbd_host", "avbd_host.cpp", [])] + [
+         ("avbd_server", "avbd_server.cu", []), ("avbd_scene_snapshot", "avbd_scene_snapshot.cu", []),
+         ("avbd_host", "avbd_host.cpp", [])] + [
     (f"avbd_batch_v{i}", "avbd_batch_v.cu", [f"-DAVBD_BATCH_ID={i}"]) for i in range(1, 8)]
 SOURCES = sorted({u[1] for u in UNITS})
 HEADERS = ["avbd_common.cuh", "avbd_narrow.cuh", "avbd_fem.cuh", "avbd_phases.cuh", "avbd_step.cuh", "avbd_host.h",

@@ -31,6 +31,8 @@ using namespace avbd::host;
 // ===========================================================================
 namespace {
 
+constexpr int kGridMinBodies = 128;   // single-scene bodies from which the broadphase uses the grid
+
 
 __global__ void k_bp_count(const __grid_constant__ World W) {
     const SceneDesc sc = W.scenes[0];
@@ -47,16 +49,185 @@ __global__ void k_scan_cand(const __grid_constant__ World W) {
     if (threadIdx.x == 0) W.sstate[0].need_cand = total;
 }
 
-__global__ void k_bp_write(const __grid_constant__ World W, int cur) {
+__global__ void k_bp_write(const __grid_constant__ World W, int cur, int all_pairs) {
     const SceneDesc sc = W.scenes[0];
-    for (int b = sc.body0 + blockIdx.x * blockDim.x + threadIdx.x; b < sc.body0 + sc.nbody;
-         b += gridDim.x * blockDim.x)
-        broadphase_body(W, sc, b, W.cpair[cur] + sc.cand0 + W.cand_off[b], W.cand_cnt[b]);
+    if (all_pairs)
+        for (int b = sc.body0 + blockIdx.x * blockDim.x + threadIdx.x; b < sc.body0 + sc.nbody;
+             b += gridDim.x * blockDim.x)
+            broadphase_body(W, sc, b, W.cpair[cur] + sc.cand0 + W.cand_off[b], W.cand_cnt[b]);
     if (blockIdx.x == 0 && threadIdx.x == 0) {
         W.sstate[0].kused[cur] = 0;
         W.sstate[0].need_k = 0;
         W.sstate[0].nlive[cur] = 0;
         W.sstate[0].nmatched = 0;
+    }
+}
+
+// ---------------------------------------------------------------------------
+// Uniform-grid broadphase of the single scene, grid-wide: the batched path's
+// grid (broadphase_grid: cells 2R wide, R the largest radius of the small
+// bodies, the big bodies' all-pairs rows beside it, candidate lists sorted by
+// partner) built by a counting sort over the whole GPU instead of one CTA.
+// Same candidate set and order as the reference's all-pairs loop
+// (solver.cpp:233-256).  Scratch: W.bcur (cell starts), W.cntB (cell items),
+// W.cand_off (each body's rank in its cell, before it takes the offsets).
+// ---------------------------------------------------------------------------
+struct GridState {
+    int red[8];               // order-preserving float bits: min xyz, max xyz, max radius, min radius
+    int nbig;
+    int big[kGridMaxBig];
+    GridDims g;
+    int ncell;
+    int valid;                // 0: use the all-pairs loop this step
+    float rbig;
+};
+
+__global__ void k_grid_reset(GridState* gs) {
+    if (threadIdx.x != 0) return;
+    for (int a = 0; a < 3; ++a) { gs->red[a] = ord_float(INFINITY); gs->red[3 + a] = ord_float(-INFINITY); }
+    gs->red[6] = ord_float(0.f);
+    gs->red[7] = ord_float(INFINITY);
+    gs->nbig = 0;
+}
+
+__global__ void k_grid_rmin(const __grid_constant__ World W, GridState* gs) {
+    const SceneDesc sc = W.scenes[0];
+    float rmin = INFINITY;
+    for (int li = blockIdx.x * blockDim.x + threadIdx.x; li < sc.nbody; li += gridDim.x * blockDim.x) {
+        const float4 p = body_sphere(W, sc, nullptr, li);
+        if (!isinf(p.w)) rmin = fminf(rmin, p.w);
+    }
+    for (int o = 16; o > 0; o >>= 1) rmin = fminf(rmin, __shfl_xor_sync(0xffffffffu, rmin, o));
+    if ((threadIdx.x & 31) == 0) atomicMin(&gs->red[7], ord_float(rmin));
+}
+
+__global__ void k_grid_extent(const __grid_constant__ World W, GridState* gs) {
+    const SceneDesc sc = W.scenes[0];
+    const float rbig = 8.f * unord_float(gs->red[7]);
+    float mn[3] = {INFINITY, INFINITY, INFINITY}, mx[3] = {-INFINITY, -INFINITY, -INFINITY}, mr = 0.f;
+    for (int li = blockIdx.x * blockDim.x + threadIdx.x; li < sc.nbody; li += gridDim.x * blockDim.x) {
+        const float4 p = body_sphere(W, sc, nullptr, li);
+        if (isinf(p.w)) continue;
+        if (p.w > rbig) {
+            const int k = atomicAdd(&gs->nbig, 1);
+            if (k < kGridMaxBig) gs->big[k] = li;
+            continue;
+        }
+        mn[0] = fminf(mn[0], p.x); mn[1] = fminf(mn[1], p.y); mn[2] = fminf(mn[2], p.z);
+        mx[0] = fmaxf(mx[0], p.x); mx[1] = fmaxf(mx[1], p.y); mx[2] = fmaxf(mx[2], p.z);
+        mr = fmaxf(mr, p.w);
+    }
+    for (int o = 16; o > 0; o >>= 1) {
+        for (int a = 0; a < 3; ++a) {
+            mn[a] = fminf(mn[a], __shfl_xor_sync(0xffffffffu, mn[a], o));
+            mx[a] = fmaxf(mx[a], __shfl_xor_sync(0xffffffffu, mx[a], o));
+        }
+        mr = fmaxf(mr, __shfl_xor_sync(0xffffffffu, mr, o));
+    }
+    if ((threadIdx.x & 31) == 0) {
+        for (int a = 0; a < 3; ++a) {
+            atomicMin(&gs->red[a], ord_float(mn[a]));
+            atomicMax(&gs->red[3 + a], ord_float(mx[a]));
+        }
+        atomicMax(&gs->red[6], ord_float(mr));
+    }
+}
+
+// Grid dimensions (as broadphase_grid chooses them: at most nbody / 2 cells).
+__global__ void k_grid_setup(const __grid_constant__ World W, GridState* gs) {
+    if (threadIdx.x != 0) return;
+    const SceneDesc sc = W.scenes[0];
+    GridDims g;
+    g.minx = unord_float(gs->red[0]); g.miny = unord_float(gs->red[1]); g.minz = unord_float(gs->red[2]);
+    const float ex = unord_float(gs->red[3]) - g.minx, ey = unord_float(gs->red[4]) - g.miny,
+                ez = unord_float(gs->red[5]) - g.minz;
+    const float R = unord_float(gs->red[6]);
+    const float rbig = 8.f * unord_float(gs->red[7]);
+    gs->rbig = rbig;
+    gs->valid = 0;
+    if (!(ex >= 0.f && ey >= 0.f && ez >= 0.f) || !(ex < 1e30f && ey < 1e30f && ez < 1e30f) || !(R < 1e30f) ||
+        !(rbig < 1e30f) || gs->nbig > kGridMaxBig)
+        return;
+    const int maxcell = max(1, sc.nbody / 2);
+    float h = fmaxf(2.f * R * 1.0001f, 1e-6f);
+    for (int it = 0; it < 64; ++it) {
+        g.nx = (int)(ex / h) + 1; g.ny = (int)(ey / h) + 1; g.nz = (int)(ez / h) + 1;
+        if ((long long)g.nx * g.ny * g.nz <= maxcell) break;
+        h *= 1.25f;
+    }
+    if ((long long)g.nx * g.ny * g.nz > maxcell) return;
+    g.inv_h = 1.f / h;
+    gs->g = g;
+    gs->ncell = g.nx * g.ny * g.nz;
+    gs->valid = 1;
+}
+
+__global__ void k_grid_clear(const __grid_constant__ World W, const GridState* gs) {
+    if (!gs->valid) return;
+    int* cstart = W.bcur + W.scenes[0].body0;
+    for (int c = blockIdx.x * blockDim.x + threadIdx.x; c <= gs->ncell; c += gridDim.x * blockDim.x) cstart[c] = 0;
+}
+
+__global__ void k_grid_rank(const __grid_constant__ World W, const GridState* gs) {
+    if (!gs->valid) return;
+    const SceneDesc sc = W.scenes[0];
+    int* cstart = W.bcur + sc.body0;
+    for (int li = blockIdx.x * blockDim.x + threadIdx.x; li < sc.nbody; li += gridDim.x * blockDim.x) {
+        const float4 p = body_sphere(W, sc, nullptr, li);
+        if (isinf(p.w) || p.w > gs->rbig) continue;
+        W.cand_off[sc.body0 + li] = atomicAdd(&cstart[gs->g.cell(p)], 1);
+    }
+}
+
+__global__ void k_grid_scan(const __grid_constant__ World W, const GridState* gs) {
+    __shared__ TeamShared s_team;
+    if (!gs->valid) return;
+    const Team T = Team::cta(&s_team, nullptr, 0);
+    int* cstart = W.bcur + W.scenes[0].body0;
+    const int total = block_exclusive_scan(T, cstart, cstart, gs->ncell);
+    if (threadIdx.x == 0) cstart[gs->ncell] = total;
+}
+
+__global__ void k_grid_scatter(const __grid_constant__ World W, const GridState* gs) {
+    if (!gs->valid) return;
+    const SceneDesc sc = W.scenes[0];
+    const int* cstart = W.bcur + sc.body0;
+    for (int li = blockIdx.x * blockDim.x + threadIdx.x; li < sc.nbody; li += gridDim.x * blockDim.x) {
+        const float4 p = body_sphere(W, sc, nullptr, li);
+        if (isinf(p.w) || p.w > gs->rbig) continue;
+        W.cntB[sc.body0 + cstart[gs->g.cell(p)] + W.cand_off[sc.body0 + li]] = li;
+    }
+}
+
+__device__ __forceinline__ GridCells grid_cells(const World& W, const SceneDesc& sc, const GridState* gs) {
+    GridCells gc;
+    gc.cstart = W.bcur + sc.body0;
+    gc.items16 = nullptr;
+    gc.items32 = W.cntB + sc.body0;
+    gc.big = gs->big;
+    gc.nbig = gs->nbig;
+    gc.rbig = gs->rbig;
+    return gc;
+}
+
+// Candidates per body (count pass) or their pairs (write pass), from the
+// grid when it is valid this step, else from the all-pairs loop.
+template <bool WRITE>
+__global__ void k_bp_grid(const __grid_constant__ World W, const GridState* gs, int cur) {
+    const SceneDesc sc = W.scenes[0];
+    const bool grid = gs->valid != 0;
+    const GridDims g = gs->g;
+    const GridCells gc = grid_cells(W, sc, gs);
+    for (int li = blockIdx.x * blockDim.x + threadIdx.x; li < sc.nbody; li += gridDim.x * blockDim.x) {
+        const int b = sc.body0 + li;
+        if (!WRITE) {
+            W.cand_cnt[b] = grid ? grid_candidates<false>(W, sc, nullptr, g, gc, li, nullptr)
+                                 : broadphase_body(W, sc, b, nullptr, 0);
+        } else {
+            int2* out = W.cpair[cur] + sc.cand0 + W.cand_off[b];
+            if (grid) grid_candidates<true>(W, sc, nullptr, g, gc, li, out);
+            else broadphase_body(W, sc, b, out, W.cand_cnt[b]);
+        }
     }
 }
 
@@ -362,6 +533,9 @@ int upload(AvbdWorld* w) {
     upload_scene(P, w->h, static_incidence(w->h, reg), reg, g, 0, w->descs[0], sink);
     if (cudaGetLastError() != cudaSuccess) return AVBD_ERR_CUDA;
     P.W.P = to_params(w->params);
+    GridState* gs = nullptr;
+    if (P.alloc(gs, 1) != cudaSuccess) return AVBD_ERR_NOMEM;
+    w->grid = gs;
     w->uploaded = true;
     return 0;
 }
@@ -414,13 +588,29 @@ int world_step(AvbdWorld* w) {
     const int old = w->st.cur, cur = old ^ 1;
     const int old_count = w->st.ncand[old];
     cudaEventRecord(w->ev[0], s);
-    // ---- broadphase ----
-    k_bp_count<<<blocks_for(d.nbody), kThreads, 0, s>>>(P.W);
+    // ---- broadphase: uniform grid from kGridMinBodies bodies, else all pairs ----
+    const bool use_grid = d.nbody >= kGridMinBodies;
+    GridState* gs = static_cast<GridState*>(w->grid);
+    if (use_grid) {
+        const int nb = blocks_for(d.nbody);
+        k_grid_reset<<<1, 32, 0, s>>>(gs);
+        k_grid_rmin<<<nb, kThreads, 0, s>>>(P.W, gs);
+        k_grid_extent<<<nb, kThreads, 0, s>>>(P.W, gs);
+        k_grid_setup<<<1, 32, 0, s>>>(P.W, gs);
+        k_grid_clear<<<nb, kThreads, 0, s>>>(P.W, gs);
+        k_grid_rank<<<nb, kThreads, 0, s>>>(P.W, gs);
+        k_grid_scan<<<1, 1024, 0, s>>>(P.W, gs);
+        k_grid_scatter<<<nb, kThreads, 0, s>>>(P.W, gs);
+        k_bp_grid<false><<<nb, kThreads, 0, s>>>(P.W, gs, cur);
+    } else {
+        k_bp_count<<<blocks_for(d.nbody), kThreads, 0, s>>>(P.W);
+    }
     k_scan_cand<<<1, 1024, 0, s>>>(P.W);
     if ((r = sync_state(w))) return r;
     const int ncand = w->st.need_cand;
     if ((r = ensure_caps(w, ncand, 0))) return r;
-    k_bp_write<<<blocks_for(d.nbody), kThreads, 0, s>>>(P.W, cur);
+    if (use_grid) k_bp_grid<true><<<blocks_for(d.nbody), kThreads, 0, s>>>(P.W, gs, cur);
+    k_bp_write<<<blocks_for(d.nbody), kThreads, 0, s>>>(P.W, cur, use_grid ? 0 : 1);
     cudaEventRecord(w->ev[1], s);
     // ---- narrowphase + manifold warm start (re-run after growing the contact pool) ----
     for (int attempt = 0; attempt < 4; ++attempt) {

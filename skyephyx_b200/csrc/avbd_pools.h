@@ -563,6 +563,7 @@ struct AvbdWorld {
     int ncolours = 0;
     std::vector<int> col_start;
     avbd::SceneState st{};   // host mirror of the scene counters after the last step
+    void* grid = nullptr;     // device scratch of the grid broadphase (avbd_api.cu)
 };
 
 // ===========================================================================

@@ -403,6 +403,18 @@ class Batch:
               "batch_get_state")
         return pos, quat, vel, omega
 
+    def snapshot_scene(self, scene: int) -> np.ndarray:
+        """Device state of one live scene as a host byte array (avbd_batch_scene_snapshot)."""
+        n = check(self._lib.avbd_batch_scene_snapshot_bytes(self._h, int(scene)), "scene_snapshot_bytes")
+        buf = np.empty(n, np.uint8)
+        check(self._lib.avbd_batch_scene_snapshot(self._h, int(scene), buf.ctypes.data, n), "scene_snapshot")
+        return buf
+
+    def restore_scene(self, buf: np.ndarray) -> int:
+        """Admits a scene snapshot wherever it fits; returns its new scene id."""
+        buf = np.ascontiguousarray(buf, dtype=np.uint8)
+        return check(self._lib.avbd_batch_scene_restore(self._h, buf.ctypes.data, buf.size), "scene_restore")
+
     def set_groups(self, rigid_group=4, fem_group=8):
         """Lanes per body in the primal sweep for rigid and FEM scenes (before the
         first step); fem_group may be GROUP_FLAT (one lane per particle-tet term)."""

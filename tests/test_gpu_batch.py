@@ -175,24 +175,27 @@ def test_grid_broadphase_matches_oracle(oracle_mod):
 
 
 def test_grid_broadphase_equals_all_pairs_over_time():
-    """A collapsing pile and a settling stack, 30 steps: the batch (grid
-    broadphase) and the single-scene path (all-pairs broadphase kernels), both
-    with one lane per body, agree bit for bit."""
+    """A collapsing pile and a settling stack, 30 steps, one lane per body:
+    the batch with its in-CTA grid broadphase, the batch with the all-pairs
+    loop, and the single-scene path with its grid-wide grid agree bit for
+    bit."""
     from skyephyx_b200 import Batch, Solver
     for build in GRID_BUILDERS[1:3]:
         w = Solver()
         w.set_group(1)
         build(w)
-        b = Batch()
-        b.set_groups(1, 4)
-        b.add_scene(staged(build))
         for _ in range(30):
             assert w.step() == "ok"
-        assert b.step(30) == "ok" and b.scene_status(0) == "ok"
-        pw, qw = w.get_state()[:2]
-        pb, qb = b.get_state(0)[:2]
-        assert np.array_equal(pw.view(np.uint32), pb.view(np.uint32))
-        assert np.array_equal(qw.view(np.uint32), qb.view(np.uint32))
+        results = [w.get_state()[:2]]
+        for grid_min in (128, 0):
+            b = Batch()
+            b.set_groups(1, 4)
+            b.set_grid_broadphase(grid_min)
+            b.add_scene(staged(build))
+            assert b.step(30) == "ok" and b.scene_status(0) == "ok"
+            results.append(b.get_state(0)[:2])
+        for other in results[1:]:
+            assert same(results[0], other)
 
 
 def test_batch_grows_full_tables():
@@ -341,3 +344,40 @@ def test_headline_launch_matches_oracle(oracle_mod):
         assert info["contacts"] == points, f"{sp}: {info['contacts']} contact points vs {points}"
         assert info["colours"] == o.colours()[1], f"{sp}: colours"
     print(f"headline slice: {len(specs)} scenes, max |dpos| {worst_p:.3g} m, max |drot| {worst_r:.3g} rad")
+
+
+def test_scene_snapshot_restores_elsewhere_and_replays():
+    """Pre-emption of scenes inside a batch: after 4 steps each scene is
+    snapshotted and removed, a newcomer takes the freed space, the snapshots
+    come back (in reverse order, so at other pool offsets) and 5 more steps
+    follow.  Every restored scene ends bitwise where it ends running 9 steps
+    alone (the flat FEM sweep's tet-term records and the grid broadphase
+    included)."""
+    from skyephyx_b200 import Batch, GROUP_FLAT
+    builders = [
+        lambda s: scenes.rigid_pile(s, 300, scenes.rng_for(4, 31), stack=False),
+        lambda s: scenes.fem_scene(s, 700, scenes.rng_for(4, 32)),
+        scenes.level_joint_playground,
+        scenes.level_cloth,
+    ]
+    b = Batch()
+    b.set_groups(1, GROUP_FLAT)
+    b.reserve(bodies=20000, forces=2000, tets=20000, tris=2000, scenes=16)
+    keep = [staged(f) for f in builders]
+    ids = [b.add_scene(w) for w in keep]
+    assert b.step(4) == "ok"
+    snaps = [b.snapshot_scene(i) for i in ids]
+    for i in ids:
+        b.remove_scene(i)
+    filler = b.add_scene(staged(lambda s: scenes.pyramid_wall(s, rows=7)))
+    back = {k: b.restore_scene(snaps[k]) for k in reversed(range(len(builders)))}
+    assert b.step(5) == "ok"
+    for k, f in enumerate(builders):
+        assert b.scene_status(back[k]) == "ok"
+        alone = Batch()
+        alone.set_groups(1, GROUP_FLAT)
+        alone.add_scene(staged(f))
+        assert alone.step(9) == "ok"
+        assert same(b.get_state(back[k])[:2], alone.get_state(0)[:2]), f"scene {k}"
+        assert b.scene_info(back[k])["steps"] == 9
+    assert b.scene_status(filler) == "ok"
