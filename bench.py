@@ -262,6 +262,28 @@ def plain_configs(steps=5):
     return out
 
 
+def plain_one(key, steps, warmup):
+    """One configuration on the single-scene GPU path: wall ms per step and
+    the per-phase device times of the last step (avbd_get_timings)."""
+    from skyephyx_b200 import Solver
+    names = {"C1": "C1", "C2": "C2 Neo-Hookean", "C2-stvk": "C2 StVK", "C3": "C3"}
+    name = next(n for n in CONFIG_SCENES if n.startswith(names[key]))
+    build, iters = CONFIG_SCENES[name]
+    s = Solver(iterations=iters)
+    build(s)
+    for _ in range(warmup):
+        s.step()
+    t0 = time.perf_counter()
+    for _ in range(steps):
+        status = s.step()
+    ms = (time.perf_counter() - t0) * 1e3 / steps
+    out = {"config": name, "iterations": iters, "status": status, "ms_per_step": ms,
+           "dynamic_bodies": s.num_dynamic, "body_iters_per_s": s.num_dynamic * iters / (ms / 1e3),
+           "phases_ms": s.timings()}
+    s.close()
+    return out
+
+
 def headline_parity(launch, n_sample=256):
     """One step of a slice of the 4,096-scene mix (every 16th scene plus the
     eight largest rigid and eight largest FEM scenes) under the benchmark's
@@ -515,6 +537,7 @@ def serve_run(rate, window, warmup, cap_s, budget_gb, launch=None, seed_base=0x5
            "body_iters_per_s": (s1["body_iterations"] - s0["body_iterations"]) / dt,
            "scenes_per_s": (s1["completed"] - s0["completed"]) / dt,
            "ticks_per_s": (s1["ticks"] - s0["ticks"]) / dt, "resident_dynamic_at_window_end": s1["resident_dynamic"],
+           "gpu_busy_fraction": (s1["device_us"] - s0["device_us"]) / 1e6 / dt,
            "p50_s": lat.get("p50_s"), "p99_s": lat.get("p99_s"), "latency_requests": lat.get("completed", 0),
            "admission_wait_p50_s": float(np.percentile(waits, 50)) if waits.size else None,
            "admission_wait_p99_s": float(np.percentile(waits, 99)) if waits.size else None,
@@ -530,12 +553,39 @@ def serve_run(rate, window, warmup, cap_s, budget_gb, launch=None, seed_base=0x5
     return out
 
 
+def served_mix_batched(n, launch, seed_base=0x5EED0005, steps=5):
+    """The first n requests' scenes of the served workload stepped as one
+    batch (all resident, no admission): the batched rate of the scene
+    composition the server runs."""
+    from skyephyx_b200 import Batch, Solver, autotune, scenes
+    sizes = serve_sizes(n, seed_base + 2)
+    b = Batch(iterations=ITERS)
+    keep = []
+    dyn = 0
+    for i, size in enumerate(sizes):
+        s = Solver(iterations=ITERS)
+        scenes.served_scene(s, size, seed_base + i)
+        keep.append(s)
+        b.add_scene(s)
+        dyn += s.num_dynamic
+    if launch:
+        autotune.apply(b, launch)
+    b.step(3)
+    b.step(steps)
+    ms = b.last_ms / steps
+    b.close()
+    return {"scenes": n, "dynamic_bodies": dyn, "ms_per_step": ms, "body_iters_per_s": dyn * ITERS / (ms / 1e3)}
+
+
 def serve_bench(rate, window, warmup, budget_gb, launch=None):
     """The served configuration at the offered rate, then at 0.8x the rate the
     server sustained there (completions per second while saturated), where
     latency is queueing-free."""
     hot = serve_run(rate, window, warmup, 20.0, budget_gb, launch)
     out = {"offered": hot}
+    same = served_mix_batched(8192, launch)
+    out["batched_same_composition"] = same
+    out["served_over_batched_same_composition"] = hot["body_iters_per_s"] / same["body_iters_per_s"]
     sustained = hot["scenes_per_s"]
     if not hot["keeps_up"] and sustained > 0:
         out["max_sustainable_rate"] = sustained
@@ -598,6 +648,9 @@ def main():
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-configs", action="store_true")
     ap.add_argument("--serve-only", action="store_true")
+    ap.add_argument("--plain-config", default=None,
+                    help="only the single-scene GPU path of one configuration (C1, C2, C2-stvk, C3): "
+                         "wall time per step and per-phase device times")
     ap.add_argument("--serve-rate", type=float, default=2000.0)
     ap.add_argument("--serve-window", type=float, default=10.0)
     ap.add_argument("--serve-warmup", type=float, default=1.0)
@@ -607,6 +660,10 @@ def main():
 
     if args.impl == "reference":
         reference_arm(args)
+        return
+
+    if args.plain_config:
+        print(json.dumps(plain_one(args.plain_config, args.steps, args.warmup)))
         return
 
     if args.serve_only:

@@ -329,6 +329,13 @@ int32_t avbd_batch_set_team_work(AvbdBatch* b, int32_t units_per_lane);
 /* The same threshold for scenes with tets (their per-colour finish leaves
  * most of a team idle, which a second scene on the CTA can use). Default 0. */
 int32_t avbd_batch_set_fem_team_work(AvbdBatch* b, int32_t units_per_lane);
+/* Thread-block clusters of cluster_size (1, 2, 4 or 8) CTAs: scenes of at
+ * least min_units bodies + tets are each run by a whole cluster (ranks over
+ * its CTAs, shared scalars in distributed shared memory, cluster barriers)
+ * before the CTAs take the smaller scenes one team each.  A scene's results
+ * do not depend on it (bitwise).  1 (the default) is a plain launch.  Before
+ * the first step (autotuner knob). */
+int32_t avbd_batch_set_cluster(AvbdBatch* b, int32_t cluster_size, int32_t min_units);
 /* Scenes of at least min_bodies bodies find broadphase candidates with a
  * uniform grid (the same candidate set and order as the reference's all-pairs
  * loop, which smaller scenes keep); 0 = all-pairs everywhere.  Default 128. */
@@ -381,6 +388,7 @@ typedef struct AvbdServerStats {
     int64_t body_iterations;   /* dynamic bodies x iterations over the steps launched */
     int64_t uploaded_bytes;    /* host-to-device bytes of admitted scenes */
     int64_t pending, active, resident_dynamic;
+    int64_t device_us;         /* device time of the steps completed, microseconds */
 } AvbdServerStats;
 
 /* Pools for `bodies` bodies (a quarter as many joints+springs and

@@ -41,7 +41,8 @@ class AvbdServedRequest(C.Structure):
 
 class AvbdServerStats(C.Structure):
     _fields_ = [(n, C.c_int64) for n in ("submitted", "admitted", "completed", "ticks", "body_iterations",
-                                         "uploaded_bytes", "pending", "active", "resident_dynamic")]
+                                         "uploaded_bytes", "pending", "active", "resident_dynamic",
+                                         "device_us")]
 
 
 class AvbdTimings(C.Structure):
@@ -129,6 +130,7 @@ SIGNATURES = [
     ("avbd_batch_set_team_work", [_V, C.c_int32], C.c_int32),
     ("avbd_batch_set_fem_team_work", [_V, C.c_int32], C.c_int32),
     ("avbd_batch_set_grid_broadphase", [_V, C.c_int32], C.c_int32),
+    ("avbd_batch_set_cluster", [_V, C.c_int32, C.c_int32], C.c_int32),
     ("avbd_batch_last_ms", [_V], C.c_float),
     ("avbd_batch_set_groups", [_V, C.c_int32, C.c_int32], C.c_int32),
     ("avbd_set_group", [_V, C.c_int32], C.c_int32),

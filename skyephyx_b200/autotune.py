@@ -82,6 +82,8 @@ def apply(batch, cfg: dict) -> None:
     batch.set_team_work(cfg.get("team_work", 0))
     batch.set_fem_team_work(cfg.get("fem_team_work", 0))
     batch.set_grid_broadphase(cfg.get("grid_min", 128))
+    if cfg.get("cluster", 1) > 1:
+        batch.set_cluster(cfg["cluster"], cfg.get("cluster_min", 0))
 
 
 def candidates(space=SPACE):

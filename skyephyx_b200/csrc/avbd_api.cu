@@ -210,8 +210,50 @@ __device__ __forceinline__ GridCells grid_cells(const World& W, const SceneDesc&
     return gc;
 }
 
+// The big bodies' all-pairs rows (a floor or wall overlaps most of the
+// scene): one block per big body, each chunk of partners tested by the
+// block's threads and its candidates placed by a block-wide prefix count, so
+// the row comes out in partner order without one thread walking it.
+template <bool WRITE>
+__global__ void __launch_bounds__(1024) k_bp_big(const __grid_constant__ World W, const GridState* gs, int cur) {
+    __shared__ int s_warp[32];
+    __shared__ int s_total;
+    if (!gs->valid) return;
+    const SceneDesc sc = W.scenes[0];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5, nwarps = blockDim.x >> 5;
+    for (int k = blockIdx.x; k < gs->nbig; k += gridDim.x) {
+        const int li = gs->big[k];
+        const int b = sc.body0 + li;
+        const float4 pi = body_sphere(W, sc, nullptr, li);
+        int2* out = WRITE ? W.cpair[cur] + sc.cand0 + W.cand_off[b] : nullptr;
+        const int cap = WRITE ? W.cand_cnt[b] : 0;
+        if (threadIdx.x == 0) s_total = 0;
+        __syncthreads();
+        for (int c0 = li + 1; c0 < sc.nbody; c0 += blockDim.x) {
+            const int lj = c0 + threadIdx.x;
+            const bool hit = !isinf(pi.w) && lj < sc.nbody && grid_pair(W, sc, nullptr, pi, li, lj);
+            const unsigned bal = __ballot_sync(0xffffffffu, hit);
+            if (lane == 0) s_warp[warp] = __popc(bal);
+            __syncthreads();
+            int before = s_total, chunk = 0;
+            for (int w = 0; w < nwarps; ++w) {
+                if (w < warp) before += s_warp[w];
+                chunk += s_warp[w];
+            }
+            const int at = before + __popc(bal & ((1u << lane) - 1u));
+            if (WRITE && hit && at < cap) out[at] = make_int2(b, sc.body0 + lj);
+            __syncthreads();
+            if (threadIdx.x == 0) s_total += chunk;
+            __syncthreads();
+        }
+        if (!WRITE && threadIdx.x == 0) W.cand_cnt[b] = s_total;
+        __syncthreads();
+    }
+}
+
 // Candidates per body (count pass) or their pairs (write pass), from the
-// grid when it is valid this step, else from the all-pairs loop.
+// grid when it is valid this step, else from the all-pairs loop.  The big
+// bodies' rows come from k_bp_big.
 template <bool WRITE>
 __global__ void k_bp_grid(const __grid_constant__ World W, const GridState* gs, int cur) {
     const SceneDesc sc = W.scenes[0];
@@ -220,6 +262,7 @@ __global__ void k_bp_grid(const __grid_constant__ World W, const GridState* gs, 
     const GridCells gc = grid_cells(W, sc, gs);
     for (int li = blockIdx.x * blockDim.x + threadIdx.x; li < sc.nbody; li += gridDim.x * blockDim.x) {
         const int b = sc.body0 + li;
+        if (grid && !(W.flags[b] & kBodyRemoved) && W.scale[b].w > gc.rbig) continue;   // k_bp_big
         if (!WRITE) {
             W.cand_cnt[b] = grid ? grid_candidates<false>(W, sc, nullptr, g, gc, li, nullptr)
                                  : broadphase_body(W, sc, b, nullptr, 0);
@@ -602,6 +645,7 @@ int world_step(AvbdWorld* w) {
         k_grid_scan<<<1, 1024, 0, s>>>(P.W, gs);
         k_grid_scatter<<<nb, kThreads, 0, s>>>(P.W, gs);
         k_bp_grid<false><<<nb, kThreads, 0, s>>>(P.W, gs, cur);
+        k_bp_big<false><<<kGridMaxBig, 1024, 0, s>>>(P.W, gs, cur);
     } else {
         k_bp_count<<<blocks_for(d.nbody), kThreads, 0, s>>>(P.W);
     }
@@ -609,7 +653,10 @@ int world_step(AvbdWorld* w) {
     if ((r = sync_state(w))) return r;
     const int ncand = w->st.need_cand;
     if ((r = ensure_caps(w, ncand, 0))) return r;
-    if (use_grid) k_bp_grid<true><<<blocks_for(d.nbody), kThreads, 0, s>>>(P.W, gs, cur);
+    if (use_grid) {
+        k_bp_grid<true><<<blocks_for(d.nbody), kThreads, 0, s>>>(P.W, gs, cur);
+        k_bp_big<true><<<kGridMaxBig, 1024, 0, s>>>(P.W, gs, cur);
+    }
     k_bp_write<<<blocks_for(d.nbody), kThreads, 0, s>>>(P.W, cur, use_grid ? 0 : 1);
     cudaEventRecord(w->ev[1], s);
     // ---- narrowphase + manifold warm start (re-run after growing the contact pool) ----
@@ -642,6 +689,14 @@ int world_step(AvbdWorld* w) {
     if (w->st.status != kStatusOk) return w->st.status == kStatusTimeout ? AVBD_STATUS_TIMEOUT : AVBD_STATUS_CAPACITY;
     const int ncol = w->st.ncolours;
     const int nlive = w->st.nlive[cur];
+    // Lanes per body: fixed by avbd_set_group, else by the scene kind and,
+    // for scenes with energies, by this step's incidence entries per body
+    // (a 0.05 m tet block's particles carry about 90: 32 lanes share them).
+    int group = d.group;
+    if (w->group == 0 && (w->h.ntet() > 0 || w->h.ntri() > 0) && d.nbody > 0) {
+        const int per_body = (w->st.ninc + d.nbody - 1) / d.nbody;
+        group = per_body > 48 ? 32 : per_body > 24 ? 16 : 8;
+    }
     w->ncolours = ncol;
     w->col_start.resize(ncol + 1);
     cudaMemcpyAsync(w->col_start.data(), P.W.col_start, (ncol + 1) * sizeof(int), cudaMemcpyDeviceToHost, s);
@@ -656,7 +711,7 @@ int world_step(AvbdWorld* w) {
     for (int it = 0; it < w->params.num_iterations; ++it) {
         for (int c = 0; c < ncol; ++c) {
             const int n = w->col_start[c + 1] - w->col_start[c];
-            if (n > 0) launch_primal(d.group, P.W, cur, w->col_start[c], n, alpha, 0, s);
+            if (n > 0) launch_primal(group, P.W, cur, w->col_start[c], n, alpha, 0, s);
         }
         const int last = it == w->params.num_iterations - 1;
         if (d.nforce + nlive > 0)
@@ -687,7 +742,7 @@ int world_step(AvbdWorld* w) {
     if (w->params.post_stabilization) {
         for (int c = 0; c < ncol; ++c) {
             const int n = w->col_start[c + 1] - w->col_start[c];
-            if (n > 0) launch_primal(d.group, P.W, cur, w->col_start[c], n, 0.f, 1, s);
+            if (n > 0) launch_primal(group, P.W, cur, w->col_start[c], n, 0.f, 1, s);
         }
     }
     cudaEventRecord(w->ev[7], s);

@@ -80,13 +80,14 @@ int batch_reserve(AvbdBatch* b, int64_t bodies, int64_t forces, int64_t tets, in
     if (b->d_fix_order) cudaFree(b->d_fix_order);
     if (b->d_fix_n) cudaFree(b->d_fix_n);
     if (cudaMalloc(&b->d_order, std::max<int64_t>(nscenes, 1) * sizeof(int)) != cudaSuccess ||
-        cudaMalloc(&b->d_nlive, sizeof(int)) != cudaSuccess || cudaMalloc(&b->d_queue, sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&b->d_nlive, 2 * sizeof(int)) != cudaSuccess ||
+        cudaMalloc(&b->d_queue, 2 * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&b->d_fail, sizeof(int)) != cudaSuccess ||
         cudaMalloc(&b->d_fix_order, std::max<int64_t>(nscenes, 1) * sizeof(int)) != cudaSuccess ||
-        cudaMalloc(&b->d_fix_n, sizeof(int)) != cudaSuccess)
+        cudaMalloc(&b->d_fix_n, 2 * sizeof(int)) != cudaSuccess)
         return AVBD_ERR_NOMEM;
     cudaMemset(b->d_fail, 0, sizeof(int));
-    cudaMemset(b->d_nlive, 0, sizeof(int));
+    cudaMemset(b->d_nlive, 0, 2 * sizeof(int));
     b->reserved = true;
     b->order_dirty = true;
     batch_drop_graph(b);
@@ -140,11 +141,43 @@ void batch_sync_order(AvbdBatch* b) {
         return (a.nbody + a.ntet) > (c.nbody + c.ntet);
     });
     b->nlive = (int)order.size();
+    const int counts[2] = {b->nlive, cluster_scenes(b, order)};
     if (!order.empty())
         cudaMemcpyAsync(b->d_order, order.data(), order.size() * sizeof(int), cudaMemcpyHostToDevice, b->stream);
-    cudaMemcpyAsync(b->d_nlive, &b->nlive, sizeof(int), cudaMemcpyHostToDevice, b->stream);
+    cudaMemcpyAsync(b->d_nlive, counts, sizeof(counts), cudaMemcpyHostToDevice, b->stream);
     cudaStreamSynchronize(b->stream);
     b->order_dirty = false;
+}
+
+int cluster_scenes(const AvbdBatch* b, const std::vector<int>& order) {
+    if (b->cluster < 2) return 0;
+    int n = 0;
+    for (int slot : order) {
+        const SceneDesc& d = b->descs[slot];
+        if (d.nbody + d.ntet < b->cluster_min) break;   // the order is by size, largest first
+        ++n;
+    }
+    return n;
+}
+
+cudaError_t launch_batch_kernel(AvbdBatch* b, const World& W, const int* order, const int* nlive, int* queue) {
+    cudaLaunchConfig_t cfg = {};
+    cfg.gridDim = dim3(b->grid);
+    cfg.blockDim = dim3(b->threads);
+    cfg.dynamicSmemBytes = (size_t)b->stage * sizeof(float4);
+    cfg.stream = b->stream;
+    cudaLaunchAttribute attr[1];
+    if (b->cluster > 1) {
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = (unsigned)b->cluster;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+    }
+    World w = W;
+    void* args[] = {&w, &order, &nlive, &queue};
+    return cudaLaunchKernelExC(&cfg, (const void*)kBatchVariants[b->variant].fn, args);
 }
 
 // First step without an explicit reservation: pools sized to the staged scenes.
@@ -225,6 +258,29 @@ int batch_launch_shape(AvbdBatch* b) {
     b->stage = stage;
     b->ctas_per_sm = per_sm;
     b->grid = sms * per_sm;
+    if (b->cluster > 1) {
+        // as many whole clusters as can be resident at once; a cluster team has at most 1024 threads
+        if (b->cluster * threads > 1024) b->cluster = std::max(1, 1024 / threads);
+        cudaLaunchConfig_t cfg = {};
+        cfg.gridDim = dim3(b->grid);
+        cfg.blockDim = dim3(threads);
+        cfg.dynamicSmemBytes = smem;
+        cudaLaunchAttribute attr[1];
+        attr[0].id = cudaLaunchAttributeClusterDimension;
+        attr[0].val.clusterDim.x = (unsigned)b->cluster;
+        attr[0].val.clusterDim.y = 1;
+        attr[0].val.clusterDim.z = 1;
+        cfg.attrs = attr;
+        cfg.numAttrs = 1;
+        int nclusters = 0;
+        if (b->cluster > 1 && cudaOccupancyMaxActiveClusters(&nclusters, kv.fn, &cfg) == cudaSuccess &&
+            nclusters > 0) {
+            b->grid = std::min(b->grid / b->cluster, nclusters) * b->cluster;
+        } else {
+            cudaGetLastError();
+            b->cluster = 1;
+        }
+    }
     return 0;
 }
 
@@ -324,21 +380,16 @@ int batch_step_listed(AvbdBatch* b, const std::vector<int>& slots) {
     const int n = (int)slots.size();
     cudaStream_t s = b->stream;
     cudaMemcpyAsync(b->d_fix_order, slots.data(), n * sizeof(int), cudaMemcpyHostToDevice, s);
-    cudaMemcpyAsync(b->d_fix_n, &n, sizeof(int), cudaMemcpyHostToDevice, s);
-    cudaMemsetAsync(b->d_queue, 0, sizeof(int), s);
+    const int counts[2] = {n, 0};   // catch-up steps: no cluster phase
+    cudaMemcpyAsync(b->d_fix_n, counts, sizeof(counts), cudaMemcpyHostToDevice, s);
+    cudaMemsetAsync(b->d_queue, 0, 2 * sizeof(int), s);
     World W = b->P.W;
     W.stage_bodies = b->stage;
     W.team_work = b->team_work;
     W.fem_team_work = b->fem_team_work;
     W.grid_min = b->grid_min;
     W.fail_count = b->d_fail;
-    const int* order = b->d_fix_order;
-    const int* nlive = b->d_fix_n;
-    int* queue = b->d_queue;
-    void* args[] = {&W, &order, &nlive, &queue};
-    if (cudaLaunchKernel((const void*)kBatchVariants[b->variant].fn, dim3(b->grid), dim3(b->threads), args,
-                         (size_t)b->stage * sizeof(float4), s) != cudaSuccess)
-        return AVBD_ERR_CUDA;
+    if (launch_batch_kernel(b, W, b->d_fix_order, b->d_fix_n, b->d_queue) != cudaSuccess) return AVBD_ERR_CUDA;
     return cudaStreamSynchronize(s) == cudaSuccess ? 0 : AVBD_ERR_CUDA;
 }
 
@@ -382,22 +433,14 @@ int batch_build_graph(AvbdBatch* b) {
     batch_drop_graph(b);
     cudaGraph_t g;
     if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return AVBD_ERR_CUDA;
-    cudaMemsetAsync(b->d_queue, 0, sizeof(int), b->stream);
+    cudaMemsetAsync(b->d_queue, 0, 2 * sizeof(int), b->stream);
     b->P.W.stage_bodies = b->stage;
     b->P.W.team_work = b->team_work;
     b->P.W.fem_team_work = b->fem_team_work;
     b->P.W.grid_min = b->grid_min;
     b->P.W.fail_count = b->d_fail;
-    const size_t smem = (size_t)b->stage * sizeof(float4);
-    {
-        const int* order = b->d_order;
-        const int* nlive = b->d_nlive;
-        int* queue = b->d_queue;
-        void* args[] = {&b->P.W, &order, &nlive, &queue};
-        cudaLaunchKernel((const void*)kBatchVariants[b->variant].fn, dim3(b->grid), dim3(b->threads), args, smem,
-                         b->stream);
-    }
-    if (cudaStreamEndCapture(b->stream, &g) != cudaSuccess) return AVBD_ERR_CUDA;
+    const cudaError_t launched = launch_batch_kernel(b, b->P.W, b->d_order, b->d_nlive, b->d_queue);
+    if (cudaStreamEndCapture(b->stream, &g) != cudaSuccess || launched != cudaSuccess) return AVBD_ERR_CUDA;
     cudaError_t e = cudaGraphInstantiate(&b->graph, g, 0);
     cudaGraphDestroy(g);
     return e == cudaSuccess ? 0 : AVBD_ERR_CUDA;
@@ -702,6 +745,16 @@ int32_t avbd_batch_set_fem_team_work(AvbdBatch* b, int32_t units_per_lane) {
     if (!b || units_per_lane < 0) return AVBD_ERR_INVALID;
     b->fem_team_work = units_per_lane;
     batch_drop_graph(b);
+    return 0;
+}
+
+int32_t avbd_batch_set_cluster(AvbdBatch* b, int32_t cluster_size, int32_t min_units) {
+    if (!b || !(cluster_size == 1 || cluster_size == 2 || cluster_size == 4 || cluster_size == 8) || min_units < 0)
+        return AVBD_ERR_INVALID;
+    if (b->graph || b->grid) return AVBD_ERR_STATE;   // before the launch shape is fixed
+    b->cluster = cluster_size;
+    b->cluster_min = min_units;
+    b->order_dirty = true;
     return 0;
 }
 

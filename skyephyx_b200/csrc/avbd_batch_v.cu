@@ -53,17 +53,37 @@ __device__ __forceinline__ bool scene_fits_half(const World& W, int scene, int t
     return (long long)(d.nbody + d.ntet) <= (long long)work * (team_size / 2);
 }
 
+// Launched plain or in thread-block clusters.  In clusters, the scenes at
+// the head of the queue (the largest; nlive[1] of them) are each run by a
+// whole cluster first; then every CTA pulls the remaining scenes as above.
+// Cluster barriers need every thread of the cluster, so the cluster phase
+// is left by all of its CTAs together, on the same queue ticket.
 template <int MAXT, int MINB>
 __global__ void __launch_bounds__(MAXT, MINB) k_batch_step(const __grid_constant__ World W, const int* order,
                                                              const int* nlive_ptr, int* queue) {
     __shared__ TeamShared s_team[kMaxTeams];
     extern __shared__ float4 s_stage[];
-    const int nlive = *nlive_ptr;   // live scenes, read from device memory so the graph stays replayable
+    const int nlive = nlive_ptr[0];   // live scenes, read from device memory so the graph stays replayable
+    const int nlarge = min(nlive_ptr[1], nlive);
+    const bool clustered = cooperative_groups::this_cluster().num_blocks() > 1;
+    if (clustered && nlarge > 0) {
+        const Team C = Team::cluster(s_team, s_stage, W.stage_bodies);
+        for (;;) {
+            if (C.rank == 0) C.sh->q = atomicAdd(queue + 1, 1);
+            C.sync();
+            const int q = C.sh->q;
+            C.sync();   // every CTA read the ticket before the next one is drawn
+            if (q >= nlarge) break;
+            scene_step(W, order[q], C);
+            C.sync();
+        }
+    }
+    const int first = clustered ? nlarge : 0;
     Team T = Team::cta(s_team, s_stage, W.stage_bodies);
     int scene = -1;
     for (;;) {
         if (scene < 0) {
-            if (T.rank == 0) T.sh->q = atomicAdd(queue, 1);
+            if (T.rank == 0) T.sh->q = first + atomicAdd(queue, 1);
             T.sync();
             const int q = T.sh->q;
             T.sync();

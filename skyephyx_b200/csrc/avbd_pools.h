@@ -598,6 +598,8 @@ struct AvbdBatch {
     int team_work = 0;   // bodies + tets per lane below which a CTA team splits (0 = never)
     int fem_team_work = 0;   // the same for scenes with tets
     int grid_min = 128;  // scenes from this many bodies use the grid broadphase (0 = never)
+    int cluster = 1;     // CTAs per thread-block cluster (1 = plain launch)
+    int cluster_min = 0; // bodies + tets from which a scene is run by a whole cluster
     std::vector<long long> steps_due;   // steps each slot's scene should have taken
     int* d_fail = nullptr;               // scene steps stopped by a full table (device counter)
     int* d_fix_order = nullptr;          // catch-up queue
@@ -625,6 +627,10 @@ int batch_reserve(AvbdBatch* b, int64_t bodies, int64_t forces, int64_t tets, in
 int batch_place(AvbdBatch* b, int slot);
 int batch_flush(AvbdBatch* b);
 int batch_launch_shape(AvbdBatch* b);
+// Scenes at the head of the size-ordered list that a whole cluster runs.
+int cluster_scenes(const AvbdBatch* b, const std::vector<int>& order);
+// Launches the batch's persistent kernel build (in clusters when set) on its stream.
+cudaError_t launch_batch_kernel(AvbdBatch* b, const World& W, const int* order, const int* nlive, int* queue);
 int batch_build_graph(AvbdBatch* b);
 void batch_sync_order(AvbdBatch* b);
 int batch_fix_capacity(AvbdBatch* b);

@@ -75,6 +75,7 @@ struct AvbdServer {
     int* order_host = nullptr;          // page-locked live-slot order
     int order_cap = 0;
     cudaEvent_t step_done = nullptr;
+    cudaEvent_t step_begin = nullptr, step_end = nullptr;   // device time of each step
     bool in_flight = false;
     int64_t resident_dynamic = 0;
     int64_t pool_bodies = 0;            // pool capacity, reserved at the first tick
@@ -140,6 +141,8 @@ int server_complete(AvbdServer* s, double now) {
     AvbdBatch* b = s->b;
     if (cudaEventSynchronize(s->step_done) != cudaSuccess) return AVBD_ERR_CUDA;
     s->in_flight = false;
+    float ms = 0.f;
+    if (cudaEventElapsedTime(&ms, s->step_begin, s->step_end) == cudaSuccess) s->stats.device_us += (int64_t)(ms * 1e3f);
     // scenes a full table stopped grow and catch up before anything reads them
     if (int r = batch_fix_capacity(b)) return r;
     bool refetch = false;
@@ -202,16 +205,17 @@ int server_sync_order(AvbdServer* s) {
         return (a.nbody + a.ntet) > (c.nbody + c.ntet);
     });
     const int n = (int)order.size();
-    if (n + 1 > s->order_cap) {
-        if (grow_pinned(reinterpret_cast<void**>(&s->order_host), (size_t)(n + 1 + 1024) * sizeof(int)))
+    if (n + 2 > s->order_cap) {
+        if (grow_pinned(reinterpret_cast<void**>(&s->order_host), (size_t)(n + 2 + 1024) * sizeof(int)))
             return AVBD_ERR_NOMEM;
-        s->order_cap = n + 1 + 1024;
+        s->order_cap = n + 2 + 1024;
     }
-    std::copy(order.begin(), order.end(), s->order_host + 1);
+    std::copy(order.begin(), order.end(), s->order_host + 2);
     s->order_host[0] = n;
+    s->order_host[1] = cluster_scenes(b, order);
     b->nlive = n;
-    if (n) cudaMemcpyAsync(b->d_order, s->order_host + 1, n * sizeof(int), cudaMemcpyHostToDevice, b->stream);
-    cudaMemcpyAsync(b->d_nlive, s->order_host, sizeof(int), cudaMemcpyHostToDevice, b->stream);
+    if (n) cudaMemcpyAsync(b->d_order, s->order_host + 2, n * sizeof(int), cudaMemcpyHostToDevice, b->stream);
+    cudaMemcpyAsync(b->d_nlive, s->order_host, 2 * sizeof(int), cudaMemcpyHostToDevice, b->stream);
     b->order_dirty = false;
     return 0;
 }
@@ -234,7 +238,9 @@ int32_t avbd_server_create(const AvbdParams* params, int32_t device, int64_t bod
     s->b = b;
     s->pool_bodies = bodies;
     s->max_scenes = max_scenes;
-    if (cudaEventCreateWithFlags(&s->step_done, cudaEventDisableTiming) != cudaSuccess) r = AVBD_ERR_CUDA;
+    if (cudaEventCreateWithFlags(&s->step_done, cudaEventDisableTiming) != cudaSuccess ||
+        cudaEventCreate(&s->step_begin) != cudaSuccess || cudaEventCreate(&s->step_end) != cudaSuccess)
+        r = AVBD_ERR_CUDA;
     if (r) {
         avbd_server_destroy(s);
         return r;
@@ -250,6 +256,8 @@ int32_t avbd_server_destroy(AvbdServer* s) {
         if (s->b->stream) cudaStreamSynchronize(s->b->stream);
     }
     if (s->step_done) cudaEventDestroy(s->step_done);
+    if (s->step_begin) cudaEventDestroy(s->step_begin);
+    if (s->step_end) cudaEventDestroy(s->step_end);
     if (s->rb) cudaFreeHost(s->rb);
     if (s->rb_state) cudaFreeHost(s->rb_state);
     if (s->order_host) cudaFreeHost(s->order_host);
@@ -311,7 +319,9 @@ int32_t avbd_server_tick(AvbdServer* s, double now_s) {
     b->P.W.P = to_params(b->params);
     if (!b->graph && batch_build_graph(b)) return AVBD_ERR_CUDA;
     cudaMemsetAsync(b->d_fail, 0, sizeof(int), b->stream);
+    cudaEventRecord(s->step_begin, b->stream);
     if (cudaGraphLaunch(b->graph, b->stream) != cudaSuccess) return AVBD_ERR_CUDA;
+    cudaEventRecord(s->step_end, b->stream);
     s->stats.ticks += 1;
     s->stats.body_iterations += s->resident_dynamic * b->params.num_iterations;
     size_t need = 0;

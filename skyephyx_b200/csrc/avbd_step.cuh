@@ -4,6 +4,8 @@
 // one CTA, and the single-scene path launches the same per-item functions as
 // grid-wide kernels between them.
 #pragma once
+#include <cooperative_groups.h>
+
 #include "avbd_phases.cuh"
 
 namespace avbd {
@@ -26,19 +28,38 @@ struct TeamShared {
 // named barrier (a single warp uses __syncwarp).  Teams only split, so the
 // teams alive at one time partition the CTA's warps; a team's barrier id and
 // shared slot follow from its first warp, which no other live team shares.
+constexpr int kClusterBar = -2;   // Team::bar of a team that is a whole thread-block cluster
+
 struct Team {
     int rank;          // thread index within the team
     int size;          // threads (a multiple of 32)
     int first_warp;    // first warp of the team within the CTA
-    int bar;           // named barrier id (0 for the whole CTA)
+    int bar;           // named barrier id (0 for the whole CTA, kClusterBar for a cluster)
     TeamShared* sh;    // the team's shared scalars
     float4* stage;     // the team's slice of the dynamic shared memory
     int stage_cap;     // float4 slots in that slice
 
     __device__ __forceinline__ void sync() const {
         if (bar == 0) __syncthreads();
+        else if (bar == kClusterBar) cooperative_groups::this_cluster().sync();
         else if (size == 32) __syncwarp();
         else asm volatile("bar.sync %0, %1;" ::"r"(bar), "r"(size) : "memory");
+    }
+    // Every thread of the thread-block cluster as one team: ranks run over
+    // the cluster's CTAs, and the team's shared scalars and stage are those
+    // of its first CTA, reached through distributed shared memory.  The
+    // cluster barrier orders global and shared memory across its CTAs.
+    __device__ __forceinline__ static Team cluster(TeamShared* shared, float4* stage, int stage_cap) {
+        cooperative_groups::cluster_group cl = cooperative_groups::this_cluster();
+        Team t;
+        t.rank = (int)(cl.block_rank() * blockDim.x + threadIdx.x);
+        t.size = (int)(cl.num_blocks() * blockDim.x);
+        t.first_warp = 0;
+        t.bar = kClusterBar;
+        t.sh = cl.map_shared_rank(shared, 0);
+        t.stage = cl.map_shared_rank(stage, 0);
+        t.stage_cap = stage_cap;
+        return t;
     }
     // Smallest team a CTA splits into: a warp, or an eighth of a larger CTA.
     __device__ __forceinline__ static int min_size() { return max(32, (int)(blockDim.x / kMaxTeams)); }
@@ -727,18 +748,28 @@ struct GridCells {
     __device__ __forceinline__ int item(int k) const { return items16 ? (int)items16[k] : items32[k]; }
 };
 
-template <bool WRITE>
+// True when (li, lj), lj > li, is a broadphase candidate: the reference's
+// sphere test and no live joint/spring between them (isConstrainedTo).
+__device__ __forceinline__ bool grid_pair(const World& W, const SceneDesc& sc, const float4* sp, const float4& pi,
+                                          int li, int lj) {
+    const float4 pj = body_sphere(W, sc, sp, lj);
+    if (!sphere_overlap_fast(pi, pj, pi.w, pj.w)) return false;
+    return !pair_constrained(W, 0, sc.body0 + li, sc.body0 + lj);
+}
+
+// SORTED: the caller visits partners in increasing order, so a candidate is
+// appended; otherwise it is inserted in partner order, as the all-pairs loop
+// emits them.
+template <bool WRITE, bool SORTED = false>
 __device__ __forceinline__ void grid_test(const World& W, const SceneDesc& sc, const float4* sp, const float4& pi,
                                           int li, int lj, int2* out, int& n) {
     if (lj <= li) return;
-    const float4 pj = body_sphere(W, sc, sp, lj);
-    if (!sphere_overlap_fast(pi, pj, pi.w, pj.w)) return;
-    const int bi = sc.body0 + li, bj = sc.body0 + lj;
-    if (pair_constrained(W, 0, bi, bj)) return;
+    if (!grid_pair(W, sc, sp, pi, li, lj)) return;
     if (WRITE) {
-        // insert in partner order, as the all-pairs loop emits them
+        const int bi = sc.body0 + li, bj = sc.body0 + lj;
         int j = n - 1;
-        while (j >= 0 && out[j].y > bj) { out[j + 1] = out[j]; --j; }
+        if (!SORTED)
+            while (j >= 0 && out[j].y > bj) { out[j + 1] = out[j]; --j; }
         out[j + 1] = make_int2(bi, bj);
     }
     ++n;
@@ -751,8 +782,8 @@ __device__ __forceinline__ int grid_candidates(const World& W, const SceneDesc& 
     if (isinf(pi.w)) return 0;
     int n = 0;
     if (pi.w > gc.rbig) {
-        // a big body: its all-pairs row
-        for (int lj = li + 1; lj < sc.nbody; ++lj) grid_test<WRITE>(W, sc, sp, pi, li, lj, out, n);
+        // a big body: its all-pairs row, in partner order
+        for (int lj = li + 1; lj < sc.nbody; ++lj) grid_test<WRITE, true>(W, sc, sp, pi, li, lj, out, n);
         return n;
     }
     const int cx = g.cell_axis(pi.x, g.minx, g.nx), cy = g.cell_axis(pi.y, g.miny, g.ny),

@@ -196,6 +196,9 @@ class _BatchKnobs:
     def set_fem_team_work(self, units):
         check(self._lib.avbd_batch_set_fem_team_work(self._h, int(units)), "set_fem_team_work")
 
+    def set_cluster(self, cluster_size, min_units):
+        check(self._lib.avbd_batch_set_cluster(self._h, int(cluster_size), int(min_units)), "set_cluster")
+
     def set_grid_broadphase(self, min_bodies):
         check(self._lib.avbd_batch_set_grid_broadphase(self._h, int(min_bodies)), "set_grid_broadphase")
 

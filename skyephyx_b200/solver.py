@@ -436,6 +436,11 @@ class Batch:
         """Scenes of at least min_bodies use the grid broadphase (0: all-pairs)."""
         check(self._lib.avbd_batch_set_grid_broadphase(self._h, int(min_bodies)), "set_grid_broadphase")
 
+    def set_cluster(self, cluster_size=1, min_units=0):
+        """Scenes of at least min_units bodies + tets run on a whole thread-block
+        cluster of cluster_size CTAs (1 = off); before stepping."""
+        check(self._lib.avbd_batch_set_cluster(self._h, int(cluster_size), int(min_units)), "set_cluster")
+
     def set_kernel(self, register_variant=1):
         """Build of the persistent kernel: 1..4 for CTAs of up to 256 threads
         (156, 128, 80 or 64 registers), 5/6 for 512 threads, 7 for 1024."""

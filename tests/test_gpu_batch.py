@@ -381,3 +381,31 @@ def test_scene_snapshot_restores_elsewhere_and_replays():
         assert same(b.get_state(back[k])[:2], alone.get_state(0)[:2]), f"scene {k}"
         assert b.scene_info(back[k])["steps"] == 9
     assert b.scene_status(filler) == "ok"
+
+
+def test_cluster_runs_change_nothing():
+    """Scenes run by a whole thread-block cluster (ranks over 2 or 4 CTAs,
+    team scalars and stage in the first CTA's shared memory) end bitwise
+    where the plain launch leaves them, large and small, rigid and FEM."""
+    from skyephyx_b200 import Batch, GROUP_FLAT
+    builders = mix_builders() + [
+        lambda s: scenes.rigid_pile(s, 400, scenes.rng_for(4, 41), stack=False),
+        lambda s: scenes.rigid_pile(s, 300, scenes.rng_for(4, 42), stack=True),
+        lambda s: scenes.fem_scene(s, 2500, scenes.rng_for(4, 43)),
+    ]
+    runs = []
+    for cluster, min_units in ((1, 0), (2, 0), (4, 300)):
+        b = Batch()
+        b.set_groups(1, GROUP_FLAT)
+        b.set_team_work(2)
+        b.set_cluster(cluster, min_units)
+        keep = [staged(f) for f in builders]
+        for w in keep:
+            b.add_scene(w)
+        assert b.step(3) == "ok"
+        runs.append([b.get_state(i)[:2] for i in range(len(builders))])
+        for i in range(len(builders)):
+            assert b.scene_status(i) == "ok", (cluster, i)
+    for run in runs[1:]:
+        for i, (a, c) in enumerate(zip(runs[0], run)):
+            assert same(a, c), f"scene {i}"
