@@ -538,6 +538,15 @@ def serve_run(rate, window, warmup, cap_s, budget_gb, launch=None, seed_base=0x5
            "scenes_per_s": (s1["completed"] - s0["completed"]) / dt,
            "ticks_per_s": (s1["ticks"] - s0["ticks"]) / dt, "resident_dynamic_at_window_end": s1["resident_dynamic"],
            "gpu_busy_fraction": (s1["device_us"] - s0["device_us"]) / 1e6 / dt,
+           # host time blocked on the step in flight, and spent growing full
+           # tables and re-running the steps their scenes missed
+           "host_wait_fraction": (s1["wait_us"] - s0["wait_us"]) / 1e6 / dt,
+           "catchup_fraction": (s1["catchup_us"] - s0["catchup_us"]) / 1e6 / dt,
+           "host_stage_fraction": (s1["stage_us"] - s0["stage_us"]) / 1e6 / dt,
+           "host_retire_fraction": (s1["retire_us"] - s0["retire_us"]) / 1e6 / dt,
+           "host_issue_fraction": (s1["issue_us"] - s0["issue_us"]) / 1e6 / dt,
+           "uploaded_mb_per_s": (s1["uploaded_bytes"] - s0["uploaded_bytes"]) / 1e6 / dt,
+           "regrown_scenes": s1["regrown"] - s0["regrown"],
            "p50_s": lat.get("p50_s"), "p99_s": lat.get("p99_s"), "latency_requests": lat.get("completed", 0),
            "admission_wait_p50_s": float(np.percentile(waits, 50)) if waits.size else None,
            "admission_wait_p99_s": float(np.percentile(waits, 99)) if waits.size else None,
@@ -553,28 +562,38 @@ def serve_run(rate, window, warmup, cap_s, budget_gb, launch=None, seed_base=0x5
     return out
 
 
-def served_mix_batched(n, launch, seed_base=0x5EED0005, steps=5):
-    """The first n requests' scenes of the served workload stepped as one
-    batch (all resident, no admission): the batched rate of the scene
-    composition the server runs."""
+# Mean age in steps of a resident served scene: a request of L steps is
+# resident through ages 0..L, so ages weigh by L: E[L^2] / (2 E[L]) for
+# L ~ U{60..600}.
+SERVED_MEAN_AGE = int(round(sum(L * L for L in range(60, 601)) / (2.0 * sum(range(60, 601)))))
+
+
+def served_mix_batched(target_dynamic, launch, seed_base=0x5EED0005, steps=5, age=SERVED_MEAN_AGE):
+    """The served workload's scenes, in request order until `target_dynamic`
+    dynamic bodies (the server's resident size), stepped as one batch with no
+    admission, timed after `age` steps (the mean resident age): the batched
+    rate of what the server runs."""
     from skyephyx_b200 import Batch, Solver, autotune, scenes
-    sizes = serve_sizes(n, seed_base + 2)
+    sizes = serve_sizes(65536, seed_base + 2)
     b = Batch(iterations=ITERS)
     keep = []
     dyn = 0
-    for i, size in enumerate(sizes):
+    n = 0
+    while dyn < target_dynamic and n < len(sizes):
         s = Solver(iterations=ITERS)
-        scenes.served_scene(s, size, seed_base + i)
+        scenes.served_scene(s, sizes[n], seed_base + n)
         keep.append(s)
         b.add_scene(s)
         dyn += s.num_dynamic
+        n += 1
     if launch:
         autotune.apply(b, launch)
-    b.step(3)
+    b.step(age)
     b.step(steps)
     ms = b.last_ms / steps
     b.close()
-    return {"scenes": n, "dynamic_bodies": dyn, "ms_per_step": ms, "body_iters_per_s": dyn * ITERS / (ms / 1e3)}
+    return {"scenes": n, "dynamic_bodies": dyn, "age_steps": age, "ms_per_step": ms,
+            "body_iters_per_s": dyn * ITERS / (ms / 1e3)}
 
 
 def serve_bench(rate, window, warmup, budget_gb, launch=None):
@@ -583,7 +602,7 @@ def serve_bench(rate, window, warmup, budget_gb, launch=None):
     latency is queueing-free."""
     hot = serve_run(rate, window, warmup, 20.0, budget_gb, launch)
     out = {"offered": hot}
-    same = served_mix_batched(8192, launch)
+    same = served_mix_batched(max(hot["resident_dynamic_at_window_end"], 1), launch)
     out["batched_same_composition"] = same
     out["served_over_batched_same_composition"] = hot["body_iters_per_s"] / same["body_iters_per_s"]
     sustained = hot["scenes_per_s"]

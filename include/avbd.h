@@ -340,6 +340,14 @@ int32_t avbd_batch_set_cluster(AvbdBatch* b, int32_t cluster_size, int32_t min_u
  * uniform grid (the same candidate set and order as the reference's all-pairs
  * loop, which smaller scenes keep); 0 = all-pairs everywhere.  Default 128. */
 int32_t avbd_batch_set_grid_broadphase(AvbdBatch* b, int32_t min_bodies);
+/* Per-scene device timing (off by default): each step stamps the GPU's
+ * global timer (ns) when a scene's team starts it and when the team is done.
+ * avbd_batch_scene_times copies (start, end) of each slot's last step, up
+ * to max_slots slots, and returns the slots copied (0, 0 for a slot that has
+ * not stepped since timing was switched on); with start_end_ns NULL it
+ * returns the number of slots. */
+int32_t avbd_batch_set_scene_timing(AvbdBatch* b, int32_t on);
+int32_t avbd_batch_scene_times(AvbdBatch* b, int64_t* start_end_ns, int32_t max_slots);
 /* Build of the persistent kernel: 1..4 serve CTAs of up to 256 threads with
  * about 156, 128, 80 or 64 registers per thread (spills traded for resident
  * warps); 5 and 6 serve 512 threads (128 or 64 registers), 7 serves 1024
@@ -389,6 +397,12 @@ typedef struct AvbdServerStats {
     int64_t uploaded_bytes;    /* host-to-device bytes of admitted scenes */
     int64_t pending, active, resident_dynamic;
     int64_t device_us;         /* device time of the steps completed, microseconds */
+    int64_t wait_us;           /* host time blocked on the step in flight, microseconds */
+    int64_t regrown;           /* scenes whose full tables grew (each re-ran the steps it missed) */
+    int64_t catchup_us;        /* host time spent growing tables and re-running steps, microseconds */
+    int64_t stage_us;          /* host time placing and staging newcomers (while a step runs) */
+    int64_t retire_us;         /* host time filing readbacks and retiring scenes after a step, incl. catch-up */
+    int64_t issue_us;          /* host time issuing uploads, the order list, the step and readbacks */
 } AvbdServerStats;
 
 /* Pools for `bodies` bodies (a quarter as many joints+springs and

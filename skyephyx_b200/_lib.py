@@ -42,7 +42,8 @@ class AvbdServedRequest(C.Structure):
 class AvbdServerStats(C.Structure):
     _fields_ = [(n, C.c_int64) for n in ("submitted", "admitted", "completed", "ticks", "body_iterations",
                                          "uploaded_bytes", "pending", "active", "resident_dynamic",
-                                         "device_us")]
+                                         "device_us", "wait_us", "regrown", "catchup_us", "stage_us",
+                                         "retire_us", "issue_us")]
 
 
 class AvbdTimings(C.Structure):
@@ -131,6 +132,8 @@ SIGNATURES = [
     ("avbd_batch_set_fem_team_work", [_V, C.c_int32], C.c_int32),
     ("avbd_batch_set_grid_broadphase", [_V, C.c_int32], C.c_int32),
     ("avbd_batch_set_cluster", [_V, C.c_int32, C.c_int32], C.c_int32),
+    ("avbd_batch_set_scene_timing", [_V, C.c_int32], C.c_int32),
+    ("avbd_batch_scene_times", [_V, C.POINTER(C.c_int64), C.c_int32], C.c_int32),
     ("avbd_batch_last_ms", [_V], C.c_float),
     ("avbd_batch_set_groups", [_V, C.c_int32, C.c_int32], C.c_int32),
     ("avbd_set_group", [_V, C.c_int32], C.c_int32),

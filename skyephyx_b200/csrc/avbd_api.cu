@@ -225,13 +225,14 @@ __global__ void __launch_bounds__(1024) k_bp_big(const __grid_constant__ World W
         const int li = gs->big[k];
         const int b = sc.body0 + li;
         const float4 pi = body_sphere(W, sc, nullptr, li);
+        const Partners pp = partners_of(W, b);
         int2* out = WRITE ? W.cpair[cur] + sc.cand0 + W.cand_off[b] : nullptr;
         const int cap = WRITE ? W.cand_cnt[b] : 0;
         if (threadIdx.x == 0) s_total = 0;
         __syncthreads();
         for (int c0 = li + 1; c0 < sc.nbody; c0 += blockDim.x) {
             const int lj = c0 + threadIdx.x;
-            const bool hit = !isinf(pi.w) && lj < sc.nbody && grid_pair(W, sc, nullptr, pi, li, lj);
+            const bool hit = !isinf(pi.w) && lj < sc.nbody && grid_pair(W, sc, nullptr, pi, pp, lj);
             const unsigned bal = __ballot_sync(0xffffffffu, hit);
             if (lane == 0) s_warp[warp] = __popc(bal);
             __syncthreads();
@@ -288,18 +289,341 @@ __global__ void k_force_init(const __grid_constant__ World W) {
         if (force_init(W, f)) atomicAdd(&W.sstate[0].topo, 1);
 }
 
-__global__ void k_incidence_colour(const __grid_constant__ World W, int cur) {
+
+// ---------------------------------------------------------------------------
+// Incidence and colouring of the single scene, grid-wide: the stages of
+// build_incidence and colour_scene (one team per scene in the batched path)
+// as kernels over all bodies.  Each Jones-Plassmann round is one launch; the
+// host launches rounds in chunks and reads in between whether the pass has
+// ended, so the colouring equals sequential greedy in priority order
+// whatever the schedule, as in the batched path.
+// ---------------------------------------------------------------------------
+struct ColourState {
+    int skip;                       // the previous colouring still holds (or the step already failed)
+    int done;                       // the current pass ended (read by the host with skip)
+    int rf[3][2];                   // per round (mod 3): bodies remaining, progress made
+    int stalled;
+    int maxc;                       // colours used
+    int count[kMaxColours + 1];     // bodies per colour, then list cursors
+};
+
+#define AVBD_BODIES(b)                                                                                   \
+    for (int b = sc.body0 + blockIdx.x * blockDim.x + threadIdx.x; b < sc.body0 + sc.nbody;            \
+         b += gridDim.x * blockDim.x)
+#define AVBD_SLOTS(c, n)                                                                                 \
+    for (int c = sc.cand0 + blockIdx.x * blockDim.x + threadIdx.x; c < sc.cand0 + (n); c += gridDim.x * blockDim.x)
+
+__global__ void k_inc_count_b(const __grid_constant__ World W, int cur) {
+    const SceneDesc sc = W.scenes[0];
+    AVBD_SLOTS(c, W.sstate->ncand[cur])
+        if (W.cn[cur][c] > 0) atomicAdd(&W.cntB[W.cpair[cur][c].y], 1);
+}
+
+__global__ void k_inc_count(const __grid_constant__ World W, int cur) {
+    const SceneDesc sc = W.scenes[0];
+    AVBD_BODIES(b) W.inc_cnt[b] = body_fixed(W, b) ? 0 : W.sinc_n[b] + W.cntB[b] + owned_live(W, cur, b, sc.cand0);
+}
+
+__global__ void k_inc_scan(const __grid_constant__ World W) {
     __shared__ TeamShared s_team;
-    __shared__ float4 s_count[(kMaxColours + 1 + 3) / 4];   // colour counts
-    const Team T = Team::cta(&s_team, s_count, (kMaxColours + 1 + 3) / 4);
+    const Team T = Team::cta(&s_team, nullptr, 0);
     const SceneDesc sc = W.scenes[0];
     SceneState* st = W.sstate;
-    if (!build_incidence(T, W, sc, st, cur)) {
-        if (threadIdx.x == 0) st->status = kStatusCapacity;
-        return;
+    const int total = block_exclusive_scan(T, W.inc_cnt + sc.body0, W.inc_off + sc.body0, sc.nbody);
+    if (threadIdx.x == 0) {
+        st->ninc = total;
+        if (total > sc.inccap) { st->need_inc = total; st->status = kStatusCapacity; }
     }
-    colour_scene_cached(T, W, sc, st, 0, cur);
 }
+
+__global__ void k_inc_fill(const __grid_constant__ World W, int cur) {
+    const SceneDesc sc = W.scenes[0];
+    if (W.sstate->status != kStatusOk) return;
+    AVBD_BODIES(b) {
+        const int off = sc.inc0 + W.inc_off[b];
+        W.inc_off[b] = off;
+        W.bcur[b] = 0;
+        if (body_fixed(W, b)) continue;
+        const int s0 = W.sinc_off[b], nf = W.sinc_nf[b], ns = W.sinc_n[b];
+        int k = off;
+        for (int e = 0; e < nf; ++e) W.inc[k++] = W.sinc[s0 + e];
+        k += W.cntB[b];
+        const int c0 = W.cand_off[b] + sc.cand0, c1 = c0 + W.cand_cnt[b];
+        for (int c = c0; c < c1; ++c)
+            if (W.cn[cur][c] > 0) W.inc[k++] = ent_make(kEntManifold, 0, (uint32_t)c);
+        for (int e = nf; e < ns; ++e) W.inc[k++] = W.sinc[s0 + e];
+    }
+}
+
+__global__ void k_inc_fill_b(const __grid_constant__ World W, int cur) {
+    const SceneDesc sc = W.scenes[0];
+    if (W.sstate->status != kStatusOk) return;
+    AVBD_SLOTS(c, W.sstate->ncand[cur]) {
+        if (W.cn[cur][c] == 0) continue;
+        const int B = W.cpair[cur][c].y;
+        if (body_fixed(W, B)) continue;
+        const int p = atomicAdd(&W.bcur[B], 1);
+        W.inc[W.inc_off[B] + W.sinc_nf[B] + p] = ent_make(kEntManifold, 1, (uint32_t)c);
+    }
+}
+
+// Each body's manifolds as Mesh::forces holds them: by creation step, then pair.
+__global__ void k_inc_sort(const __grid_constant__ World W, int cur) {
+    const SceneDesc sc = W.scenes[0];
+    if (W.sstate->status != kStatusOk) return;
+    AVBD_BODIES(b) {
+        if (!body_fixed(W, b))
+            sort_manifold_entries(W, cur, W.inc + W.inc_off[b] + W.sinc_nf[b], W.inc_cnt[b] - W.sinc_n[b]);
+    }
+}
+
+// Whether the colouring is redone this step (colour_scene_cached's test):
+// not when the contact graph is the one the colours were made for.
+__global__ void k_col_prepare(const __grid_constant__ World W, ColourState* cs, int cur) {
+    if (blockIdx.x != 0 || threadIdx.x != 0) return;
+    const SceneState* st = W.sstate;
+    const int old = cur ^ 1;
+    const bool reuse = st->colours_valid && st->nlive[cur] == st->nlive[old] && st->nmatched == st->nlive[cur] &&
+                       st->topo == st->coloured_topo;
+    cs->skip = (reuse || st->status != kStatusOk) ? 1 : 0;
+    cs->done = cs->skip;
+    cs->stalled = 0;
+    cs->maxc = 0;
+    for (int r = 0; r < 3; ++r) cs->rf[r][0] = cs->rf[r][1] = 0;
+    for (int c = 0; c <= kMaxColours; ++c) cs->count[c] = 0;
+}
+
+// Neighbour lists and priorities of the colouring, once per colouring.
+struct ColourLists {
+    int* nbr;                  // body b's dynamic neighbours from 3 * (inc_off[b] - inc0), one per
+                               // live neighbour visit of for_each_neighbour (repeats kept)
+    int* cnt;
+    unsigned long long* key;   // u precedes v in pass 0 iff key[u] > key[v]
+    int* pos;                  // neighbours already scanned this pass (bit 30: one held a colour >= 64)
+    unsigned long long* used;  // colours < 64 of the scanned neighbours
+};
+constexpr int kPosWide = 1 << 30;
+
+// Pass-0 priority as one integer: larger live degree first, then smaller
+// colour_priority(local index), which is a bijection, so ties cannot remain
+// (colour_before's order exactly).
+__device__ __forceinline__ unsigned long long colour_key(int degree, int local) {
+    return ((unsigned long long)(unsigned)degree << 32) | (unsigned long long)(~colour_priority((uint32_t)local));
+}
+
+// Live degree and pass-0 priority of every dynamic body.
+__global__ void k_col_init(const __grid_constant__ World W, const ColourState* cs, ColourLists L) {
+    const SceneDesc sc = W.scenes[0];
+    if (cs->skip) return;
+    AVBD_BODIES(b) {
+        if (body_fixed(W, b)) {
+            W.colour[b] = -2;
+            L.cnt[b] = 0;
+            continue;
+        }
+        W.colour[b] = -1;
+        L.key[b] = colour_key(live_degree(W, b), W.local[b]);
+    }
+}
+
+// Body u precedes body v in the pass's order (colour_before with the
+// pass-0 priority as one integer).
+__device__ __forceinline__ bool precedes(const World& W, const ColourLists& L, int pass, int u, int v) {
+    if (pass == 1) {
+        const int pu = W.bcur[u], pv = W.bcur[v];
+        if (pu != pv) return pu > pv;
+    }
+    return L.key[u] > L.key[v];
+}
+
+// Each dynamic body's list of the neighbours that precede it in this pass
+// (one entry per neighbour visit of for_each_neighbour; repeats kept), the
+// only ones a Jones-Plassmann body waits for or takes colours from.
+__global__ void k_col_pred(const __grid_constant__ World W, const ColourState* cs, ColourLists L, int cur, int pass) {
+    const SceneDesc sc = W.scenes[0];
+    if (cs->skip) return;
+    AVBD_BODIES(b) {
+        L.pos[b] = 0;
+        L.used[b] = 0ull;
+        if (body_fixed(W, b)) continue;
+        int* out = L.nbr + 3 * (size_t)(W.inc_off[b] - sc.inc0);
+        int n = 0;
+        for_each_neighbour(W, cur, b, [&](int o) {
+            if (o != b && !body_fixed(W, o) && precedes(W, L, pass, o, b)) out[n++] = o;
+        });
+        L.cnt[b] = n;
+    }
+}
+
+// Second pass (iterated greedy): the first pass's colours become priorities.
+__global__ void k_col_repass(const __grid_constant__ World W, ColourState* cs) {
+    const SceneDesc sc = W.scenes[0];
+    if (cs->skip) return;
+    AVBD_BODIES(b) {
+        const int c = W.colour[b];
+        W.bcur[b] = c;
+        if (c >= 0) W.colour[b] = -1;
+    }
+}
+
+__global__ void k_col_next_pass(ColourState* cs) {
+    if (cs->skip || blockIdx.x != 0 || threadIdx.x != 0) return;
+    cs->done = 0;
+    cs->maxc = 0;
+    for (int r = 0; r < 3; ++r) cs->rf[r][0] = cs->rf[r][1] = 0;
+}
+
+constexpr int kJpSweeps = 16;   // sweeps over a thread's bodies per round launch
+
+// Colours are read and written with relaxed GPU-scope accesses: every sweep
+// must see what other blocks wrote meanwhile (a plain or .cg load could be
+// merged across sweeps), and nothing else is ordered by them.
+__device__ __forceinline__ int ld_colour(const int* p) {
+    int v;
+    asm volatile("ld.relaxed.gpu.global.s32 %0, [%1];" : "=r"(v) : "l"(p) : "memory");
+    return v;
+}
+__device__ __forceinline__ void st_colour(int* p, int v) {
+    asm volatile("st.relaxed.gpu.global.s32 [%0], %1;" ::"l"(p), "r"(v) : "memory");
+}
+constexpr int kJpChunk = 8;     // predecessors whose colours are fetched together
+
+// One Jones-Plassmann round (jp_pass's loop body) over the predecessor
+// lists: a body takes the smallest colour its predecessors do not use once
+// they are all coloured, which is sequential greedy in priority order
+// whatever the schedule.  Colours are final once written, so a body resumes
+// its scan at the predecessor that held it up, with the colours seen so far
+// (pos / used).  A thread sweeps its bodies up to kJpSweeps times, picking
+// up predecessors that other blocks coloured meanwhile.  Round r records its
+// flags in slot r % 3, reads round r - 1's from slot (r - 1) % 3 to see
+// whether the pass ended, and clears slot (r + 1) % 3 for the next round.
+__global__ void k_jp_round(const __grid_constant__ World W, ColourState* cs, ColourLists L, int pass, int round) {
+    const SceneDesc sc = W.scenes[0];
+    if (cs->done) return;
+    if (round > 0) {
+        const int* prev = cs->rf[(round + 2) % 3];
+        if (!prev[0] || !prev[1]) {
+            if (blockIdx.x == 0 && threadIdx.x == 0) {
+                cs->done = 1;
+                if (prev[0]) { cs->stalled = 1; W.sstate->status = kStatusTimeout; }
+            }
+            return;
+        }
+    }
+    if (blockIdx.x == 0 && threadIdx.x == 0) { cs->rf[(round + 1) % 3][0] = 0; cs->rf[(round + 1) % 3][1] = 0; }
+    int* flags = cs->rf[round % 3];
+    int* col = W.colour;
+    bool remaining = false, progress = false;
+    for (int sweep = 0; sweep < kJpSweeps; ++sweep) {
+        bool left = false;
+        AVBD_BODIES(b) {
+            if (ld_colour(col + b) != -1) continue;
+            const int* nb = L.nbr + 3 * (size_t)(W.inc_off[b] - sc.inc0);
+            const int n = L.cnt[b];
+            int pos = L.pos[b];
+            bool wide = (pos & kPosWide) != 0;
+            int i = pos & ~kPosWide;
+            unsigned long long used = L.used[b];
+            bool ready = true;
+            while (i < n) {
+                int cu[kJpChunk];
+#pragma unroll
+                for (int k = 0; k < kJpChunk; ++k) cu[k] = ld_colour(col + (i + k < n ? nb[i + k] : b));
+                const int m = min(kJpChunk, n - i);
+                int k = 0;
+                for (; k < m; ++k) {
+                    if (cu[k] < 0) { ready = false; break; }   // a predecessor is not coloured yet
+                    if (cu[k] < 64) used |= 1ull << cu[k];
+                    else wide = true;
+                }
+                i += k;
+                if (!ready) break;
+            }
+            if (!ready) {
+                L.pos[b] = i | (wide ? kPosWide : 0);
+                L.used[b] = used;
+                left = true;
+                continue;
+            }
+            int chosen = ~used ? __ffsll((long long)~used) - 1 : -1;
+            if (chosen < 0 || wide) {
+                // some neighbour holds a colour >= 64: first fit over 64-colour windows
+                chosen = -1;
+                for (int base = 0; base < kMaxColours && chosen < 0; base += 64) {
+                    unsigned long long w = 0ull;
+                    for (int j = 0; j < n; ++j) {
+                        const int c = ld_colour(col + nb[j]);
+                        if (c >= base && c < base + 64) w |= 1ull << (c - base);
+                    }
+                    if (~w) chosen = base + __ffsll((long long)~w) - 1;
+                }
+            }
+            if (chosen < 0 || chosen >= kMaxColours) {
+                W.sstate->status = kStatusCapacity;
+                chosen = kMaxColours - 1;
+            }
+            st_colour(col + b, chosen);
+            atomicMax(&cs->maxc, chosen + 1);
+            progress = true;
+        }
+        remaining = left;
+        if (!left) break;
+    }
+    if (__any_sync(0xffffffffu, remaining) && (threadIdx.x & 31) == 0) atomicOr(&flags[0], 1);
+    if (__any_sync(0xffffffffu, progress) && (threadIdx.x & 31) == 0) atomicOr(&flags[1], 1);
+}
+
+// A pass that took more rounds than bodies (cannot happen for a proper
+// priority order) stops the step with TIMEOUT.
+__global__ void k_col_timeout(const __grid_constant__ World W, ColourState* cs) {
+    if (blockIdx.x != 0 || threadIdx.x != 0 || cs->done) return;
+    cs->done = 1;
+    cs->stalled = 1;
+    W.sstate->status = kStatusTimeout;
+}
+
+__global__ void k_col_count(const __grid_constant__ World W, ColourState* cs) {
+    const SceneDesc sc = W.scenes[0];
+    if (cs->skip || cs->stalled) return;
+    AVBD_BODIES(b) {
+        const int c = W.colour[b];
+        if (c >= 0) atomicAdd(&cs->count[c], 1);
+    }
+}
+
+__global__ void k_col_starts(const __grid_constant__ World W, ColourState* cs) {
+    if (cs->skip || cs->stalled || blockIdx.x != 0 || threadIdx.x != 0) return;
+    int* out = W.col_start;   // scene slot 0
+    const int ncol = cs->maxc;
+    int acc = 0;
+    for (int c = 0; c < ncol; ++c) { out[c] = acc; acc += cs->count[c]; cs->count[c] = out[c]; }
+    out[ncol] = acc;
+    W.sstate->ncolours = ncol;
+}
+
+// Colour lists, bodies of more work first within a colour (one launch per
+// work class, so the classes stay in order).
+__global__ void k_col_list(const __grid_constant__ World W, ColourState* cs, int key) {
+    const SceneDesc sc = W.scenes[0];
+    if (cs->skip || cs->stalled) return;
+    const int g = (sc.group > 0 && sc.group <= 32) ? sc.group : 1;
+    AVBD_BODIES(b) {
+        const int c = W.colour[b];
+        if (c < 0) continue;
+        if (min(kColourWorkBuckets - 1, (W.inc_cnt[b] + g - 1) / g) == key)
+            W.col_list[sc.body0 + atomicAdd(&cs->count[c], 1)] = b;
+    }
+}
+
+__global__ void k_col_done(const __grid_constant__ World W, const ColourState* cs) {
+    if (cs->skip || blockIdx.x != 0 || threadIdx.x != 0) return;
+    SceneState* st = W.sstate;
+    st->colours_valid = (!cs->stalled && st->status == kStatusOk) ? 1 : 0;
+    st->coloured_topo = st->topo;
+}
+
+#undef AVBD_BODIES
+#undef AVBD_SLOTS
 
 __global__ void k_predict(const __grid_constant__ World W) {
     const SceneDesc sc = W.scenes[0];
@@ -577,8 +901,15 @@ int upload(AvbdWorld* w) {
     if (cudaGetLastError() != cudaSuccess) return AVBD_ERR_CUDA;
     P.W.P = to_params(w->params);
     GridState* gs = nullptr;
-    if (P.alloc(gs, 1) != cudaSuccess) return AVBD_ERR_NOMEM;
+    ColourState* cs = nullptr;
+    if (P.alloc(gs, 1) != cudaSuccess || P.alloc(cs, 1) != cudaSuccess) return AVBD_ERR_NOMEM;
     w->grid = gs;
+    w->colour = cs;
+    w->nbr_cap = 3 * (size_t)P.ninc;
+    if (P.alloc(w->nbr, w->nbr_cap, false) != cudaSuccess || P.alloc(w->nbr_cnt, (size_t)P.nb) != cudaSuccess ||
+        P.alloc(w->nbr_key, (size_t)P.nb) != cudaSuccess || P.alloc(w->nbr_pos, (size_t)P.nb) != cudaSuccess ||
+        P.alloc(w->nbr_used, (size_t)P.nb) != cudaSuccess)
+        return AVBD_ERR_NOMEM;
     w->uploaded = true;
     return 0;
 }
@@ -601,6 +932,10 @@ int ensure_caps(AvbdWorld* w, int need_cand, int need_k) {
     if (inccap > w->P.ninc) {
         if (w->P.grow(w->P.W.inc, (size_t)w->P.ninc, (size_t)inccap, 0) != cudaSuccess) return AVBD_ERR_NOMEM;
         w->P.ninc = inccap;
+    }
+    if (3 * (size_t)w->P.ninc > w->nbr_cap) {
+        if (w->P.grow(w->nbr, w->nbr_cap, 3 * (size_t)w->P.ninc, 0) != cudaSuccess) return AVBD_ERR_NOMEM;
+        w->nbr_cap = 3 * (size_t)w->P.ninc;
     }
     d.candcap = nc;
     d.kcap = nk;
@@ -682,9 +1017,46 @@ int world_step(AvbdWorld* w) {
         cudaMemcpyAsync(P.d_sstate, &upd, sizeof(SceneState), cudaMemcpyHostToDevice, s);
     }
     if (d.nforce) k_force_init<<<blocks_for(d.nforce), kThreads, 0, s>>>(P.W);
-    // ---- incidence + colouring (one CTA) ----
-    k_incidence_colour<<<1, 1024, 0, s>>>(P.W, cur);
+    // ---- incidence, grid-wide ----
+    const int nb = blocks_for(d.nbody), nc = blocks_for(std::max(ncand, 1));
+    cudaMemsetAsync(P.W.cntB + d.body0, 0, (size_t)d.nbody * sizeof(int), s);
+    k_inc_count_b<<<nc, kThreads, 0, s>>>(P.W, cur);
+    k_inc_count<<<nb, kThreads, 0, s>>>(P.W, cur);
+    k_inc_scan<<<1, 1024, 0, s>>>(P.W);
+    k_inc_fill<<<nb, kThreads, 0, s>>>(P.W, cur);
+    k_inc_fill_b<<<nc, kThreads, 0, s>>>(P.W, cur);
+    k_inc_sort<<<nb, kThreads, 0, s>>>(P.W, cur);
     cudaEventRecord(w->ev[2], s);
+    // ---- colouring, grid-wide (skipped when the contact graph is unchanged) ----
+    {
+        ColourState* cs = static_cast<ColourState*>(w->colour);
+        const ColourLists L{w->nbr, w->nbr_cnt, w->nbr_key, w->nbr_pos, w->nbr_used};
+        k_col_prepare<<<1, 32, 0, s>>>(P.W, cs, cur);
+        k_col_init<<<nb, kThreads, 0, s>>>(P.W, cs, L);
+        // Rounds in chunks of 8; between chunks the host reads whether the
+        // pass has ended (and, after the first, whether colouring is skipped).
+        int flags[2] = {0, 0};   // skip, done
+        for (int pass = 0; pass < 2 && !flags[0]; ++pass) {
+            if (pass == 1) {
+                k_col_repass<<<nb, kThreads, 0, s>>>(P.W, cs);
+                k_col_next_pass<<<1, 32, 0, s>>>(cs);
+            }
+            k_col_pred<<<nb, kThreads, 0, s>>>(P.W, cs, L, cur, pass);
+            int round = 0;
+            flags[1] = 0;
+            while (!flags[1] && round <= d.nbody + 2) {
+                for (int k = 0; k < 8; ++k, ++round) k_jp_round<<<nb, kThreads, 0, s>>>(P.W, cs, L, pass, round);
+                cudaMemcpyAsync(flags, &cs->skip, 2 * sizeof(int), cudaMemcpyDeviceToHost, s);
+                if (cudaStreamSynchronize(s) != cudaSuccess) return AVBD_ERR_CUDA;
+            }
+            if (!flags[1]) k_col_timeout<<<1, 32, 0, s>>>(P.W, cs);
+        }
+        k_col_count<<<nb, kThreads, 0, s>>>(P.W, cs);
+        k_col_starts<<<1, 32, 0, s>>>(P.W, cs);
+        for (int key = kColourWorkBuckets - 1; key >= 0; --key) k_col_list<<<nb, kThreads, 0, s>>>(P.W, cs, key);
+        k_col_done<<<1, 32, 0, s>>>(P.W, cs);
+    }
+    cudaEventRecord(w->ev[3], s);
     if ((r = sync_state(w))) return r;
     if (w->st.status != kStatusOk) return w->st.status == kStatusTimeout ? AVBD_STATUS_TIMEOUT : AVBD_STATUS_CAPACITY;
     const int ncol = w->st.ncolours;
@@ -701,7 +1073,6 @@ int world_step(AvbdWorld* w) {
     w->col_start.resize(ncol + 1);
     cudaMemcpyAsync(w->col_start.data(), P.W.col_start, (ncol + 1) * sizeof(int), cudaMemcpyDeviceToHost, s);
     cudaStreamSynchronize(s);
-    cudaEventRecord(w->ev[3], s);
     // ---- prediction ----
     k_predict<<<blocks_for(d.nbody), kThreads, 0, s>>>(P.W);
     cudaEventRecord(w->ev[4], s);
@@ -751,7 +1122,7 @@ int world_step(AvbdWorld* w) {
     AvbdTimings& t = w->timings;
     t.broad_phase_ms = ev_ms(w->ev[0], w->ev[1]);
     t.warmstart_ms = ev_ms(w->ev[1], w->ev[2]);
-    t.colouring_ms = 0.f;
+    t.colouring_ms = ev_ms(w->ev[2], w->ev[3]);
     t.prediction_ms = ev_ms(w->ev[3], w->ev[4]);
     t.primal_dual_ms = ev_ms(w->ev[4], w->ev[5]);
     t.velocity_update_ms = ev_ms(w->ev[5], w->ev[6]);

@@ -79,6 +79,13 @@ int batch_reserve(AvbdBatch* b, int64_t bodies, int64_t forces, int64_t tets, in
     if (b->d_fail) cudaFree(b->d_fail);
     if (b->d_fix_order) cudaFree(b->d_fix_order);
     if (b->d_fix_n) cudaFree(b->d_fix_n);
+    if (b->d_scene_ns) {   // timing stays on, sized for the new slot count
+        cudaFree(b->d_scene_ns);
+        b->d_scene_ns = nullptr;
+        if (cudaMalloc(&b->d_scene_ns, 2 * std::max<int64_t>(nscenes, 1) * sizeof(unsigned long long)) != cudaSuccess)
+            return AVBD_ERR_NOMEM;
+        cudaMemset(b->d_scene_ns, 0, 2 * std::max<int64_t>(nscenes, 1) * sizeof(unsigned long long));
+    }
     if (cudaMalloc(&b->d_order, std::max<int64_t>(nscenes, 1) * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&b->d_nlive, 2 * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&b->d_queue, 2 * sizeof(int)) != cudaSuccess ||
@@ -389,13 +396,14 @@ int batch_step_listed(AvbdBatch* b, const std::vector<int>& slots) {
     W.fem_team_work = b->fem_team_work;
     W.grid_min = b->grid_min;
     W.fail_count = b->d_fail;
+    W.scene_ns = b->d_scene_ns;
     if (launch_batch_kernel(b, W, b->d_fix_order, b->d_fix_n, b->d_queue) != cudaSuccess) return AVBD_ERR_CUDA;
     return cudaStreamSynchronize(s) == cudaSuccess ? 0 : AVBD_ERR_CUDA;
 }
 
 // After a batched step: scenes a full table stopped get larger tables and
 // take the steps they missed (a few rounds, in case one growth is not enough).
-int batch_fix_capacity(AvbdBatch* b) {
+int batch_fix_capacity(AvbdBatch* b, int64_t* grown_count) {
     const int nslots = (int)b->state.size();
     std::vector<SceneState> hs(nslots);
     for (int round = 0; round < 4; ++round) {
@@ -412,6 +420,7 @@ int batch_fix_capacity(AvbdBatch* b) {
             if (batch_grow_scene(b, i, hs[i]) == 0) grown.push_back(i);
         }
         if (grown.empty()) return 0;
+        if (grown_count) *grown_count += (int64_t)grown.size();
         if (!b->graph) batch_build_graph(b);
         // catch up: every grown scene takes the steps it missed
         for (;;) {
@@ -439,6 +448,7 @@ int batch_build_graph(AvbdBatch* b) {
     b->P.W.fem_team_work = b->fem_team_work;
     b->P.W.grid_min = b->grid_min;
     b->P.W.fail_count = b->d_fail;
+    b->P.W.scene_ns = b->d_scene_ns;
     const cudaError_t launched = launch_batch_kernel(b, b->P.W, b->d_order, b->d_nlive, b->d_queue);
     if (cudaStreamEndCapture(b->stream, &g) != cudaSuccess || launched != cudaSuccess) return AVBD_ERR_CUDA;
     cudaError_t e = cudaGraphInstantiate(&b->graph, g, 0);
@@ -495,6 +505,7 @@ int32_t avbd_batch_destroy(AvbdBatch* b) {
     if (b->d_fail) cudaFree(b->d_fail);
     if (b->d_fix_order) cudaFree(b->d_fix_order);
     if (b->d_fix_n) cudaFree(b->d_fix_n);
+    if (b->d_scene_ns) cudaFree(b->d_scene_ns);
     if (b->e0) cudaEventDestroy(b->e0);
     if (b->e1) cudaEventDestroy(b->e1);
     if (b->stream) cudaStreamDestroy(b->stream);
@@ -756,6 +767,38 @@ int32_t avbd_batch_set_cluster(AvbdBatch* b, int32_t cluster_size, int32_t min_u
     b->cluster_min = min_units;
     b->order_dirty = true;
     return 0;
+}
+
+int32_t avbd_batch_set_scene_timing(AvbdBatch* b, int32_t on) {
+    if (!b) return AVBD_ERR_INVALID;
+    if (int r = batch_settle(b)) return r;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (!on) {
+        if (b->d_scene_ns) cudaFree(b->d_scene_ns);
+        b->d_scene_ns = nullptr;
+    } else if (!b->d_scene_ns) {
+        const size_t n = 2 * (size_t)std::max(b->P.ns, (int)b->state.size()) + 2;
+        if (cudaMalloc(&b->d_scene_ns, n * sizeof(unsigned long long)) != cudaSuccess) return AVBD_ERR_NOMEM;
+        cudaMemset(b->d_scene_ns, 0, n * sizeof(unsigned long long));
+    }
+    b->P.W.scene_ns = b->d_scene_ns;
+    batch_drop_graph(b);
+    return 0;
+}
+
+int32_t avbd_batch_scene_times(AvbdBatch* b, int64_t* start_end_ns, int32_t max_slots) {
+    if (!b || max_slots < 0) return AVBD_ERR_INVALID;
+    if (!start_end_ns) return (int32_t)b->state.size();
+    if (!b->d_scene_ns) return AVBD_ERR_STATE;
+    if (int r = batch_settle(b)) return r;
+    cudaSetDevice(b->device);
+    const int n = std::min(max_slots, (int)b->state.size());
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    if (n > 0 && cudaMemcpy(start_end_ns, b->d_scene_ns, 2 * (size_t)n * sizeof(int64_t), cudaMemcpyDeviceToHost) !=
+                     cudaSuccess)
+        return AVBD_ERR_CUDA;
+    return n;
 }
 
 int32_t avbd_batch_set_grid_broadphase(AvbdBatch* b, int32_t min_bodies) {

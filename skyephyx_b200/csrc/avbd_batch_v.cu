@@ -35,6 +35,20 @@
 namespace avbd {
 namespace {
 
+__device__ __forceinline__ unsigned long long global_ns() {
+    unsigned long long t;
+    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+    return t;
+}
+
+// Runs one scene's step on team T, stamping its start and end when timing is on.
+__device__ __forceinline__ void timed_scene_step(const World& W, int scene, const Team& T) {
+    if (W.scene_ns && T.rank == 0) W.scene_ns[2 * (size_t)scene] = global_ns();
+    scene_step(W, scene, T);
+    T.sync();
+    if (W.scene_ns && T.rank == 0) W.scene_ns[2 * (size_t)scene + 1] = global_ns();
+}
+
 // MAXT is the largest CTA the build serves and MINB sets its register budget
 // (about 65536 / (MAXT * MINB) per thread).  The 256-thread builds keep a
 // step in about 156 (MINB 1), 128, 80 or 64 registers; the 512- and
@@ -74,8 +88,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_batch_step(const __grid_constant
             const int q = C.sh->q;
             C.sync();   // every CTA read the ticket before the next one is drawn
             if (q >= nlarge) break;
-            scene_step(W, order[q], C);
-            C.sync();
+            timed_scene_step(W, order[q], C);
         }
     }
     const int first = clustered ? nlarge : 0;
@@ -96,8 +109,7 @@ __global__ void __launch_bounds__(MAXT, MINB) k_batch_step(const __grid_constant
             if (!lower) scene = -1;
             continue;
         }
-        scene_step(W, scene, T);
-        T.sync();
+        timed_scene_step(W, scene, T);
         scene = -1;
     }
 }

@@ -150,6 +150,8 @@ struct World {
     int fem_team_work;  // the same for scenes with tets (0 = never)
     int grid_min;       // batched kernel: scenes from this many bodies use the grid broadphase (0 = never)
     int* fail_count;    // batched kernel: scene steps stopped by a full table (host grows and catches up)
+    unsigned long long* scene_ns;   // batched kernel, optional: per scene slot the global timer (ns) at the
+                                    // start and end of its last step
     const SceneDesc* scenes;
     SceneState* sstate;
 

@@ -101,10 +101,21 @@ AVBD_HD void predict_body(const World& W, int b) {
 // circumscribed spheres overlap (exact predicate of the reference) and that
 // no live joint/spring links (isConstrainedTo, force.hpp:81-89).
 // ===========================================================================
-AVBD_HD bool pair_constrained(const World& W, int sc_sinc_base, int i, int j) {
-    // static partner list of i: (partner body, force) pairs
-    const int b0 = W.spartner_off[i], b1 = b0 + W.spartner_n[i];
-    for (int k = b0; k < b1; ++k) {
+// Static partner list of body i, (partner body, force) pairs; read once per
+// broadphase row, so a body without joints or springs costs no lookup per pair.
+struct Partners {
+    int off, n;
+};
+AVBD_HD Partners partners_of(const World& W, int i) {
+    Partners p;
+    p.off = W.spartner_off[i];
+    p.n = W.spartner_n[i];
+    return p;
+}
+
+// isConstrainedTo: a live joint or spring of i (partners p) links it to j.
+AVBD_HD bool pair_constrained(const World& W, Partners p, int j) {
+    for (int k = p.off; k < p.off + p.n; ++k) {
         int2 pf = reinterpret_cast<const int2*>(W.spartner)[k];
         if (pf.x == j && !(W.ftype[pf.y] & kForceRemoved)) return true;
     }
@@ -138,11 +149,12 @@ AVBD_HD int broadphase_body(const World& W, const SceneDesc& sc, int i, int2* ou
     const float4 pi = W.pos[i];
     const float ri = W.scale[i].w;
     const int end = sc.body0 + sc.nbody;
+    const Partners pp = partners_of(W, i);
     int n = 0;
     for (int j = i + 1; j < end; ++j) {
         if (W.flags[j] & kBodyRemoved) continue;
         if (!sphere_overlap_fast(pi, W.pos[j], ri, W.scale[j].w)) continue;
-        if (pair_constrained(W, 0, i, j)) continue;
+        if (pair_constrained(W, pp, j)) continue;
         if (out && n < cap) out[n] = make_int2(i, j);
         ++n;
     }
@@ -155,12 +167,13 @@ AVBD_HD int broadphase_body_staged(const World& W, const SceneDesc& sc, int i, c
     const int li = i - sc.body0;
     const float4 pi = sp[li];
     if (isinf(pi.w)) return 0;
+    const Partners pp = partners_of(W, i);
     int n = 0;
     for (int lj = li + 1; lj < sc.nbody; ++lj) {
         const float4 pj = sp[lj];
         if (!sphere_overlap_fast(pi, pj, pi.w, pj.w)) continue;
         const int j = sc.body0 + lj;
-        if (pair_constrained(W, 0, i, j)) continue;
+        if (pair_constrained(W, pp, j)) continue;
         if (out && n < cap) out[n] = make_int2(i, j);
         ++n;
     }

@@ -427,6 +427,26 @@ struct ArenaSink {
         if (n) ops.push_back({static_cast<void*>(dst + at), 0, n * sizeof(T), true});
     }
     void finish() {}
+    // Appends the op table to the arena as ScatterOps (16-byte aligned) and
+    // returns its offset, for a single copy of data and table followed by a
+    // device scatter; -1 if the arena cannot grow.
+    struct ScatterOp {
+        unsigned long long dst, src, bytes;   // src: arena offset; bytes | 1 << 63 for a memset
+    };
+    int64_t append_table() {
+        const size_t off = (used + 15) & ~size_t(15);
+        const size_t n = ops.size() * sizeof(ScatterOp);
+        if (!grow(off + n)) { overflow = true; return -1; }
+        ScatterOp* t = reinterpret_cast<ScatterOp*>(arena + off);
+        for (size_t i = 0; i < ops.size(); ++i) {
+            const Op& o = ops[i];
+            t[i].dst = reinterpret_cast<unsigned long long>(o.dst);
+            t[i].src = o.off;
+            t[i].bytes = (unsigned long long)o.bytes | (o.memset ? (1ull << 63) : 0ull);
+        }
+        used = off + n;
+        return (int64_t)off;
+    }
     // Issues every recorded copy and memset on `st`; returns the bytes copied.
     int64_t issue(cudaStream_t st) const {
         int64_t bytes = 0;
@@ -564,6 +584,14 @@ struct AvbdWorld {
     std::vector<int> col_start;
     avbd::SceneState st{};   // host mirror of the scene counters after the last step
     void* grid = nullptr;     // device scratch of the grid broadphase (avbd_api.cu)
+    void* colour = nullptr;   // device scratch of the grid-wide colouring (avbd_api.cu)
+    // colouring neighbour lists: up to 3 per incidence entry, at 3 x the entry's offset
+    int* nbr = nullptr;
+    int* nbr_cnt = nullptr;
+    unsigned long long* nbr_key = nullptr;   // pass-0 priority of each body
+    int* nbr_pos = nullptr;                  // per body: neighbours scanned this pass
+    unsigned long long* nbr_used = nullptr;  // per body: colours seen so far
+    size_t nbr_cap = 0;
 };
 
 // ===========================================================================
@@ -602,6 +630,7 @@ struct AvbdBatch {
     int cluster_min = 0; // bodies + tets from which a scene is run by a whole cluster
     std::vector<long long> steps_due;   // steps each slot's scene should have taken
     int* d_fail = nullptr;               // scene steps stopped by a full table (device counter)
+    unsigned long long* d_scene_ns = nullptr;   // per-slot step start/end (avbd_batch_set_scene_timing)
     int* d_fix_order = nullptr;          // catch-up queue
     int* d_fix_n = nullptr;
     float last_ms = 0.f;
@@ -633,7 +662,9 @@ int cluster_scenes(const AvbdBatch* b, const std::vector<int>& order);
 cudaError_t launch_batch_kernel(AvbdBatch* b, const World& W, const int* order, const int* nlive, int* queue);
 int batch_build_graph(AvbdBatch* b);
 void batch_sync_order(AvbdBatch* b);
-int batch_fix_capacity(AvbdBatch* b);
+// Grows the scenes a full table stopped and re-runs the steps they missed;
+// `grown` (optional) counts the scenes grown.
+int batch_fix_capacity(AvbdBatch* b, int64_t* grown = nullptr);
 int batch_settle(AvbdBatch* b);
 void batch_drop_graph(AvbdBatch* b);
 

@@ -22,6 +22,7 @@
 #include <cuda_runtime.h>
 
 #include <algorithm>
+#include <chrono>
 #include <deque>
 #include <new>
 #include <vector>
@@ -64,10 +65,15 @@ struct AvbdServer {
     std::vector<ServedRequest> reqs;    // by request id
     std::deque<int> pending;            // request ids waiting for admission, arrival order
     std::vector<int> slot_req;          // request id of each batch slot (-1 free)
+    std::vector<int> live;              // resident slots, largest scene first (ties by slot)
+    std::vector<int> free_slots;        // retired slots, reused before new ones
     std::deque<int> finished;           // request ids ready for avbd_server_poll
     ArenaSink arena[2];                 // upload staging, alternating per tick
     int arena_cur = 0;
+    char* d_stage = nullptr;            // device copy of the upload arena, scattered by k_scatter
+    size_t d_stage_cap = 0;
     float4* rb = nullptr;               // page-locked readback arena
+    std::vector<void*> free_after_step; // page-locked buffers replaced while a step was in flight
     size_t rb_cap = 0;
     SceneState* rb_state = nullptr;     // page-locked scene states of the readbacks
     int rb_state_cap = 0;
@@ -85,23 +91,77 @@ struct AvbdServer {
 
 namespace {
 
-int grow_pinned(void** p, size_t bytes) {
-    if (*p) cudaFreeHost(*p);
+// Replaces a page-locked buffer by a larger one.  The old one may still be
+// the target of a readback in flight; it is freed after the next wait (a
+// free of page-locked memory would wait for the device).
+int grow_pinned(AvbdServer* s, void** p, size_t bytes) {
+    if (*p) s->free_after_step.push_back(*p);
     *p = nullptr;
     if (cudaHostAlloc(p, bytes, cudaHostAllocDefault) != cudaSuccess) return AVBD_ERR_NOMEM;
     return 0;
+}
+
+// The upload arena's copies and memsets, one block per op: bytes from the
+// device copy of the arena (or zeros) to their pool addresses.  Ops are
+// whole 4-byte words (every pool element is 4, 8 or 16 bytes); 16-byte
+// vectors where source, destination and length allow.
+__global__ void k_scatter(const char* stage, const ArenaSink::ScatterOp* ops) {
+    const ArenaSink::ScatterOp o = ops[blockIdx.x];
+    const bool zero = (o.bytes >> 63) != 0;
+    const size_t bytes = (size_t)(o.bytes & ~(1ull << 63));
+    char* dst = reinterpret_cast<char*>(o.dst);
+    const char* src = stage + o.src;
+    const bool v16 = ((o.dst | (zero ? 0ull : reinterpret_cast<unsigned long long>(src)) | bytes) & 15ull) == 0;
+    if (v16) {
+        const size_t n = bytes / 16;
+        float4* d = reinterpret_cast<float4*>(dst);
+        const float4* s = reinterpret_cast<const float4*>(src);
+        for (size_t i = threadIdx.x; i < n; i += blockDim.x) d[i] = zero ? make_float4(0.f, 0.f, 0.f, 0.f) : s[i];
+    } else {
+        const size_t n = bytes / 4;
+        int* d = reinterpret_cast<int*>(dst);
+        const int* s = reinterpret_cast<const int*>(src);
+        for (size_t i = threadIdx.x; i < n; i += blockDim.x) d[i] = zero ? 0 : s[i];
+    }
+}
+
+// Issues the arena on the stream as one copy plus one scatter launch.
+int issue_arena(AvbdServer* s, ArenaSink& a, cudaStream_t st) {
+    if (a.ops.empty()) return 0;
+    const int64_t table = a.append_table();
+    if (table < 0) return AVBD_ERR_NOMEM;
+    if (a.used > s->d_stage_cap) {
+        if (s->d_stage) cudaFree(s->d_stage);   // the previous scatter finished: the step after it was waited for
+        s->d_stage = nullptr;
+        const size_t cap = std::max(a.used, 2 * s->d_stage_cap);
+        if (cudaMalloc(&s->d_stage, cap) != cudaSuccess) { s->d_stage_cap = 0; return AVBD_ERR_NOMEM; }
+        s->d_stage_cap = cap;
+    }
+    cudaMemcpyAsync(s->d_stage, a.arena, a.used, a.pinned ? cudaMemcpyHostToDevice : cudaMemcpyDefault, st);
+    k_scatter<<<(unsigned)a.ops.size(), 256, 0, st>>>(
+        s->d_stage, reinterpret_cast<const ArenaSink::ScatterOp*>(s->d_stage + table));
+    int64_t bytes = 0;
+    for (const auto& o : a.ops) bytes += o.memset ? 0 : (int64_t)o.bytes;
+    s->stats.uploaded_bytes += bytes;
+    return cudaGetLastError() == cudaSuccess ? 0 : AVBD_ERR_CUDA;
+}
+
+// Order of the resident scenes in the queue: largest (bodies + tets) first, ties by slot.
+bool live_before(const AvbdBatch* b, int x, int y) {
+    const SceneDesc& a = b->descs[x];
+    const SceneDesc& c = b->descs[y];
+    const int wa = a.nbody + a.ntet, wc = c.nbody + c.ntet;
+    return wa != wc ? wa > wc : x < y;
 }
 
 // Places a newcomer in the pools and stages its upload; false if it does not fit.
 bool server_admit(AvbdServer* s, int rid, double now) {
     AvbdBatch* b = s->b;
     ServedRequest& r = s->reqs[rid];
-    int slot = -1;
-    for (size_t i = 0; i < b->state.size(); ++i)
-        if (b->state[i] == 0 && s->slot_req[i] < 0) { slot = (int)i; break; }
-    if (slot < 0) {
+    if (s->free_slots.empty()) {
+        // a new slot joins the free list (and stays there if the scene does not fit)
         if ((int)b->state.size() >= b->P.ns) return false;
-        slot = (int)b->state.size();
+        s->free_slots.push_back((int)b->state.size());
         b->scenes.emplace_back();
         b->state.push_back(0);
         b->regions.emplace_back();
@@ -110,12 +170,14 @@ bool server_admit(AvbdServer* s, int rid, double now) {
         b->dynamic.push_back(0);
         s->slot_req.push_back(-1);
     }
+    const int slot = s->free_slots.back();
     const HostScene& h = r.scene;
     int cc, kc, nsinc, nsp;
     scene_caps(h, cc, kc);
     static_counts(h, nsinc, nsp);
     Region reg;
     if (!place_scene(b->A, h, cc, kc, nsinc, nsp, reg)) return false;
+    s->free_slots.pop_back();
     b->regions[slot] = reg;
     upload_scene(b->P, h, static_incidence(h, reg), reg, scene_group(h, b->group_rigid, b->group_fem), slot,
                  b->descs[slot], s->arena[s->arena_cur]);
@@ -126,6 +188,11 @@ bool server_admit(AvbdServer* s, int rid, double now) {
     b->steps_due[slot] = 0;
     b->order_dirty = true;
     s->slot_req[slot] = rid;
+    {
+        const auto pos = std::lower_bound(s->live.begin(), s->live.end(), slot,
+                                          [&](int x, int y) { return live_before(b, x, y); });
+        s->live.insert(pos, slot);
+    }
     r.slot = slot;
     r.admitted = now;
     r.scene = HostScene();   // the device holds it now
@@ -139,12 +206,20 @@ bool server_admit(AvbdServer* s, int rid, double now) {
 int server_complete(AvbdServer* s, double now) {
     if (!s->in_flight) return 0;
     AvbdBatch* b = s->b;
+    using clock = std::chrono::steady_clock;
+    const auto t0 = clock::now();
     if (cudaEventSynchronize(s->step_done) != cudaSuccess) return AVBD_ERR_CUDA;
+    const auto t_wait = clock::now();
+    s->stats.wait_us += std::chrono::duration_cast<std::chrono::microseconds>(t_wait - t0).count();
+    for (void* p : s->free_after_step) cudaFreeHost(p);
+    s->free_after_step.clear();
     s->in_flight = false;
     float ms = 0.f;
     if (cudaEventElapsedTime(&ms, s->step_begin, s->step_end) == cudaSuccess) s->stats.device_us += (int64_t)(ms * 1e3f);
     // scenes a full table stopped grow and catch up before anything reads them
-    if (int r = batch_fix_capacity(b)) return r;
+    const auto t1 = clock::now();
+    if (int r = batch_fix_capacity(b, &s->stats.regrown)) return r;
+    s->stats.catchup_us += std::chrono::duration_cast<std::chrono::microseconds>(clock::now() - t1).count();
     bool refetch = false;
     for (const Readback& rb : s->rb_list)
         if (s->rb_state[rb.state_off].status == kStatusCapacity) refetch = true;
@@ -181,6 +256,12 @@ int server_complete(AvbdServer* s, double now) {
         b->bodies[r.slot] = 0;
         b->dynamic[r.slot] = 0;
         b->order_dirty = true;
+        {
+            const auto pos = std::lower_bound(s->live.begin(), s->live.end(), r.slot,
+                                              [&](int x, int y) { return live_before(b, x, y); });
+            if (pos != s->live.end() && *pos == r.slot) s->live.erase(pos);
+        }
+        s->free_slots.push_back(r.slot);
         s->slot_req[r.slot] = -1;
         s->resident_dynamic -= r.dynamic;
         r.finished = now;
@@ -188,6 +269,7 @@ int server_complete(AvbdServer* s, double now) {
         s->stats.completed += 1;
     }
     s->rb_list.clear();
+    s->stats.retire_us += std::chrono::duration_cast<std::chrono::microseconds>(clock::now() - t_wait).count();
     return 0;
 }
 
@@ -195,20 +277,12 @@ int server_complete(AvbdServer* s, double now) {
 int server_sync_order(AvbdServer* s) {
     AvbdBatch* b = s->b;
     if (!b->order_dirty) return 0;
-    std::vector<int> order;
-    order.reserve(b->state.size());
-    for (size_t i = 0; i < b->state.size(); ++i)
-        if (b->state[i] == 1) order.push_back((int)i);
-    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-        const SceneDesc& a = b->descs[x];
-        const SceneDesc& c = b->descs[y];
-        return (a.nbody + a.ntet) > (c.nbody + c.ntet);
-    });
+    const std::vector<int>& order = s->live;
     const int n = (int)order.size();
     if (n + 2 > s->order_cap) {
-        if (grow_pinned(reinterpret_cast<void**>(&s->order_host), (size_t)(n + 2 + 1024) * sizeof(int)))
-            return AVBD_ERR_NOMEM;
-        s->order_cap = n + 2 + 1024;
+        const int cap = std::max(n + 2 + 1024, s->max_scenes + 2);
+        if (grow_pinned(s, reinterpret_cast<void**>(&s->order_host), (size_t)cap * sizeof(int))) return AVBD_ERR_NOMEM;
+        s->order_cap = cap;
     }
     std::copy(order.begin(), order.end(), s->order_host + 2);
     s->order_host[0] = n;
@@ -258,6 +332,8 @@ int32_t avbd_server_destroy(AvbdServer* s) {
     if (s->step_done) cudaEventDestroy(s->step_done);
     if (s->step_begin) cudaEventDestroy(s->step_begin);
     if (s->step_end) cudaEventDestroy(s->step_end);
+    for (void* p : s->free_after_step) cudaFreeHost(p);
+    if (s->d_stage) cudaFree(s->d_stage);
     if (s->rb) cudaFreeHost(s->rb);
     if (s->rb_state) cudaFreeHost(s->rb_state);
     if (s->order_host) cudaFreeHost(s->order_host);
@@ -299,6 +375,11 @@ int32_t avbd_server_tick(AvbdServer* s, double now_s) {
         if (int r = avbd_batch_reserve(b, nb, nb / 4, 2 * nb, nb / 4, s->max_scenes)) return r;
     }
     if (!b->grid && batch_launch_shape(b)) return AVBD_ERR_CUDA;
+    using clock = std::chrono::steady_clock;
+    auto us_since = [](clock::time_point t) {
+        return (int64_t)std::chrono::duration_cast<std::chrono::microseconds>(clock::now() - t).count();
+    };
+    const auto t_stage = clock::now();
     // 1. admissions staged while the previous step runs
     s->arena_cur ^= 1;
     ArenaSink& arena = s->arena[s->arena_cur];
@@ -310,10 +391,12 @@ int32_t avbd_server_tick(AvbdServer* s, double now_s) {
         ++admitted;
     }
     if (arena.overflow) return AVBD_ERR_NOMEM;
+    s->stats.stage_us += us_since(t_stage);
     // 2. the step in flight and its readbacks
     if (int r = server_complete(s, now_s)) return r;
+    const auto t_issue = clock::now();
     // 3. uploads, order, next step, readbacks of the scenes it finishes
-    s->stats.uploaded_bytes += arena.issue(b->stream);
+    if (int r = issue_arena(s, arena, b->stream)) return r;
     if (int r = server_sync_order(s)) return r;
     if (b->nlive == 0) return 0;
     b->P.W.P = to_params(b->params);
@@ -326,9 +409,8 @@ int32_t avbd_server_tick(AvbdServer* s, double now_s) {
     s->stats.body_iterations += s->resident_dynamic * b->params.num_iterations;
     size_t need = 0;
     int nstate = 0;
-    for (size_t slot = 0; slot < s->slot_req.size(); ++slot) {
+    for (const int slot : s->live) {
         const int rid = s->slot_req[slot];
-        if (rid < 0 || b->state[slot] != 1) continue;
         ServedRequest& r = s->reqs[rid];
         r.taken += 1;
         b->steps_due[slot] += 1;
@@ -344,13 +426,15 @@ int32_t avbd_server_tick(AvbdServer* s, double now_s) {
         }
     }
     if (need > s->rb_cap) {
-        if (grow_pinned(reinterpret_cast<void**>(&s->rb), (need + need / 2) * sizeof(float4))) return AVBD_ERR_NOMEM;
-        s->rb_cap = need + need / 2;
+        const size_t cap = std::max(need + need / 2, 2 * s->rb_cap);
+        if (grow_pinned(s, reinterpret_cast<void**>(&s->rb), cap * sizeof(float4))) return AVBD_ERR_NOMEM;
+        s->rb_cap = cap;
     }
     if (nstate > s->rb_state_cap) {
-        if (grow_pinned(reinterpret_cast<void**>(&s->rb_state), (size_t)(nstate + 256) * sizeof(SceneState)))
+        const int cap = std::max(nstate + 256, 2 * s->rb_state_cap);
+        if (grow_pinned(s, reinterpret_cast<void**>(&s->rb_state), (size_t)cap * sizeof(SceneState)))
             return AVBD_ERR_NOMEM;
-        s->rb_state_cap = nstate + 256;
+        s->rb_state_cap = cap;
     }
     for (const Readback& rb : s->rb_list) {
         const ServedRequest& r = s->reqs[rb.req];
@@ -365,6 +449,7 @@ int32_t avbd_server_tick(AvbdServer* s, double now_s) {
     }
     if (cudaEventRecord(s->step_done, b->stream) != cudaSuccess) return AVBD_ERR_CUDA;
     s->in_flight = true;
+    s->stats.issue_us += us_since(t_issue);
     return b->nlive;
 }
 

@@ -132,7 +132,14 @@ static __device__ int block_exclusive_scan(const Team& T, const int* in, int* ou
 // Incidence (CSR) of one scene: per body
 //   [static forces][manifolds as body B, by slot][manifolds as body A][energies]
 // which follows Mesh::forces then Mesh::energies (solver.cpp:395-435).
+// Static and removed bodies get no entries: nothing solves or colours them,
+// and a ground box touching thousands of boxes would otherwise be one
+// thread's serial work.
 // ---------------------------------------------------------------------------
+__device__ __forceinline__ bool body_fixed(const World& W, int b) {
+    return (W.flags[b] & (kBodyStatic | kBodyRemoved)) != 0;
+}
+
 static __device__ int owned_live(const World& W, int cur, int b, int base_slot) {
     const int c0 = W.cand_off[b] + base_slot, c1 = c0 + W.cand_cnt[b];
     int n = 0;
@@ -170,7 +177,7 @@ static __device__ __noinline__ bool build_incidence(const Team& T, const World& 
     T.sync();
     for (int b = b0 + tid; b < b1; b += nt) {
         const int ns = W.sinc_n[b];
-        W.inc_cnt[b] = ns + W.cntB[b] + owned_live(W, cur, b, sc.cand0);
+        W.inc_cnt[b] = body_fixed(W, b) ? 0 : ns + W.cntB[b] + owned_live(W, cur, b, sc.cand0);
     }
     T.sync();
     const int total = block_exclusive_scan(T, W.inc_cnt + b0, W.inc_off + b0, sc.nbody);
@@ -181,6 +188,8 @@ static __device__ __noinline__ bool build_incidence(const Team& T, const World& 
     for (int b = b0 + tid; b < b1; b += nt) {
         const int off = sc.inc0 + W.inc_off[b];
         W.inc_off[b] = off;
+        W.bcur[b] = 0;
+        if (body_fixed(W, b)) continue;
         const int s0 = W.sinc_off[b], nf = W.sinc_nf[b], ns = W.sinc_n[b];
         int k = off;
         for (int e = 0; e < nf; ++e) W.inc[k++] = W.sinc[s0 + e];
@@ -189,12 +198,12 @@ static __device__ __noinline__ bool build_incidence(const Team& T, const World& 
         for (int c = c0; c < c1; ++c)
             if (W.cn[cur][c] > 0) W.inc[k++] = ent_make(kEntManifold, 0, (uint32_t)c);
         for (int e = nf; e < ns; ++e) W.inc[k++] = W.sinc[s0 + e];
-        W.bcur[b] = 0;
     }
     T.sync();
     for (int c = sc.cand0 + tid; c < sc.cand0 + ncand; c += nt) {
         if (W.cn[cur][c] == 0) continue;
         const int B = W.cpair[cur][c].y;
+        if (body_fixed(W, B)) continue;
         const int p = atomicAdd(&W.bcur[B], 1);
         W.inc[W.inc_off[B] + W.sinc_nf[B] + p] = ent_make(kEntManifold, 1, (uint32_t)c);
     }
@@ -202,6 +211,7 @@ static __device__ __noinline__ bool build_incidence(const Team& T, const World& 
     // order each body's manifolds as Mesh::forces holds them: by creation step,
     // then by pair (creation order within a broadphase pass)
     for (int b = b0 + tid; b < b1; b += nt) {
+        if (body_fixed(W, b)) continue;
         uint32_t* seg = W.inc + W.inc_off[b] + W.sinc_nf[b];
         const int n = W.inc_cnt[b] - W.sinc_n[b];
         sort_manifold_entries(W, cur, seg, n);
@@ -751,10 +761,10 @@ struct GridCells {
 // True when (li, lj), lj > li, is a broadphase candidate: the reference's
 // sphere test and no live joint/spring between them (isConstrainedTo).
 __device__ __forceinline__ bool grid_pair(const World& W, const SceneDesc& sc, const float4* sp, const float4& pi,
-                                          int li, int lj) {
+                                          const Partners& pp, int lj) {
     const float4 pj = body_sphere(W, sc, sp, lj);
     if (!sphere_overlap_fast(pi, pj, pi.w, pj.w)) return false;
-    return !pair_constrained(W, 0, sc.body0 + li, sc.body0 + lj);
+    return !pair_constrained(W, pp, sc.body0 + lj);
 }
 
 // SORTED: the caller visits partners in increasing order, so a candidate is
@@ -762,9 +772,9 @@ __device__ __forceinline__ bool grid_pair(const World& W, const SceneDesc& sc, c
 // emits them.
 template <bool WRITE, bool SORTED = false>
 __device__ __forceinline__ void grid_test(const World& W, const SceneDesc& sc, const float4* sp, const float4& pi,
-                                          int li, int lj, int2* out, int& n) {
+                                          const Partners& pp, int li, int lj, int2* out, int& n) {
     if (lj <= li) return;
-    if (!grid_pair(W, sc, sp, pi, li, lj)) return;
+    if (!grid_pair(W, sc, sp, pi, pp, lj)) return;
     if (WRITE) {
         const int bi = sc.body0 + li, bj = sc.body0 + lj;
         int j = n - 1;
@@ -775,15 +785,53 @@ __device__ __forceinline__ void grid_test(const World& W, const SceneDesc& sc, c
     ++n;
 }
 
+// A big body's all-pairs row by the whole team: each chunk of partners is
+// tested one per thread and its candidates placed by a team-wide count, so
+// the row comes out in partner order (as the all-pairs loop emits it)
+// without one thread walking it.  Returns the row's candidates.
+template <bool WRITE>
+__device__ int big_row(const Team& T, const World& W, const SceneDesc& sc, const float4* sp, int li, int2* out) {
+    const int lane = T.rank & 31, warp = T.rank >> 5, nwarps = T.size >> 5;
+    const float4 pi = body_sphere(W, sc, sp, li);
+    const Partners pp = partners_of(W, sc.body0 + li);
+    if (T.rank == 0) T.sh->carry = 0;
+    T.sync();
+    if (!isinf(pi.w)) {
+        for (int c0 = li + 1; c0 < sc.nbody; c0 += T.size) {
+            const int lj = c0 + T.rank;
+            const bool hit = lj < sc.nbody && grid_pair(W, sc, sp, pi, pp, lj);
+            const unsigned bal = __ballot_sync(kFull, hit);
+            if (lane == 0) T.sh->warp_tot[warp] = __popc(bal);
+            T.sync();
+            int before = T.sh->carry, chunk = 0;
+            for (int w = 0; w < nwarps; ++w) {
+                const int c = T.sh->warp_tot[w];
+                if (w < warp) before += c;
+                chunk += c;
+            }
+            if (WRITE && hit)
+                out[before + __popc(bal & ((1u << lane) - 1u))] = make_int2(sc.body0 + li, sc.body0 + lj);
+            T.sync();
+            if (T.rank == 0) T.sh->carry += chunk;
+            T.sync();
+        }
+    }
+    const int total = T.sh->carry;
+    T.sync();
+    return total;
+}
+
+// Candidates of a small body (big bodies' rows come from big_row).
 template <bool WRITE>
 __device__ __forceinline__ int grid_candidates(const World& W, const SceneDesc& sc, const float4* sp, const GridDims& g,
                                                const GridCells& gc, int li, int2* out) {
     const float4 pi = body_sphere(W, sc, sp, li);
     if (isinf(pi.w)) return 0;
+    const Partners pp = partners_of(W, sc.body0 + li);
     int n = 0;
     if (pi.w > gc.rbig) {
         // a big body: its all-pairs row, in partner order
-        for (int lj = li + 1; lj < sc.nbody; ++lj) grid_test<WRITE, true>(W, sc, sp, pi, li, lj, out, n);
+        for (int lj = li + 1; lj < sc.nbody; ++lj) grid_test<WRITE, true>(W, sc, sp, pi, pp, li, lj, out, n);
         return n;
     }
     const int cx = g.cell_axis(pi.x, g.minx, g.nx), cy = g.cell_axis(pi.y, g.miny, g.ny),
@@ -793,9 +841,9 @@ __device__ __forceinline__ int grid_candidates(const World& W, const SceneDesc& 
             const int row = (z * g.ny + y) * g.nx;
             // the three cells of a row are contiguous in the item list
             const int k0 = gc.cstart[row + max(cx - 1, 0)], k1 = gc.cstart[row + min(cx + 1, g.nx - 1) + 1];
-            for (int k = k0; k < k1; ++k) grid_test<WRITE>(W, sc, sp, pi, li, gc.item(k), out, n);
+            for (int k = k0; k < k1; ++k) grid_test<WRITE>(W, sc, sp, pi, pp, li, gc.item(k), out, n);
         }
-    for (int k = 0; k < gc.nbig; ++k) grid_test<WRITE>(W, sc, sp, pi, li, gc.big[k], out, n);
+    for (int k = 0; k < gc.nbig; ++k) grid_test<WRITE>(W, sc, sp, pi, pp, li, gc.big[k], out, n);
     return n;
 }
 
@@ -901,13 +949,23 @@ static __device__ __noinline__ int broadphase_grid(const Team& T, const World& W
     gc.big = big;
     gc.nbig = nbig;
     gc.rbig = rbig;
+    auto is_big = [&](int li) {
+        const float4 p = body_sphere(W, sc, sp, li);
+        return !isinf(p.w) && p.w > rbig;
+    };
     for (int li = tid; li < n; li += nt)
-        W.cand_cnt[b0 + li] = grid_candidates<false>(W, sc, sp, g, gc, li, nullptr);
+        if (!is_big(li)) W.cand_cnt[b0 + li] = grid_candidates<false>(W, sc, sp, g, gc, li, nullptr);
+    for (int k = 0; k < nbig; ++k) {
+        const int cnt = big_row<false>(T, W, sc, sp, big[k], nullptr);
+        if (tid == 0) W.cand_cnt[b0 + big[k]] = cnt;
+    }
     T.sync();
     const int ncand = block_exclusive_scan(T, W.cand_cnt + b0, W.cand_off + b0, n);
     if (ncand > sc.candcap) return ncand;
     for (int li = tid; li < n; li += nt)
-        grid_candidates<true>(W, sc, sp, g, gc, li, W.cpair[cur] + sc.cand0 + W.cand_off[b0 + li]);
+        if (!is_big(li)) grid_candidates<true>(W, sc, sp, g, gc, li, W.cpair[cur] + sc.cand0 + W.cand_off[b0 + li]);
+    for (int k = 0; k < nbig; ++k)
+        big_row<true>(T, W, sc, sp, big[k], W.cpair[cur] + sc.cand0 + W.cand_off[b0 + big[k]]);
     T.sync();
     return ncand;
 }

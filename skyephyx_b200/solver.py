@@ -441,6 +441,20 @@ class Batch:
         cluster of cluster_size CTAs (1 = off); before stepping."""
         check(self._lib.avbd_batch_set_cluster(self._h, int(cluster_size), int(min_units)), "set_cluster")
 
+    def set_scene_timing(self, on=True):
+        """Per-scene device timing of each step (global timer stamps at the
+        start and end of every scene's step)."""
+        check(self._lib.avbd_batch_set_scene_timing(self._h, 1 if on else 0), "set_scene_timing")
+
+    def scene_times(self):
+        """(slots, 2) int64 array: global-timer ns at the start and end of each
+        slot's last step (0 for slots not stepped since timing was switched on)."""
+        n = check(self._lib.avbd_batch_scene_times(self._h, None, 0), "scene_times")
+        out = np.zeros((max(n, 1), 2), np.int64)
+        k = check(self._lib.avbd_batch_scene_times(self._h, out.ctypes.data_as(C.POINTER(C.c_int64)), n),
+                  "scene_times")
+        return out[:k]
+
     def set_kernel(self, register_variant=1):
         """Build of the persistent kernel: 1..4 for CTAs of up to 256 threads
         (156, 128, 80 or 64 registers), 5/6 for 512 threads, 7 for 1024."""
