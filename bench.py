@@ -114,6 +114,14 @@ class ClockSampler:
 TRAFFIC_PER_DYNAMIC_BODY = 3.386e9 / 432494
 
 
+def autotune_launch(n_scenes):
+    """The tuned launch of the n-scene mix."""
+    from skyephyx_b200 import autotune
+    specs = rank_specs(n_scenes, 0, 1)
+    nfem = sum(1 for sp in specs if sp[0] == "fem")
+    return autotune.lookup(autotune.signature(n_scenes, nfem, n_scenes * 420))
+
+
 def build_batch(specs, config_base=4, tuned=None):
     """Stages every scene and adds it to a Batch with the autotuned launch
     shape for this mix; returns (batch, staged, counts)."""
@@ -281,6 +289,47 @@ def plain_one(key, steps, warmup):
            "dynamic_bodies": s.num_dynamic, "body_iters_per_s": s.num_dynamic * iters / (ms / 1e3),
            "phases_ms": s.timings()}
     s.close()
+    return out
+
+
+PHASES = ["broadphase", "narrowphase", "warm start + incidence", "colouring", "prediction", "iterations",
+          "velocity", "post-stabilisation"]
+
+
+def scene_phases(n_scenes, warmup):
+    """Per-scene device timing of one step of the mix under its tuned launch:
+    mean ms per phase for each scene class (kind x size band), each phase's
+    share of all scene time, and the step's critical path (the scene that
+    ended last)."""
+    specs = rank_specs(n_scenes, 0, 1)
+    batch, staged, counts = build_batch(specs)
+    batch.step(warmup)
+    batch.set_scene_timing(True)
+    batch.step(1)
+    ms = batch.last_ms
+    t = batch.scene_times()[:len(specs)].astype(np.float64)
+    batch.close()
+    kinds = np.array([sp[0] for sp in specs])
+    sizes = np.array([sp[1] for sp in specs])
+    seg = np.diff(t, axis=1) / 1e6                     # (scenes, 8) ms per phase
+    bands = {"rigid 8-127": (kinds != "fem") & (sizes < 128),
+             "rigid 128-511": (kinds != "fem") & (sizes >= 128) & (sizes < 512),
+             "rigid 512-2048": (kinds != "fem") & (sizes >= 512),
+             "fem 500-1999 tets": (kinds == "fem") & (sizes < 2000),
+             "fem 2000-5000 tets": (kinds == "fem") & (sizes >= 2000)}
+    out = {"scenes": len(specs), "step_ms": ms, "launch": counts["launch"], "phases": PHASES, "classes": {}}
+    total = seg.sum()
+    for name, m in bands.items():
+        if m.any():
+            out["classes"][name] = {"scenes": int(m.sum()), "mean_ms": float(seg[m].sum(axis=1).mean()),
+                                    "share_of_scene_time": float(seg[m].sum() / total),
+                                    "phase_mean_ms": [float(x) for x in seg[m].mean(axis=0)]}
+    out["phase_share"] = {p: float(seg[:, i].sum() / total) for i, p in enumerate(PHASES)}
+    last = int(np.argmax(t[:, -1]))
+    out["critical_path"] = {"scene": last, "kind": str(kinds[last]), "size": int(sizes[last]),
+                            "start_ms": float((t[last, 0] - t[:, 0].min()) / 1e6),
+                            "ms": float((t[last, -1] - t[last, 0]) / 1e6),
+                            "span_ms": float((t[:, -1].max() - t[:, 0].min()) / 1e6)}
     return out
 
 
@@ -667,6 +716,10 @@ def main():
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-configs", action="store_true")
     ap.add_argument("--serve-only", action="store_true")
+    ap.add_argument("--only", choices=["fem", "rigid"], default=None,
+                    help="step only the FEM or only the rigid scenes of the mix (profiling)")
+    ap.add_argument("--phases", action="store_true",
+                    help="per-scene, per-phase device time of one step of the mix (scene classes, critical path)")
     ap.add_argument("--plain-config", default=None,
                     help="only the single-scene GPU path of one configuration (C1, C2, C2-stvk, C3): "
                          "wall time per step and per-phase device times")
@@ -683,6 +736,10 @@ def main():
 
     if args.plain_config:
         print(json.dumps(plain_one(args.plain_config, args.steps, args.warmup)))
+        return
+
+    if args.phases:
+        print(json.dumps(scene_phases(args.scenes, args.warmup)))
         return
 
     if args.serve_only:
@@ -702,9 +759,12 @@ def main():
     device = local
 
     specs = rank_specs(args.scenes, rank, ws)
+    if args.only:
+        # a part of the mix, for profiling one kind of scene (not a headline line)
+        specs = [sp for sp in specs if (sp[0] == "fem") == (args.only == "fem")]
 
     t_build = time.perf_counter()
-    batch, staged, counts = build_batch(specs)
+    batch, staged, counts = build_batch(specs, tuned=autotune_launch(args.scenes) if args.only else None)
     build_s = time.perf_counter() - t_build
 
     # ---- e2e: upload from host + steps + per-step pose readback to pinned host memory ----
@@ -801,8 +861,10 @@ def main():
         "metric": METRIC, "value": value, "unit": UNIT, "n_gpus": ws, "steps": args.steps, "warmup": args.warmup,
         "ms_per_step": ms_per_step, "higher_is_better": True, "scaling": "weak", "vs_baseline": None,
         "dtype": "f32", "data": "synthetic (seeded scene generator; no public dataset)",
-        "config": {"workload": f"batched mix: {len(specs)} scenes, box counts log-uniform 8-2048, 25% Neo-Hookean "
-                               f"blocks of 500-5000 tets; dt=1/60, {ITERS} iterations",
+        "config": {"workload": (f"batched mix: {len(specs)} scenes, box counts log-uniform 8-2048, 25% Neo-Hookean "
+                                f"blocks of 500-5000 tets; dt=1/60, {ITERS} iterations") if not args.only else
+                               (f"the {args.only} scenes of the {args.scenes}-scene batched mix ({len(specs)} scenes) "
+                                f"under the whole mix's launch; dt=1/60, {ITERS} iterations"),
                    "scenes": len(specs), "dynamic_bodies": counts["dynamic"], "tets": counts["tets"],
                    "live_contacts": ncontacts, "l2": "working set larger than L2 (126 MB)",
                    "launch": {"threads_per_cta": threads, "ctas_per_sm": ctas,

@@ -341,13 +341,24 @@ int32_t avbd_batch_set_cluster(AvbdBatch* b, int32_t cluster_size, int32_t min_u
  * loop, which smaller scenes keep); 0 = all-pairs everywhere.  Default 128. */
 int32_t avbd_batch_set_grid_broadphase(AvbdBatch* b, int32_t min_bodies);
 /* Per-scene device timing (off by default): each step stamps the GPU's
- * global timer (ns) when a scene's team starts it and when the team is done.
- * avbd_batch_scene_times copies (start, end) of each slot's last step, up
- * to max_slots slots, and returns the slots copied (0, 0 for a slot that has
- * not stepped since timing was switched on); with start_end_ns NULL it
- * returns the number of slots. */
+ * global timer (ns) AVBD_SCENE_STAMPS times per scene: when its team starts
+ * the step, after the broadphase, the narrowphase, the joint/spring warm
+ * start and incidence, the colouring, the prediction, the iterations, the
+ * velocity update and removals, and at the end (post-stabilisation done).
+ * avbd_batch_scene_times copies those stamps of each slot's last step, up to
+ * max_slots slots, and returns the slots copied (zeros for a slot that has
+ * not stepped since timing was switched on; a step that stopped early leaves
+ * its later stamps from the previous step); with stamps_ns NULL it returns
+ * the number of slots. */
+#define AVBD_SCENE_STAMPS 9
+/* Debug builds (libavbd_checks.so, compiled with AVBD_CHECKS): the first
+ * failed device index check of a world / batch as (code, index, bound,
+ * failures); returns 1 and fills out[4] in a debug build, 0 otherwise.  A
+ * failed check skips its access and never traps. */
+int32_t avbd_check_word(const AvbdWorld* w, int32_t out[4]);
+int32_t avbd_batch_check_word(AvbdBatch* b, int32_t out[4]);
 int32_t avbd_batch_set_scene_timing(AvbdBatch* b, int32_t on);
-int32_t avbd_batch_scene_times(AvbdBatch* b, int64_t* start_end_ns, int32_t max_slots);
+int32_t avbd_batch_scene_times(AvbdBatch* b, int64_t* stamps_ns, int32_t max_slots);
 /* Build of the persistent kernel: 1..4 serve CTAs of up to 256 threads with
  * about 156, 128, 80 or 64 registers per thread (spills traded for resident
  * warps); 5 and 6 serve 512 threads (128 or 64 registers), 7 serves 1024

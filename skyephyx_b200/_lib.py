@@ -9,7 +9,8 @@ import ctypes as C
 import os
 
 HERE = os.path.dirname(os.path.abspath(__file__))
-LIB_PATH = os.path.join(HERE, "libavbd.so")
+# AVBD_CHECKS=1 selects the debug build with device index checks
+LIB_PATH = os.path.join(HERE, "libavbd_checks.so" if os.environ.get("AVBD_CHECKS") == "1" else "libavbd.so")
 
 STATUS = {0: "ok", 1: "exploded", 2: "nan", 3: "capacity", 4: "timeout"}
 
@@ -133,6 +134,8 @@ SIGNATURES = [
     ("avbd_batch_set_grid_broadphase", [_V, C.c_int32], C.c_int32),
     ("avbd_batch_set_cluster", [_V, C.c_int32, C.c_int32], C.c_int32),
     ("avbd_batch_set_scene_timing", [_V, C.c_int32], C.c_int32),
+    ("avbd_check_word", [_V, C.POINTER(C.c_int32)], C.c_int32),
+    ("avbd_batch_check_word", [_V, C.POINTER(C.c_int32)], C.c_int32),
     ("avbd_batch_scene_times", [_V, C.POINTER(C.c_int64), C.c_int32], C.c_int32),
     ("avbd_batch_last_ms", [_V], C.c_float),
     ("avbd_batch_set_groups", [_V, C.c_int32, C.c_int32], C.c_int32),
@@ -157,7 +160,7 @@ def load(path: str = LIB_PATH):
         return _lib
     if not os.path.exists(path):
         from . import build as _build
-        _build.build()
+        _build.build(checks=path.endswith("libavbd_checks.so"))
     if not os.path.exists(path):
         raise AvbdError(f"CUDA library not found at {path}; build it with `python -m skyephyx_b200.build`")
     lib = C.CDLL(path)

@@ -1,12 +1,15 @@
 """Builds the in-tree CUDA library ``skyephyx_b200/libavbd.so`` for sm_100a.
 
     python -m skyephyx_b200.build          # or skyephyx_b200.build.build()
+    python -m skyephyx_b200.build --checks # debug build libavbd_checks.so (AVBD_CHECKS)
 
 nvcc compiles device code for ``sm_100a`` only (no PTX for other targets).
 Host code is compiled with ``-ffp-contract=off`` so the scene staging rounds
 exactly like the reference's constructors.  The translation units (the host
 side, and one per build of the batched persistent kernel) compile in
-parallel.
+parallel.  The debug build (checks=True, -DAVBD_CHECKS) adds device index
+checks that record the first violation in a check word instead of trapping
+(avbd_check_word); the loader takes it when AVBD_CHECKS=1 is set.
 """
 from __future__ import annotations
 
@@ -18,6 +21,7 @@ from concurrent.futures import ThreadPoolExecutor
 HERE = os.path.dirname(os.path.abspath(__file__))
 CSRC = os.path.join(HERE, "csrc")
 LIB = os.path.join(HERE, "libavbd.so")
+LIB_CHECKS = os.path.join(HERE, "libavbd_checks.so")
 # (object name, source, extra flags)
 UNITS = [("avbd_api", "avbd_api.cu", []), ("avbd_batch_host", "avbd_batch_host.cu", []),
          ("avbd_server", "avbd_server.cu", []), ("avbd_scene_snapshot", "avbd_scene_snapshot.cu", []),
@@ -42,25 +46,29 @@ def _nvcc() -> str:
     return "nvcc"
 
 
-def _stale() -> bool:
-    if not os.path.exists(LIB):
+def _stale(lib: str = LIB) -> bool:
+    if not os.path.exists(lib):
         return True
-    t = os.path.getmtime(LIB)
+    t = os.path.getmtime(lib)
     deps = [os.path.join(CSRC, f) for f in SOURCES + HEADERS]
     deps.append(os.path.join(HERE, "..", "include", "avbd.h"))
     deps.append(__file__)
     return any(os.path.getmtime(d) > t for d in deps if os.path.exists(d))
 
 
-def build(force: bool = False, verbose: bool = False, csrc: str = CSRC, lib: str = LIB) -> str:
-    """Compiles libavbd.so if any source is newer than it; returns its path."""
-    if not force and lib == LIB and not _stale():
+def build(force: bool = False, verbose: bool = False, csrc: str = CSRC, lib: str = None, checks: bool = False) -> str:
+    """Compiles libavbd.so (libavbd_checks.so with checks=True) if any source
+    is newer than it; returns its path."""
+    lib = lib or (LIB_CHECKS if checks else LIB)
+    if not force and lib in (LIB, LIB_CHECKS) and not _stale(lib):
         return lib
+    flags = ["-DAVBD_CHECKS"] if checks else []
+    tag = "_checks" if checks else ""
 
     def compile_unit(unit):
         name, src, extra = unit
-        obj = os.path.join(csrc, name + ".o")
-        cmd = [_nvcc(), *NVCC_FLAGS, *extra, "-c", os.path.join(csrc, src), "-o", obj]
+        obj = os.path.join(csrc, name + tag + ".o")
+        cmd = [_nvcc(), *NVCC_FLAGS, *flags, *extra, "-c", os.path.join(csrc, src), "-o", obj]
         if verbose:
             print(" ".join(cmd), file=sys.stderr)
         r = subprocess.run(cmd, capture_output=True, text=True)
@@ -90,4 +98,4 @@ def build(force: bool = False, verbose: bool = False, csrc: str = CSRC, lib: str
 
 
 if __name__ == "__main__":
-    print(build(force="--force" in sys.argv, verbose=True))
+    print(build(force="--force" in sys.argv, verbose=True, checks="--checks" in sys.argv))

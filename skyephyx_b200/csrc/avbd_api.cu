@@ -269,7 +269,10 @@ __global__ void k_bp_grid(const __grid_constant__ World W, const GridState* gs, 
                                  : broadphase_body(W, sc, b, nullptr, 0);
         } else {
             int2* out = W.cpair[cur] + sc.cand0 + W.cand_off[b];
-            if (grid) grid_candidates<true>(W, sc, nullptr, g, gc, li, out);
+            if (grid) {
+                const int wrote = grid_candidates<true>(W, sc, nullptr, g, gc, li, out);
+                AVBD_CHECK(W, wrote == W.cand_cnt[b], 3, wrote, W.cand_cnt[b]);
+            }
             else broadphase_body(W, sc, b, out, W.cand_cnt[b]);
         }
     }
@@ -344,6 +347,8 @@ __global__ void k_inc_fill(const __grid_constant__ World W, int cur) {
         W.inc_off[b] = off;
         W.bcur[b] = 0;
         if (body_fixed(W, b)) continue;
+        if (!AVBD_CHECK(W, off + W.inc_cnt[b] <= sc.inc0 + sc.inccap, 1, off + W.inc_cnt[b], sc.inc0 + sc.inccap))
+            continue;
         const int s0 = W.sinc_off[b], nf = W.sinc_nf[b], ns = W.sinc_n[b];
         int k = off;
         for (int e = 0; e < nf; ++e) W.inc[k++] = W.sinc[s0 + e];
@@ -363,6 +368,7 @@ __global__ void k_inc_fill_b(const __grid_constant__ World W, int cur) {
         const int B = W.cpair[cur][c].y;
         if (body_fixed(W, B)) continue;
         const int p = atomicAdd(&W.bcur[B], 1);
+        if (!AVBD_CHECK(W, p < W.cntB[B], 2, p, W.cntB[B])) continue;
         W.inc[W.inc_off[B] + W.sinc_nf[B] + p] = ent_make(kEntManifold, 1, (uint32_t)c);
     }
 }
@@ -610,8 +616,9 @@ __global__ void k_col_list(const __grid_constant__ World W, ColourState* cs, int
     AVBD_BODIES(b) {
         const int c = W.colour[b];
         if (c < 0) continue;
-        if (min(kColourWorkBuckets - 1, (W.inc_cnt[b] + g - 1) / g) == key)
-            W.col_list[sc.body0 + atomicAdd(&cs->count[c], 1)] = b;
+        if (min(kColourWorkBuckets - 1, (W.inc_cnt[b] + g - 1) / g) != key) continue;
+        const int at = atomicAdd(&cs->count[c], 1);
+        if (AVBD_CHECK(W, at >= 0 && at < sc.nbody, 4, at, sc.nbody)) W.col_list[sc.body0 + at] = b;
     }
 }
 
@@ -965,7 +972,10 @@ int world_step(AvbdWorld* w) {
     if (r) return r;
     const int old = w->st.cur, cur = old ^ 1;
     const int old_count = w->st.ncand[old];
+    const Range range("avbd_step");
+    PhaseRanges phases;
     cudaEventRecord(w->ev[0], s);
+    phases.next("broadphase");
     // ---- broadphase: uniform grid from kGridMinBodies bodies, else all pairs ----
     const bool use_grid = d.nbody >= kGridMinBodies;
     GridState* gs = static_cast<GridState*>(w->grid);
@@ -994,6 +1004,7 @@ int world_step(AvbdWorld* w) {
     }
     k_bp_write<<<blocks_for(d.nbody), kThreads, 0, s>>>(P.W, cur, use_grid ? 0 : 1);
     cudaEventRecord(w->ev[1], s);
+    phases.next("narrowphase, warm start, incidence");
     // ---- narrowphase + manifold warm start (re-run after growing the contact pool) ----
     for (int attempt = 0; attempt < 4; ++attempt) {
         k_narrow<<<blocks_for(ncand), kThreads, 0, s>>>(P.W, cur, ncand, old_count);
@@ -1027,6 +1038,7 @@ int world_step(AvbdWorld* w) {
     k_inc_fill_b<<<nc, kThreads, 0, s>>>(P.W, cur);
     k_inc_sort<<<nb, kThreads, 0, s>>>(P.W, cur);
     cudaEventRecord(w->ev[2], s);
+    phases.next("colouring");
     // ---- colouring, grid-wide (skipped when the contact graph is unchanged) ----
     {
         ColourState* cs = static_cast<ColourState*>(w->colour);
@@ -1057,6 +1069,7 @@ int world_step(AvbdWorld* w) {
         k_col_done<<<1, 32, 0, s>>>(P.W, cs);
     }
     cudaEventRecord(w->ev[3], s);
+    phases.next("prediction");
     if ((r = sync_state(w))) return r;
     if (w->st.status != kStatusOk) return w->st.status == kStatusTimeout ? AVBD_STATUS_TIMEOUT : AVBD_STATUS_CAPACITY;
     const int ncol = w->st.ncolours;
@@ -1076,6 +1089,7 @@ int world_step(AvbdWorld* w) {
     // ---- prediction ----
     k_predict<<<blocks_for(d.nbody), kThreads, 0, s>>>(P.W);
     cudaEventRecord(w->ev[4], s);
+    phases.next("iterations");
     // ---- iterations ----
     const float alpha = w->params.alpha;
     const bool has_fracture = d.nforce > 0;
@@ -1094,10 +1108,12 @@ int world_step(AvbdWorld* w) {
         }
     }
     cudaEventRecord(w->ev[5], s);
+    phases.next("velocity");
     // ---- velocities ----
     k_velocity<<<blocks_for(d.nbody), kThreads, 0, s>>>(P.W);
     if ((r = sync_state(w))) return r;
     cudaEventRecord(w->ev[6], s);
+    phases.next("post-stabilisation");
     int status = AVBD_STATUS_OK;
     if (w->st.flags & 1) status = AVBD_STATUS_EXPLODED;
     else if (w->st.flags & 2) status = AVBD_STATUS_NAN;
@@ -1117,6 +1133,7 @@ int world_step(AvbdWorld* w) {
         }
     }
     cudaEventRecord(w->ev[7], s);
+    phases.end();
     if (cudaStreamSynchronize(s) != cudaSuccess) return AVBD_ERR_CUDA;
     if (cudaGetLastError() != cudaSuccess) return AVBD_ERR_CUDA;
     AvbdTimings& t = w->timings;
@@ -1649,6 +1666,19 @@ int32_t avbd_collide(AvbdWorld* w, int32_t a, int32_t b, uint32_t* ids, float* d
     cudaFree(d_data);
     cudaFree(d_n);
     return cudaGetLastError() == cudaSuccess ? n : AVBD_ERR_CUDA;
+}
+
+int32_t avbd_check_word(const AvbdWorld* w, int32_t out[4]) {
+    if (!w || !out) return AVBD_ERR_INVALID;
+#ifdef AVBD_CHECKS
+    for (int i = 0; i < 4; ++i) out[i] = 0;
+    if (!w->uploaded || !w->P.W.check) return 1;
+    cudaSetDevice(w->device);
+    if (w->stream) cudaStreamSynchronize(w->stream);
+    return cudaMemcpy(out, w->P.W.check, 4 * sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess ? 1 : AVBD_ERR_CUDA;
+#else
+    return 0;
+#endif
 }
 
 int32_t avbd_set_group(AvbdWorld* w, int32_t group) {

@@ -82,9 +82,9 @@ int batch_reserve(AvbdBatch* b, int64_t bodies, int64_t forces, int64_t tets, in
     if (b->d_scene_ns) {   // timing stays on, sized for the new slot count
         cudaFree(b->d_scene_ns);
         b->d_scene_ns = nullptr;
-        if (cudaMalloc(&b->d_scene_ns, 2 * std::max<int64_t>(nscenes, 1) * sizeof(unsigned long long)) != cudaSuccess)
-            return AVBD_ERR_NOMEM;
-        cudaMemset(b->d_scene_ns, 0, 2 * std::max<int64_t>(nscenes, 1) * sizeof(unsigned long long));
+        const size_t n = (size_t)kSceneStamps * std::max<int64_t>(nscenes, 1);
+        if (cudaMalloc(&b->d_scene_ns, n * sizeof(unsigned long long)) != cudaSuccess) return AVBD_ERR_NOMEM;
+        cudaMemset(b->d_scene_ns, 0, n * sizeof(unsigned long long));
     }
     if (cudaMalloc(&b->d_order, std::max<int64_t>(nscenes, 1) * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&b->d_nlive, 2 * sizeof(int)) != cudaSuccess ||
@@ -582,6 +582,7 @@ int32_t avbd_batch_prepare(AvbdBatch* b) {
 
 int32_t avbd_batch_step(AvbdBatch* b, int32_t steps) {
     if (!b || steps < 0) return AVBD_ERR_INVALID;
+    const Range range("avbd_batch_step");
     int r;
     if (!b->reserved && (r = batch_stage(b, false))) return r;
     cudaSetDevice(b->device);
@@ -600,7 +601,10 @@ int32_t avbd_batch_step(AvbdBatch* b, int32_t steps) {
     if (cudaGetLastError() != cudaSuccess) return AVBD_ERR_CUDA;
     for (size_t i = 0; i < b->state.size() && i < b->steps_due.size(); ++i)
         if (b->state[i] == 1) b->steps_due[i] += steps;
-    if ((r = batch_fix_capacity(b))) return r;
+    {
+        const Range grow("grow and catch up");
+        if ((r = batch_fix_capacity(b))) return r;
+    }
     return AVBD_STATUS_OK;
 }
 
@@ -778,7 +782,7 @@ int32_t avbd_batch_set_scene_timing(AvbdBatch* b, int32_t on) {
         if (b->d_scene_ns) cudaFree(b->d_scene_ns);
         b->d_scene_ns = nullptr;
     } else if (!b->d_scene_ns) {
-        const size_t n = 2 * (size_t)std::max(b->P.ns, (int)b->state.size()) + 2;
+        const size_t n = (size_t)kSceneStamps * (std::max(b->P.ns, (int)b->state.size()) + 1);
         if (cudaMalloc(&b->d_scene_ns, n * sizeof(unsigned long long)) != cudaSuccess) return AVBD_ERR_NOMEM;
         cudaMemset(b->d_scene_ns, 0, n * sizeof(unsigned long long));
     }
@@ -787,16 +791,32 @@ int32_t avbd_batch_set_scene_timing(AvbdBatch* b, int32_t on) {
     return 0;
 }
 
-int32_t avbd_batch_scene_times(AvbdBatch* b, int64_t* start_end_ns, int32_t max_slots) {
+static_assert(kSceneStamps == AVBD_SCENE_STAMPS, "stamps per scene");
+
+int32_t avbd_batch_check_word(AvbdBatch* b, int32_t out[4]) {
+    if (!b || !out) return AVBD_ERR_INVALID;
+#ifdef AVBD_CHECKS
+    if (int r = batch_settle(b)) return r;
+    for (int i = 0; i < 4; ++i) out[i] = 0;
+    if (!b->P.W.check) return 1;
+    cudaSetDevice(b->device);
+    if (b->stream) cudaStreamSynchronize(b->stream);
+    return cudaMemcpy(out, b->P.W.check, 4 * sizeof(int), cudaMemcpyDeviceToHost) == cudaSuccess ? 1 : AVBD_ERR_CUDA;
+#else
+    return 0;
+#endif
+}
+
+int32_t avbd_batch_scene_times(AvbdBatch* b, int64_t* stamps_ns, int32_t max_slots) {
     if (!b || max_slots < 0) return AVBD_ERR_INVALID;
-    if (!start_end_ns) return (int32_t)b->state.size();
+    if (!stamps_ns) return (int32_t)b->state.size();
     if (!b->d_scene_ns) return AVBD_ERR_STATE;
     if (int r = batch_settle(b)) return r;
     cudaSetDevice(b->device);
     const int n = std::min(max_slots, (int)b->state.size());
     if (b->stream) cudaStreamSynchronize(b->stream);
-    if (n > 0 && cudaMemcpy(start_end_ns, b->d_scene_ns, 2 * (size_t)n * sizeof(int64_t), cudaMemcpyDeviceToHost) !=
-                     cudaSuccess)
+    if (n > 0 && cudaMemcpy(stamps_ns, b->d_scene_ns, (size_t)kSceneStamps * n * sizeof(int64_t),
+                            cudaMemcpyDeviceToHost) != cudaSuccess)
         return AVBD_ERR_CUDA;
     return n;
 }

@@ -35,18 +35,13 @@
 namespace avbd {
 namespace {
 
-__device__ __forceinline__ unsigned long long global_ns() {
-    unsigned long long t;
-    asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
-    return t;
-}
-
-// Runs one scene's step on team T, stamping its start and end when timing is on.
+// Runs one scene's step on team T, stamping its start and end when timing is on
+// (scene_step stamps the phase ends in between).
 __device__ __forceinline__ void timed_scene_step(const World& W, int scene, const Team& T) {
-    if (W.scene_ns && T.rank == 0) W.scene_ns[2 * (size_t)scene] = global_ns();
+    scene_stamp(W, T, scene, 0);
     scene_step(W, scene, T);
     T.sync();
-    if (W.scene_ns && T.rank == 0) W.scene_ns[2 * (size_t)scene + 1] = global_ns();
+    scene_stamp(W, T, scene, kSceneStamps - 1);
 }
 
 // MAXT is the largest CTA the build serves and MINB sets its register budget

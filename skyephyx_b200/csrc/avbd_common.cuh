@@ -50,6 +50,7 @@ constexpr float kNewContactPenaltyMax = 100000.0f;   // manifold.cpp:186
 
 constexpr int kMaxContacts = 8;       // Manifold::contactPoints[8] (force.hpp:172)
 constexpr int kMaxColours = 1024;     // colour slots per scene
+constexpr int kSceneStamps = 9;         // AVBD_SCENE_STAMPS: start, 7 phase ends, end
 constexpr int kColourWorkBuckets = 16; // work classes used to order bodies within a colour
 constexpr int kGroupFlat = 64;         // SceneDesc::group of scenes swept term-per-lane (AVBD_GROUP_FLAT)
 constexpr int kStagedBodies = 2560;    // batched kernel: shared-memory stage of a 256-thread CTA in float4 (40 KB);
@@ -150,8 +151,9 @@ struct World {
     int fem_team_work;  // the same for scenes with tets (0 = never)
     int grid_min;       // batched kernel: scenes from this many bodies use the grid broadphase (0 = never)
     int* fail_count;    // batched kernel: scene steps stopped by a full table (host grows and catches up)
-    unsigned long long* scene_ns;   // batched kernel, optional: per scene slot the global timer (ns) at the
-                                    // start and end of its last step
+    int* check;         // debug builds: first failed index check (code, index, bound) and the failure count
+    unsigned long long* scene_ns;   // batched kernel, optional: per scene slot kSceneStamps global-timer
+                                    // readings (ns) through its last step
     const SceneDesc* scenes;
     SceneState* sstate;
 
@@ -412,6 +414,31 @@ AVBD_HD V3 quaternion_to_rotvec(Q4 q) {
 
 AVBD_HD float clampf(float v, float lo, float hi) { return v < lo ? lo : (hi < v ? hi : v); }
 
+
+// Index checks of debug builds (-DAVBD_CHECKS, skyephyx_b200.build
+// checks=True): a failed check records the first violation (code, index,
+// bound) and counts it in the world's check word, and the caller skips the
+// access; nothing traps.  Release builds compile the checks away.  Codes:
+// 1 / 2 incidence entry (owned / B side) outside the scene's incidence
+// region, 3 a broadphase row wrote another count than it counted, 4 a colour
+// list slot outside the scene's bodies, 5 a tet-term record outside the
+// scene's records, 6 a contact block outside the scene's contact region.
+#if defined(AVBD_CHECKS) && defined(__CUDACC__)
+__device__ __forceinline__ bool avbd_check(const World& W, bool ok, int code, long long index, long long bound) {
+    if (ok) return true;
+    if (W.check) {
+        if (atomicCAS(W.check, 0, code) == 0) {
+            W.check[1] = (int)index;
+            W.check[2] = (int)bound;
+        }
+        atomicAdd(W.check + 3, 1);
+    }
+    return false;
+}
+#define AVBD_CHECK(W, ok, code, index, bound) avbd_check((W), (ok), (code), (long long)(index), (long long)(bound))
+#else
+#define AVBD_CHECK(W, ok, code, index, bound) true
+#endif
 
 AVBD_HD uint32_t colour_priority(uint32_t x) {
     // integer mixer (Wellons "lowbias32"); the CPU colouring twin uses the same function

@@ -214,6 +214,12 @@ AVBD_HD void narrowphase_slot(const World& W, const SceneDesc& sc, SceneState* s
         return;
     }
     const int base = sc.k0 + kofs;
+#ifdef __CUDA_ARCH__
+    if (!AVBD_CHECK(W, kofs >= 0 && kofs + col.n <= sc.kcap, 6, kofs + col.n, sc.kcap)) {
+        W.cn[cur][slot] = 0;
+        return;
+    }
+#endif
     W.kbase[cur][slot] = base;
     W.cn[cur][slot] = col.n;
     const int li = AVBD_ATOMIC_ADD(&st->nlive[cur], 1);

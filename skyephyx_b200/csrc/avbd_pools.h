@@ -3,6 +3,7 @@
 // scene upload, and the AvbdWorld / AvbdBatch handles of include/avbd.h.
 #pragma once
 #include <cuda_runtime.h>
+#include <nvtx3/nvToolsExt.h>
 
 #include <algorithm>
 #include <atomic>
@@ -26,6 +27,31 @@ inline int blocks_for(int n, int threads = kThreads) {
     int b = (n + threads - 1) / threads;
     return std::max(1, std::min(b, 148 * 32));
 }
+
+// A named NVTX range over a scope: phases of the host loops show up on the
+// timeline of an attached profiler (nvtx3 is header-only; without a tool the
+// calls return at once).
+struct Range {
+    explicit Range(const char* name) { nvtxRangePushA(name); }
+    ~Range() { nvtxRangePop(); }
+    Range(const Range&) = delete;
+    Range& operator=(const Range&) = delete;
+};
+
+// Consecutive phases of one loop as NVTX ranges: next() closes the open one.
+struct PhaseRanges {
+    bool open = false;
+    void next(const char* name) {
+        if (open) nvtxRangePop();
+        nvtxRangePushA(name);
+        open = true;
+    }
+    void end() {
+        if (open) nvtxRangePop();
+        open = false;
+    }
+    ~PhaseRanges() { end(); }
+};
 
 inline bool valid_group(int g) { return g == 1 || g == 2 || g == 4 || g == 8 || g == 16 || g == 32; }
 
@@ -107,6 +133,7 @@ struct Pools {
         A(alloc(W.trm2, 4 * (size_t)nt));
         A(alloc(W.ridx, nr)); A(alloc(W.rDmInv, nr)); A(alloc(W.rgradN, 6 * (size_t)nr)); A(alloc(W.rparam, nr));
         A(alloc(W.inc, ninc));
+        A(alloc(W.check, 4));
         for (int t = 0; t < 2; ++t) A(alloc_tables(t, ncand, nk));
 #undef A
         return e;

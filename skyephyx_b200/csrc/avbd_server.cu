@@ -367,6 +367,7 @@ int32_t avbd_server_submit(AvbdServer* s, const AvbdWorld* scene, int32_t steps,
 
 int32_t avbd_server_tick(AvbdServer* s, double now_s) {
     if (!s) return AVBD_ERR_INVALID;
+    const Range range("avbd_server_tick");
     AvbdBatch* b = s->b;
     if (cudaSetDevice(b->device) != cudaSuccess) return AVBD_ERR_CUDA;
     if (!b->reserved) {

@@ -190,6 +190,8 @@ static __device__ __noinline__ bool build_incidence(const Team& T, const World& 
         W.inc_off[b] = off;
         W.bcur[b] = 0;
         if (body_fixed(W, b)) continue;
+        if (!AVBD_CHECK(W, off + W.inc_cnt[b] <= sc.inc0 + sc.inccap, 1, off + W.inc_cnt[b], sc.inc0 + sc.inccap))
+            continue;
         const int s0 = W.sinc_off[b], nf = W.sinc_nf[b], ns = W.sinc_n[b];
         int k = off;
         for (int e = 0; e < nf; ++e) W.inc[k++] = W.sinc[s0 + e];
@@ -205,6 +207,7 @@ static __device__ __noinline__ bool build_incidence(const Team& T, const World& 
         const int B = W.cpair[cur][c].y;
         if (body_fixed(W, B)) continue;
         const int p = atomicAdd(&W.bcur[B], 1);
+        if (!AVBD_CHECK(W, p < W.cntB[B], 2, p, W.cntB[B])) continue;
         W.inc[W.inc_off[B] + W.sinc_nf[B] + p] = ent_make(kEntManifold, 1, (uint32_t)c);
     }
     T.sync();
@@ -500,6 +503,18 @@ __device__ __forceinline__ void primal_colour(const Team& T, const World& W, con
 static __device__ __noinline__ bool colour_scene(const Team& T, const World& W, const SceneDesc& sc, SceneState* st,
                                           int scene, int cur);
 
+// Per-scene device timing (W.scene_ns set): the global timer when the team
+// reaches stamp k of the scene's step (0 start, 1 broadphase done, 2
+// narrowphase, 3 joint/spring warm start and incidence, 4 colouring, 5
+// prediction, 6 iterations, 7 velocities and removals, 8 end).
+__device__ __forceinline__ void scene_stamp(const World& W, const Team& T, int scene, int k) {
+    if (W.scene_ns && T.rank == 0) {
+        unsigned long long t;
+        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t));
+        W.scene_ns[(size_t)kSceneStamps * scene + k] = t;
+    }
+}
+
 // Keeps the previous step's colouring when the contact graph is unchanged:
 // the same number of live manifolds in both tables, every live one already
 // live last step, and no force or body removed since the colouring was made.
@@ -658,7 +673,9 @@ static __device__ __noinline__ bool colour_scene(const Team& T, const World& W, 
             const int c = col[b];
             if (c < 0) continue;
             const int k = min(kColourWorkBuckets - 1, (W.inc_cnt[b] + g - 1) / g);
-            if (k == key) W.col_list[b0 + atomicAdd(&s_count[c], 1)] = b;
+            if (k != key) continue;
+            const int at = atomicAdd(&s_count[c], 1);
+            if (AVBD_CHECK(W, at >= 0 && at < sc.nbody, 4, at, sc.nbody)) W.col_list[b0 + at] = b;
         }
         T.sync();
     }
@@ -676,6 +693,7 @@ static __device__ __noinline__ bool colour_scene(const Team& T, const World& W, 
             const int k = tet_terms(W, b);
             const uint32_t* ent = W.inc + W.inc_off[b] + W.inc_cnt[b] - k;
             const int q0 = tinc[i];
+            if (!AVBD_CHECK(W, q0 + k <= 4 * sc.ntet, 5, q0 + k, 4 * sc.ntet)) continue;
             for (int e = 0; e < k; ++e) write_term_record(W, rec0 + q0 + e, ent[e]);
             tinc[i] = q0 + k;
         }
@@ -962,8 +980,11 @@ static __device__ __noinline__ int broadphase_grid(const Team& T, const World& W
     T.sync();
     const int ncand = block_exclusive_scan(T, W.cand_cnt + b0, W.cand_off + b0, n);
     if (ncand > sc.candcap) return ncand;
-    for (int li = tid; li < n; li += nt)
-        if (!is_big(li)) grid_candidates<true>(W, sc, sp, g, gc, li, W.cpair[cur] + sc.cand0 + W.cand_off[b0 + li]);
+    for (int li = tid; li < n; li += nt) {
+        if (is_big(li)) continue;
+        const int wrote = grid_candidates<true>(W, sc, sp, g, gc, li, W.cpair[cur] + sc.cand0 + W.cand_off[b0 + li]);
+        AVBD_CHECK(W, wrote == W.cand_cnt[b0 + li], 3, wrote, W.cand_cnt[b0 + li]);
+    }
     for (int k = 0; k < nbig; ++k)
         big_row<true>(T, W, sc, sp, big[k], W.cpair[cur] + sc.cand0 + W.cand_off[b0 + big[k]]);
     T.sync();
@@ -1021,6 +1042,7 @@ static __device__ void scene_step(const World& W, int scene, const Team& T) {
     }
     if (tid == 0) { st->kused[cur] = 0; st->nlive[cur] = 0; st->nmatched = 0; }
     T.sync();
+    scene_stamp(W, T, scene, 1);
     // 2. narrowphase + manifold warm start into the other table
     const int old_count = st->ncand[old];
     narrowphase_cta(T, W, sc, st, cur, ncand, old_count);
@@ -1034,6 +1056,7 @@ static __device__ void scene_step(const World& W, int scene, const Team& T) {
         return;
     }
     if (tid == 0) { st->ncand[cur] = ncand; st->cur = cur; }
+    scene_stamp(W, T, scene, 2);
     // 2b. joints / springs warm start
     for (int f = sc.force0 + tid; f < sc.force0 + sc.nforce; f += nt)
         if (force_init(W, f)) atomicAdd(&st->topo, 1);
@@ -1046,14 +1069,17 @@ static __device__ void scene_step(const World& W, int scene, const Team& T) {
         }
         return;
     }
+    scene_stamp(W, T, scene, 3);
     // colouring
     if (!colour_scene_cached(T, W, sc, st, scene, cur)) return;
+    scene_stamp(W, T, scene, 4);
     // 4. prediction
     for (int b = b0 + tid; b < b1; b += nt) predict_body(W, b);
     T.sync();
     const int ncol = st->ncolours;
     const int nlive = st->nlive[cur];
     const int* cs = W.col_start + (size_t)scene * (kMaxColours + 1);
+    scene_stamp(W, T, scene, 5);
     // 5. iterations
     for (int it = 0; it < W.P.num_iterations; ++it) {
         for (int c = 0; c < ncol; ++c) {
@@ -1073,6 +1099,7 @@ static __device__ void scene_step(const World& W, int scene, const Team& T) {
             T.sync();
         }
     }
+    scene_stamp(W, T, scene, 6);
     // 6. velocities, explosion, out of bounds
     if (tid == 0) s_flags = 0;
     T.sync();
@@ -1107,6 +1134,7 @@ static __device__ void scene_step(const World& W, int scene, const Team& T) {
         T.sync();
     }
     if (tid == 0) st->step += 1;
+    scene_stamp(W, T, scene, 7);
     // 7. post-stabilisation
     if (W.P.post_stabilization) {
         for (int c = 0; c < ncol; ++c) {

@@ -446,11 +446,15 @@ class Batch:
         start and end of every scene's step)."""
         check(self._lib.avbd_batch_set_scene_timing(self._h, 1 if on else 0), "set_scene_timing")
 
+    SCENE_STAMPS = 9   # AVBD_SCENE_STAMPS
+
     def scene_times(self):
-        """(slots, 2) int64 array: global-timer ns at the start and end of each
-        slot's last step (0 for slots not stepped since timing was switched on)."""
+        """(slots, 9) int64 array of global-timer ns through each slot's last
+        step: start, after broadphase, narrowphase, warm start + incidence,
+        colouring, prediction, iterations, velocities, end (0 for slots not
+        stepped since timing was switched on)."""
         n = check(self._lib.avbd_batch_scene_times(self._h, None, 0), "scene_times")
-        out = np.zeros((max(n, 1), 2), np.int64)
+        out = np.zeros((max(n, 1), self.SCENE_STAMPS), np.int64)
         k = check(self._lib.avbd_batch_scene_times(self._h, out.ctypes.data_as(C.POINTER(C.c_int64)), n),
                   "scene_times")
         return out[:k]

@@ -409,3 +409,33 @@ def test_cluster_runs_change_nothing():
     for run in runs[1:]:
         for i, (a, c) in enumerate(zip(runs[0], run)):
             assert same(a, c), f"scene {i}"
+
+
+def test_scene_timing_stamps_every_scene_and_changes_nothing():
+    """Per-scene device timing: after a step every slot holds its nine stamps
+    in order (start, the phase ends, end) within one launch, and the results
+    are bitwise those of a batch stepped without timing."""
+    from skyephyx_b200 import Batch
+    builders = mix_builders()
+    runs = []
+    for timed in (False, True):
+        b = Batch()
+        keep = [staged(f) for f in builders]
+        for w in keep:
+            b.add_scene(w)
+        assert b.step(1) == "ok"
+        if timed:
+            b.set_scene_timing(True)
+        assert b.step(2) == "ok"
+        runs.append([b.get_state(i)[:2] for i in range(len(builders))])
+        if timed:
+            t = b.scene_times()
+            assert t.shape == (len(builders), b.SCENE_STAMPS)
+            assert (t[:, 0] > 0).all() and (np.diff(t, axis=1) >= 0).all() and (t[:, -1] > t[:, 0]).all()
+            # the stamps of the last step lie within one launch
+            assert t[:, -1].max() - t[:, 0].min() < 5e9
+            b.set_scene_timing(False)
+            with pytest.raises(Exception):
+                b.scene_times()
+    for i, (a, c) in enumerate(zip(*runs)):
+        assert same(a, c), f"scene {i}"
