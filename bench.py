@@ -716,6 +716,8 @@ def main():
     ap.add_argument("--no-serve", action="store_true")
     ap.add_argument("--no-configs", action="store_true")
     ap.add_argument("--serve-only", action="store_true")
+    ap.add_argument("--launch-scenes", type=int, default=0,
+                    help="run under the tuned launch of the mix of this many scenes (profiling a smaller case)")
     ap.add_argument("--only", choices=["fem", "rigid"], default=None,
                     help="step only the FEM or only the rigid scenes of the mix (profiling)")
     ap.add_argument("--phases", action="store_true",
@@ -764,7 +766,8 @@ def main():
         specs = [sp for sp in specs if (sp[0] == "fem") == (args.only == "fem")]
 
     t_build = time.perf_counter()
-    batch, staged, counts = build_batch(specs, tuned=autotune_launch(args.scenes) if args.only else None)
+    launch_of = args.launch_scenes or (args.scenes if args.only else 0)
+    batch, staged, counts = build_batch(specs, tuned=autotune_launch(launch_of) if launch_of else None)
     build_s = time.perf_counter() - t_build
 
     # ---- e2e: upload from host + steps + per-step pose readback to pinned host memory ----
