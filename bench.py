@@ -109,9 +109,9 @@ class ClockSampler:
 
 
 # DRAM bytes (read + write) per launch per dynamic body: one ncu capture of
-# the 1,024-scene mix of this workload (2.487 GB read + 0.899 GB written over
-# 432,494 dynamic bodies).
-TRAFFIC_PER_DYNAMIC_BODY = 3.386e9 / 432494
+# the 1,024-scene mix of this workload under the 4,096-scene launch (3.197 GB
+# read + 0.875 GB written over 432,494 dynamic bodies).
+TRAFFIC_PER_DYNAMIC_BODY = 4.072e9 / 432494
 
 
 def autotune_launch(n_scenes):
