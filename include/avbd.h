@@ -296,6 +296,13 @@ int32_t avbd_batch_get_state(AvbdBatch* b, int32_t scene, float* pos, float* qua
  * host buffers of max_bodies float4; a scene's bodies start at
  * avbd_batch_scene_body_offset(). */
 int32_t avbd_batch_get_all_poses(AvbdBatch* b, float* pos, float* quat_xyzw, int64_t max_bodies);
+/* The same poses, read back while the next step runs: the call snapshots them
+ * on the device (so avbd_batch_step may follow at once) and returns; the copy
+ * into the host buffers (page-locked for an asynchronous copy) completes by
+ * avbd_batch_read_poses_wait, or before the read after next reuses the
+ * snapshot.  The host buffers must stay valid until then. */
+int32_t avbd_batch_read_poses(AvbdBatch* b, float* pos, float* quat_xyzw, int64_t max_bodies);
+int32_t avbd_batch_read_poses_wait(AvbdBatch* b);
 /* Snapshot of one live scene of a batch (no reference counterpart): every
  * device value of the scene (bodies, forces, energies, both manifold tables
  * and contacts, incidence, colours, counters).  dst may be host or device
@@ -340,6 +347,11 @@ int32_t avbd_batch_set_cluster(AvbdBatch* b, int32_t cluster_size, int32_t min_u
  * uniform grid (the same candidate set and order as the reference's all-pairs
  * loop, which smaller scenes keep); 0 = all-pairs everywhere.  Default 128. */
 int32_t avbd_batch_set_grid_broadphase(AvbdBatch* b, int32_t min_bodies);
+/* The persistent kernel's queue takes scenes in decreasing body_weight x
+ * bodies + tets (default 1: bodies + tets; with clusters always 1), an
+ * estimate of each scene's step time for the largest-first order.
+ * Autotuner knob; results do not depend on it. */
+int32_t avbd_batch_set_queue_weight(AvbdBatch* b, int32_t body_weight);
 /* Per-scene device timing (off by default): each step stamps the GPU's
  * global timer (ns) AVBD_SCENE_STAMPS times per scene: when its team starts
  * the step, after the broadphase, the narrowphase, the joint/spring warm

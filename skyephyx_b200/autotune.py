@@ -39,6 +39,7 @@ SPACE = {
     "team_work": (0, 2, 4, 8),    # scene work per lane below which CTAs split into teams
     "grid_min": (0, 128, 512),    # scenes from this many bodies use the grid broadphase
     "fem_team_work": (0, 4, 8, 16),   # the split threshold for scenes with tets
+    "queue_body_weight": (1, 2, 3, 4),   # queue key: weight x bodies + tets
 }
 
 
@@ -84,6 +85,8 @@ def apply(batch, cfg: dict) -> None:
     batch.set_grid_broadphase(cfg.get("grid_min", 128))
     if cfg.get("cluster", 1) > 1:
         batch.set_cluster(cfg["cluster"], cfg.get("cluster_min", 0))
+    if cfg.get("queue_body_weight", 1) != 1:
+        batch.set_queue_weight(cfg["queue_body_weight"])
 
 
 def candidates(space=SPACE):

@@ -607,12 +607,23 @@ __global__ void k_col_starts(const __grid_constant__ World W, ColourState* cs) {
     W.sstate->ncolours = ncol;
 }
 
+// Lanes per body of a scene with energies when the caller fixed none: from
+// the step's incidence entries per body (a 0.05 m tet block's particles
+// carry about 90, and 32 lanes share them).
+__host__ __device__ __forceinline__ int adaptive_group(int ninc, int nbody) {
+    const int per_body = (ninc + nbody - 1) / max(nbody, 1);
+    return per_body > 48 ? 32 : per_body > 24 ? 16 : 8;
+}
+
 // Colour lists, bodies of more work first within a colour (one launch per
-// work class, so the classes stay in order).
-__global__ void k_col_list(const __grid_constant__ World W, ColourState* cs, int key) {
+// work class, so the classes stay in order).  Work is counted in entries per
+// lane of the lanes-per-body the sweep will use (adaptive: from this step's
+// incidence, as the host picks it after the colouring).
+__global__ void k_col_list(const __grid_constant__ World W, ColourState* cs, int key, int adaptive) {
     const SceneDesc sc = W.scenes[0];
     if (cs->skip || cs->stalled) return;
-    const int g = (sc.group > 0 && sc.group <= 32) ? sc.group : 1;
+    const int g = adaptive ? adaptive_group(W.sstate->ninc, sc.nbody)
+                           : (sc.group > 0 && sc.group <= 32) ? sc.group : 1;
     AVBD_BODIES(b) {
         const int c = W.colour[b];
         if (c < 0) continue;
@@ -1040,6 +1051,7 @@ int world_step(AvbdWorld* w) {
     cudaEventRecord(w->ev[2], s);
     phases.next("colouring");
     // ---- colouring, grid-wide (skipped when the contact graph is unchanged) ----
+    const int adaptive = w->group == 0 && (w->h.ntet() > 0 || w->h.ntri() > 0) && d.nbody > 0;
     {
         ColourState* cs = static_cast<ColourState*>(w->colour);
         const ColourLists L{w->nbr, w->nbr_cnt, w->nbr_key, w->nbr_pos, w->nbr_used};
@@ -1065,7 +1077,7 @@ int world_step(AvbdWorld* w) {
         }
         k_col_count<<<nb, kThreads, 0, s>>>(P.W, cs);
         k_col_starts<<<1, 32, 0, s>>>(P.W, cs);
-        for (int key = kColourWorkBuckets - 1; key >= 0; --key) k_col_list<<<nb, kThreads, 0, s>>>(P.W, cs, key);
+        for (int key = kColourWorkBuckets - 1; key >= 0; --key) k_col_list<<<nb, kThreads, 0, s>>>(P.W, cs, key, adaptive);
         k_col_done<<<1, 32, 0, s>>>(P.W, cs);
     }
     cudaEventRecord(w->ev[3], s);
@@ -1077,11 +1089,7 @@ int world_step(AvbdWorld* w) {
     // Lanes per body: fixed by avbd_set_group, else by the scene kind and,
     // for scenes with energies, by this step's incidence entries per body
     // (a 0.05 m tet block's particles carry about 90: 32 lanes share them).
-    int group = d.group;
-    if (w->group == 0 && (w->h.ntet() > 0 || w->h.ntri() > 0) && d.nbody > 0) {
-        const int per_body = (w->st.ninc + d.nbody - 1) / d.nbody;
-        group = per_body > 48 ? 32 : per_body > 24 ? 16 : 8;
-    }
+    const int group = adaptive ? adaptive_group(w->st.ninc, d.nbody) : d.group;
     w->ncolours = ncol;
     w->col_start.resize(ncol + 1);
     cudaMemcpyAsync(w->col_start.data(), P.W.col_start, (ncol + 1) * sizeof(int), cudaMemcpyDeviceToHost, s);

@@ -142,11 +142,8 @@ void batch_sync_order(AvbdBatch* b) {
     std::vector<int> order;
     for (size_t i = 0; i < b->state.size(); ++i)
         if (b->state[i] == 1) order.push_back((int)i);
-    std::stable_sort(order.begin(), order.end(), [&](int x, int y) {
-        const SceneDesc& a = b->descs[x];
-        const SceneDesc& c = b->descs[y];
-        return (a.nbody + a.ntet) > (c.nbody + c.ntet);
-    });
+    std::stable_sort(order.begin(), order.end(),
+                     [&](int x, int y) { return queue_key(b, b->descs[x]) > queue_key(b, b->descs[y]); });
     b->nlive = (int)order.size();
     const int counts[2] = {b->nlive, cluster_scenes(b, order)};
     if (!order.empty())
@@ -497,6 +494,15 @@ int32_t avbd_batch_destroy(AvbdBatch* b) {
     if (!b) return AVBD_ERR_INVALID;
     cudaSetDevice(b->device);
     if (b->stream) cudaStreamSynchronize(b->stream);
+    if (b->copy_stream) {
+        cudaStreamSynchronize(b->copy_stream);
+        cudaStreamDestroy(b->copy_stream);
+    }
+    for (int k = 0; k < 2; ++k) {
+        if (b->d_pose_snap[k]) cudaFree(b->d_pose_snap[k]);
+        if (b->snap_ev[k]) cudaEventDestroy(b->snap_ev[k]);
+        if (b->read_ev[k]) cudaEventDestroy(b->read_ev[k]);
+    }
     batch_drop_graph(b);
     if (b->upload) b->upload->release();
     if (b->d_order) cudaFree(b->d_order);
@@ -695,6 +701,57 @@ int32_t avbd_batch_get_all_poses(AvbdBatch* b, float* pos, float* quat, int64_t 
     return n;
 }
 
+// Pose readback overlapped with the next step: the poses are copied to a
+// device snapshot on the batch stream (so the next step may change them at
+// once) and from there to the caller's (page-locked) buffers on a copy
+// stream.  Two snapshots alternate; a third read waits for the first's copy.
+int32_t avbd_batch_read_poses(AvbdBatch* b, float* pos, float* quat, int64_t max_bodies) {
+    if (!b || !b->reserved) return AVBD_ERR_STATE;
+    if (int r = batch_settle(b)) return r;
+    cudaSetDevice(b->device);
+    const int64_t n = b->P.nb;
+    if (n > max_bodies) return AVBD_ERR_INVALID;
+    if (!b->copy_stream) {
+        if (cudaStreamCreateWithFlags(&b->copy_stream, cudaStreamNonBlocking) != cudaSuccess) return AVBD_ERR_CUDA;
+        for (int k = 0; k < 2; ++k)
+            if (cudaEventCreateWithFlags(&b->snap_ev[k], cudaEventDisableTiming) != cudaSuccess ||
+                cudaEventCreateWithFlags(&b->read_ev[k], cudaEventDisableTiming) != cudaSuccess)
+                return AVBD_ERR_CUDA;
+    }
+    if (b->pose_snap_n < n) {
+        cudaStreamSynchronize(b->copy_stream);
+        for (int k = 0; k < 2; ++k) {
+            if (b->d_pose_snap[k]) cudaFree(b->d_pose_snap[k]);
+            b->d_pose_snap[k] = nullptr;
+            if (cudaMalloc(&b->d_pose_snap[k], 2 * (size_t)n * sizeof(float4)) != cudaSuccess) {
+                b->pose_snap_n = 0;
+                return AVBD_ERR_NOMEM;
+            }
+        }
+        b->pose_snap_n = n;
+    }
+    const int k = b->pose_snap_cur;
+    b->pose_snap_cur ^= 1;
+    if (cudaEventSynchronize(b->read_ev[k]) != cudaSuccess) return AVBD_ERR_CUDA;   // this snapshot's last read
+    const World& W = b->P.W;
+    float4* snap = b->d_pose_snap[k];
+    cudaMemcpyAsync(snap, W.pos, n * sizeof(float4), cudaMemcpyDeviceToDevice, b->stream);
+    cudaMemcpyAsync(snap + n, W.rot, n * sizeof(float4), cudaMemcpyDeviceToDevice, b->stream);
+    cudaEventRecord(b->snap_ev[k], b->stream);
+    cudaStreamWaitEvent(b->copy_stream, b->snap_ev[k], 0);
+    if (pos) cudaMemcpyAsync(pos, snap, n * sizeof(float4), cudaMemcpyDeviceToHost, b->copy_stream);
+    if (quat) cudaMemcpyAsync(quat, snap + n, n * sizeof(float4), cudaMemcpyDeviceToHost, b->copy_stream);
+    if (cudaEventRecord(b->read_ev[k], b->copy_stream) != cudaSuccess) return AVBD_ERR_CUDA;
+    return (int32_t)n;
+}
+
+int32_t avbd_batch_read_poses_wait(AvbdBatch* b) {
+    if (!b) return AVBD_ERR_INVALID;
+    if (!b->copy_stream) return 0;
+    cudaSetDevice(b->device);
+    return cudaStreamSynchronize(b->copy_stream) == cudaSuccess ? 0 : AVBD_ERR_CUDA;
+}
+
 int32_t avbd_batch_export_instances(AvbdBatch* b, int32_t scene, AvbdInstance* dst, int32_t capacity,
                                     int32_t first_per_model[3], int32_t count_per_model[3]) {
     if (!live_slot(b, scene)) return AVBD_ERR_INVALID;
@@ -819,6 +876,13 @@ int32_t avbd_batch_scene_times(AvbdBatch* b, int64_t* stamps_ns, int32_t max_slo
                             cudaMemcpyDeviceToHost) != cudaSuccess)
         return AVBD_ERR_CUDA;
     return n;
+}
+
+int32_t avbd_batch_set_queue_weight(AvbdBatch* b, int32_t body_weight) {
+    if (!b || body_weight < 1 || body_weight > 64) return AVBD_ERR_INVALID;
+    b->queue_body_weight = body_weight;
+    b->order_dirty = true;
+    return 0;
 }
 
 int32_t avbd_batch_set_grid_broadphase(AvbdBatch* b, int32_t min_bodies) {

@@ -201,10 +201,12 @@ AVBD_HD void vertex_hessian(const M3& U, const M3& V, V3 gradN, float a00, float
     // Scaling modes: sum_k proj(lam_k) w_k w_k^T = M proj(A) M^T with M = [vg0 u0, vg1 u1, vg2 u2]
     // (math.cpp:196-202).  When A is positive definite (all Cholesky pivots > 0) both ABSOLUTE and
     // CLAMP projections leave it unchanged up to the 1e-6 floor, so proj(A) = A needs no eigensolve.
+    // (reciprocal pivots: the test only chooses between two forms of the same matrix)
     const float piv0 = a00;
-    const float l10 = a01 / piv0, l20 = a02 / piv0;
+    const float r0 = fast_rcp(piv0);
+    const float l10 = a01 * r0, l20 = a02 * r0;
     const float piv1 = a11 - l10 * a01;
-    const float l21 = (a12 - l20 * a01) / piv1;
+    const float l21 = (a12 - l20 * a01) * fast_rcp(piv1);
     const float piv2 = a22 - l20 * a02 - l21 * l21 * piv1;
     if (piv0 > 0.f && piv1 > 0.f && piv2 > 0.f) {
         const V3 m0 = vg0 * U.c[0], m1 = vg1 * U.c[1], m2 = vg2 * U.c[2];
@@ -272,7 +274,9 @@ AVBD_HD void neohookean_terms(V3 p0, V3 p1, V3 p2, V3 p3, const float* DmInv, V3
         return;
     }
     const float logJ = logf(J);
-    const float scalar = (lambda * logJ - mu) / J;
+    // one division by J; the other quotients multiply by its reciprocal
+    const float invJ = 1.f / J;
+    const float scalar = (lambda * logJ - mu) * invJ;
     M3 P;
 #pragma unroll
     for (int j = 0; j < 3; ++j) P.c[j] = mu * F.c[j] + scalar * cof.c[j];
@@ -285,13 +289,14 @@ AVBD_HD void neohookean_terms(V3 p0, V3 p1, V3 p2, V3 p3, const float* DmInv, V3
     const float s0 = S.x, s1 = S.y, s2 = S.z;
     float ev[9];
     ev[0] = ev[1] = ev[2] = 0.f;
-    const float dPhi = (lambda * logJ - mu) / J;
+    const float dPhi = scalar;
     ev[3] = mu + dPhi * s2; ev[4] = mu + dPhi * s1; ev[5] = mu + dPhi * s0;
     ev[6] = mu - dPhi * s2; ev[7] = mu - dPhi * s1; ev[8] = mu - dPhi * s0;
     const float diagExtra = mu + lambda * (1.0f - logJ);
     // scaling block A (math.cpp:112-119)
-    const float a00 = mu + diagExtra / (s0 * s0), a11 = mu + diagExtra / (s1 * s1), a22 = mu + diagExtra / (s2 * s2);
-    const float a01 = lambda * s2 / J, a02 = lambda * s1 / J, a12 = lambda * s0 / J;
+    const float a00 = mu + diagExtra * fast_rcp(s0 * s0), a11 = mu + diagExtra * fast_rcp(s1 * s1),
+                a22 = mu + diagExtra * fast_rcp(s2 * s2);
+    const float a01 = lambda * s2 * invJ, a02 = lambda * s1 * invJ, a12 = lambda * s0 * invJ;
     vertex_hessian(U, V, gradN, a00, a11, a22, a01, a02, a12, ev, mode, rho, restVolume, H);
 }
 

@@ -637,13 +637,20 @@ struct AvbdBatch {
     bool reserved = false;           // pools allocated
     avbd::host::Pools P;
     avbd::host::Allocs A;
-    int* d_order = nullptr;          // live slots, largest first
+    int* d_order = nullptr;          // live slots, largest first (queue_key)
+    int queue_body_weight = 1;       // queue key = weight x bodies + tets (avbd_batch_set_queue_weight)
     int* d_nlive = nullptr;
     int* d_queue = nullptr;
     int nlive = 0;
     bool order_dirty = true;
     cudaStream_t stream = nullptr;
     cudaEvent_t e0 = nullptr, e1 = nullptr;
+    // avbd_batch_read_poses: two device snapshots of (pos, rot), read back on a copy stream
+    float4* d_pose_snap[2] = {nullptr, nullptr};
+    int64_t pose_snap_n = 0;
+    int pose_snap_cur = 0;
+    cudaStream_t copy_stream = nullptr;
+    cudaEvent_t snap_ev[2] = {nullptr, nullptr}, read_ev[2] = {nullptr, nullptr};
     cudaGraphExec_t graph = nullptr;
     int threads = 0, ctas_per_sm = 0;   // 0 = automatic
     int group_rigid = 4, group_fem = 8;  // lanes per body in the primal sweep
@@ -668,6 +675,13 @@ struct AvbdBatch {
     bool upload_pinned = false;   // the staging buffers are page-locked
     int64_t uploaded_bytes = 0;   // host-to-device bytes of the last staged upload
 };
+
+// Queue order of a scene: estimated work, largest first.  With clusters the
+// key stays bodies + tets, the unit of the cluster threshold.
+inline int64_t queue_key(const AvbdBatch* b, const avbd::SceneDesc& d) {
+    const int64_t w = b->cluster > 1 ? 1 : b->queue_body_weight;
+    return w * d.nbody + d.ntet;
+}
 
 namespace avbd {
 namespace host {

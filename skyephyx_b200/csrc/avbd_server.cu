@@ -66,6 +66,7 @@ struct AvbdServer {
     std::deque<int> pending;            // request ids waiting for admission, arrival order
     std::vector<int> slot_req;          // request id of each batch slot (-1 free)
     std::vector<int> live;              // resident slots, largest scene first (ties by slot)
+    int64_t live_weight = 1;            // queue weight the live order was made with
     std::vector<int> free_slots;        // retired slots, reused before new ones
     std::deque<int> finished;           // request ids ready for avbd_server_poll
     ArenaSink arena[2];                 // upload staging, alternating per tick
@@ -146,11 +147,9 @@ int issue_arena(AvbdServer* s, ArenaSink& a, cudaStream_t st) {
     return cudaGetLastError() == cudaSuccess ? 0 : AVBD_ERR_CUDA;
 }
 
-// Order of the resident scenes in the queue: largest (bodies + tets) first, ties by slot.
+// Order of the resident scenes in the queue: largest queue_key first, ties by slot.
 bool live_before(const AvbdBatch* b, int x, int y) {
-    const SceneDesc& a = b->descs[x];
-    const SceneDesc& c = b->descs[y];
-    const int wa = a.nbody + a.ntet, wc = c.nbody + c.ntet;
+    const int64_t wa = queue_key(b, b->descs[x]), wc = queue_key(b, b->descs[y]);
     return wa != wc ? wa > wc : x < y;
 }
 
@@ -368,6 +367,16 @@ int32_t avbd_server_submit(AvbdServer* s, const AvbdWorld* scene, int32_t steps,
 int32_t avbd_server_tick(AvbdServer* s, double now_s) {
     if (!s) return AVBD_ERR_INVALID;
     const Range range("avbd_server_tick");
+    {
+        // a queue weight set since the live order was made: order again
+        const int64_t w = s->b->cluster > 1 ? 1 : s->b->queue_body_weight;
+        if (w != s->live_weight) {
+            s->live_weight = w;
+            AvbdBatch* b = s->b;
+            std::sort(s->live.begin(), s->live.end(), [&](int x, int y) { return live_before(b, x, y); });
+            b->order_dirty = true;
+        }
+    }
     AvbdBatch* b = s->b;
     if (cudaSetDevice(b->device) != cudaSuccess) return AVBD_ERR_CUDA;
     if (!b->reserved) {

@@ -199,6 +199,9 @@ class _BatchKnobs:
     def set_cluster(self, cluster_size, min_units):
         check(self._lib.avbd_batch_set_cluster(self._h, int(cluster_size), int(min_units)), "set_cluster")
 
+    def set_queue_weight(self, body_weight):
+        check(self._lib.avbd_batch_set_queue_weight(self._h, int(body_weight)), "set_queue_weight")
+
     def set_grid_broadphase(self, min_bodies):
         check(self._lib.avbd_batch_set_grid_broadphase(self._h, int(min_bodies)), "set_grid_broadphase")
 

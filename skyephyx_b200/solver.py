@@ -441,6 +441,10 @@ class Batch:
         cluster of cluster_size CTAs (1 = off); before stepping."""
         check(self._lib.avbd_batch_set_cluster(self._h, int(cluster_size), int(min_units)), "set_cluster")
 
+    def set_queue_weight(self, body_weight=1):
+        """Queue order key: body_weight x bodies + tets, largest first."""
+        check(self._lib.avbd_batch_set_queue_weight(self._h, int(body_weight)), "set_queue_weight")
+
     def set_scene_timing(self, on=True):
         """Per-scene device timing of each step (global timer stamps at the
         start and end of every scene's step)."""

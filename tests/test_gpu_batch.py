@@ -439,3 +439,40 @@ def test_scene_timing_stamps_every_scene_and_changes_nothing():
                 b.scene_times()
     for i, (a, c) in enumerate(zip(*runs)):
         assert same(a, c), f"scene {i}"
+
+
+def test_overlapped_pose_readback_equals_synchronous():
+    """avbd_batch_read_poses (device snapshot, copy on a second stream while
+    the next step runs) delivers each step's poses exactly as the
+    synchronous avbd_batch_get_all_poses read right after that step."""
+    import ctypes as C
+    from skyephyx_b200 import Batch
+    b = Batch()
+    keep = [staged(f) for f in mix_builders()[:4]]
+    for w in keep:
+        b.add_scene(w)
+    assert b.step(1) == "ok"
+    lib, h = b._lib, b._h
+    n = lib.avbd_batch_get_all_poses(h, None, None, 1 << 30)
+    fp = C.POINTER(C.c_float)
+    sync = []
+    for _ in range(3):
+        p, q = np.zeros((n, 4), np.float32), np.zeros((n, 4), np.float32)
+        assert lib.avbd_batch_get_all_poses(h, p.ctypes.data_as(fp), q.ctypes.data_as(fp), n) == n
+        sync.append((p, q))
+        assert b.step(1) == "ok"
+    # the same three steps again, from the same start, read with overlap
+    b2 = Batch()
+    keep2 = [staged(f) for f in mix_builders()[:4]]
+    for w in keep2:
+        b2.add_scene(w)
+    assert b2.step(1) == "ok"
+    bufs = [(np.zeros((n, 4), np.float32), np.zeros((n, 4), np.float32)) for _ in range(3)]
+    for k in range(3):
+        p, q = bufs[k]
+        assert b2._lib.avbd_batch_read_poses(b2._h, p.ctypes.data_as(fp), q.ctypes.data_as(fp), n) == n
+        assert b2.step(1) == "ok"
+    assert b2._lib.avbd_batch_read_poses_wait(b2._h) == 0
+    for (p, q), (ps, qs) in zip(bufs, sync):
+        assert np.array_equal(p.view(np.uint32), ps.view(np.uint32))
+        assert np.array_equal(q.view(np.uint32), qs.view(np.uint32))
