@@ -347,8 +347,10 @@ __global__ void k_inc_fill(const __grid_constant__ World W, int cur) {
         W.inc_off[b] = off;
         W.bcur[b] = 0;
         if (body_fixed(W, b)) continue;
-        if (!AVBD_CHECK(W, off + W.inc_cnt[b] <= sc.inc0 + sc.inccap, 1, off + W.inc_cnt[b], sc.inc0 + sc.inccap))
+        if (!AVBD_CHECK(W, off + W.inc_cnt[b] <= sc.inc0 + sc.inccap, 1, off + W.inc_cnt[b], sc.inc0 + sc.inccap)) {
+            W.inc_cnt[b] = 0;   // readers then see no entries rather than unwritten ones
             continue;
+        }
         const int s0 = W.sinc_off[b], nf = W.sinc_nf[b], ns = W.sinc_n[b];
         int k = off;
         for (int e = 0; e < nf; ++e) W.inc[k++] = W.sinc[s0 + e];
