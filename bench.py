@@ -112,6 +112,12 @@ class ClockSampler:
 # the 1,024-scene mix of this workload under the 4,096-scene launch (3.197 GB
 # read + 0.875 GB written over 432,494 dynamic bodies).
 TRAFFIC_PER_DYNAMIC_BODY = 4.072e9 / 432494
+# FMA-pipe and DRAM utilisation of the FEM work: one ncu capture of the FEM
+# blocks of the 1,024-scene mix under the benchmark launch (FMA pipe cycles
+# active, of active cycles: mean over SMs and the busiest SM; DRAM throughput
+# of peak over the launch).
+FEM_PIPES = {"fma_pipe_mean": 0.252, "fma_pipe_busiest_sm": 0.959, "dram_throughput": 0.023,
+             "source": "ncu of bench.py --scenes 1024 --only fem --launch-scenes 4096"}
 
 
 def autotune_launch(n_scenes):
@@ -904,7 +910,10 @@ def main():
                      "traffic": TRAFFIC_PER_DYNAMIC_BODY * counts["dynamic"],
                      "traffic_note": "DRAM read+write bytes per launch from one ncu capture of the 1,024-scene "
                                      "mix, scaled by dynamic bodies", "peak_kind": peak_kind,
-                     "algorithmic_bytes_per_launch": alg_bytes},
+                     "algorithmic_bytes_per_launch": alg_bytes,
+                     # the FEM scenes alone (one ncu capture of the mix's FEM blocks under its launch):
+                     # FP32-bound where they run, far from the HBM bound
+                     "fem": FEM_PIPES},
         "clocks": clk,
         "served": served,
         "cpu_baseline": cpu,

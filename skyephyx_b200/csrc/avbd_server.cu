@@ -66,6 +66,12 @@ struct AvbdServer {
     std::deque<int> pending;            // request ids waiting for admission, arrival order
     std::vector<int> slot_req;          // request id of each batch slot (-1 free)
     std::vector<int> live;              // resident slots, largest scene first (ties by slot)
+    // per slot, what a tick needs of its request (compact: the tick loop
+    // touches every resident scene)
+    struct SlotRun {
+        int rid = -1, taken = 0, steps = 0, flags = 0, nbody = 0;
+    };
+    std::vector<SlotRun> run;
     int64_t live_weight = 1;            // queue weight the live order was made with
     std::vector<int> free_slots;        // retired slots, reused before new ones
     std::deque<int> finished;           // request ids ready for avbd_server_poll
@@ -187,6 +193,8 @@ bool server_admit(AvbdServer* s, int rid, double now) {
     b->steps_due[slot] = 0;
     b->order_dirty = true;
     s->slot_req[slot] = rid;
+    if ((int)s->run.size() <= slot) s->run.resize(slot + 1);
+    s->run[slot] = AvbdServer::SlotRun{rid, 0, r.steps, r.flags, r.nbody};
     {
         const auto pos = std::lower_bound(s->live.begin(), s->live.end(), slot,
                                           [&](int x, int y) { return live_before(b, x, y); });
@@ -420,18 +428,18 @@ int32_t avbd_server_tick(AvbdServer* s, double now_s) {
     size_t need = 0;
     int nstate = 0;
     for (const int slot : s->live) {
-        const int rid = s->slot_req[slot];
-        ServedRequest& r = s->reqs[rid];
-        r.taken += 1;
+        AvbdServer::SlotRun& q = s->run[slot];
+        q.taken += 1;
         b->steps_due[slot] += 1;
-        const bool final = r.taken >= r.steps;
-        const bool first = r.taken == 1 && (r.flags & AVBD_SERVE_KEEP_FIRST);
+        const bool final = q.taken >= q.steps;
+        const bool first = q.taken == 1 && (q.flags & AVBD_SERVE_KEEP_FIRST);
         if (final || first) {
-            s->rb_list.push_back({rid, final, need, r.nbody, nstate});
-            need += 2 * (size_t)r.nbody;
+            s->reqs[q.rid].taken = q.taken;
+            s->rb_list.push_back({q.rid, final, need, q.nbody, nstate});
+            need += 2 * (size_t)q.nbody;
             ++nstate;
             if (final && first) {   // a one-step request: the same poses serve both
-                s->rb_list.push_back({rid, false, need - 2 * (size_t)r.nbody, r.nbody, nstate - 1});
+                s->rb_list.push_back({q.rid, false, need - 2 * (size_t)q.nbody, q.nbody, nstate - 1});
             }
         }
     }
