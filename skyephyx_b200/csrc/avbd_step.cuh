@@ -1,8 +1,10 @@
-// Step drivers.  Block-cooperative functions (scans, incidence build,
-// Jones-Plassmann colouring, colour lists) run on one CTA per scene; the
-// persistent batched kernel strings every phase of a scene's step together on
-// one CTA, and the single-scene path launches the same per-item functions as
-// grid-wide kernels between them.
+// Step drivers of the batched path.  Team-cooperative functions (scans,
+// incidence build, Jones-Plassmann colouring, colour lists) run on the team
+// (a CTA, part of one, or a thread-block cluster) that owns a scene; the
+// persistent batched kernel strings every phase of a scene's step together
+// on that team.  The single-scene path (avbd_api.cu) launches the same
+// per-item functions as grid-wide kernels, with grid-wide counterparts of the
+// team functions.
 #pragma once
 #include <cooperative_groups.h>
 

@@ -101,6 +101,27 @@ def test_c2_full_size_one_step(oracle_mod, Solver, model):
     assert r.max() <= C2_ROT_TAIL, f"max rotation error {r.max():.3g} rad"
 
 
+def test_c3_full_size_one_step(oracle_mod, Solver):
+    """The configuration's large mixed scene at full size (32,768 boxes in a
+    5-box container, 64 hinge chains of 32 links, 2,048 springs; the grid
+    broadphase on the device, the reference's all-pairs loop in the oracle):
+    candidate manifolds and colours bit-exact, poses within 1e-4."""
+    o = oracle_mod.OracleSolver(iterations=10)
+    g = Solver(iterations=10)
+    scenes.mixed_large(o)
+    scenes.mixed_large(g)
+    assert o.step_coloured() == 0
+    assert g.step() == "ok"
+    assert contact_ids(o.contacts()) == contact_ids(g.contacts())
+    (col_o, nco), (col_g, ncg) = o.colours(), g.colours()
+    assert nco == ncg and np.array_equal(col_o, col_g)
+    po, qo = o.get_state()[:2]
+    pg, qg = g.get_state()[:2]
+    assert np.abs(po - pg).max() <= POS_TOL
+    assert rot_err(qo, qg).max() <= ROT_TOL
+    g.close()
+
+
 @pytest.mark.parametrize("name", ["pyramid_wall_210", "joint_playground", "cloth", "mixed_small", "soft_beam",
                                   "stvk_beam"])
 def test_ten_steps_close(oracle_mod, Solver, name):
