@@ -109,14 +109,14 @@ class ClockSampler:
 
 
 # DRAM bytes (read + write) per launch per dynamic body: one ncu capture of
-# the 1,024-scene mix of this workload under the 4,096-scene launch (3.197 GB
-# read + 0.875 GB written over 432,494 dynamic bodies).
-TRAFFIC_PER_DYNAMIC_BODY = 4.072e9 / 432494
+# the 1,024-scene mix of this workload under the 4,096-scene launch (3.087 GB
+# read + 0.831 GB written over 432,494 dynamic bodies).
+TRAFFIC_PER_DYNAMIC_BODY = 3.918e9 / 432494
 # FMA-pipe and DRAM utilisation of the FEM work: one ncu capture of the FEM
 # blocks of the 1,024-scene mix under the benchmark launch (FMA pipe cycles
 # active, of active cycles: mean over SMs and the busiest SM; DRAM throughput
 # of peak over the launch).
-FEM_PIPES = {"fma_pipe_mean": 0.252, "fma_pipe_busiest_sm": 0.959, "dram_throughput": 0.023,
+FEM_PIPES = {"fma_pipe_mean": 0.263, "fma_pipe_busiest_sm": 1.0, "dram_throughput": 0.023,
              "source": "ncu of bench.py --scenes 1024 --only fem --launch-scenes 4096"}
 
 
