@@ -194,13 +194,20 @@ AVBD_HD void s3_add_outer(S3& h, float lam, V3 w) {
 // (NeoHookeanMath::ReconstructVertexHessian, math.cpp:196-231): the scaling
 // block a.. (3x3, symmetric) and the twist / flip eigenvalues ev[3..8]
 // (ev[0..2] are filled here), each mode contracted with V^T gradN.
+// Every mode vector lies in the span of U's columns, so the sum of the
+// rank-one terms is assembled as a 3x3 K in U's basis and turned once into
+// H = restVolume U K U^T (the same matrix, with a third of the multiplies of
+// summing nine outer products in world coordinates).  With g = V^T gradN:
+//   scaling modes: K = diag(g) proj(A) diag(g);
+//   twist / flip (i, j), vectors (g_j e_i -+ g_i e_j) / sqrt 2:
+//     K_ii += (l_t + l_f) g_j^2 / 2, K_jj += (l_t + l_f) g_i^2 / 2,
+//     K_ij += (l_f - l_t) g_i g_j / 2.
 AVBD_HD void vertex_hessian(const M3& U, const M3& V, V3 gradN, float a00, float a11, float a22, float a01, float a02,
                             float a12, float (&ev)[9], int mode, float rho, float restVolume, S3& H) {
-    const float vg0 = dot(V.c[0], gradN), vg1 = dot(V.c[1], gradN), vg2 = dot(V.c[2], gradN);
-    s3_zero(H);
-    // Scaling modes: sum_k proj(lam_k) w_k w_k^T = M proj(A) M^T with M = [vg0 u0, vg1 u1, vg2 u2]
-    // (math.cpp:196-202).  When A is positive definite (all Cholesky pivots > 0) both ABSOLUTE and
-    // CLAMP projections leave it unchanged up to the 1e-6 floor, so proj(A) = A needs no eigensolve.
+    const float g0 = dot(V.c[0], gradN), g1 = dot(V.c[1], gradN), g2 = dot(V.c[2], gradN);
+    float k00, k11, k22, k01, k02, k12;
+    // Scaling modes: when A is positive definite (all Cholesky pivots > 0) both ABSOLUTE and CLAMP
+    // projections leave it unchanged up to the 1e-6 floor, so proj(A) = A needs no eigensolve.
     // (reciprocal pivots: the test only chooses between two forms of the same matrix)
     const float piv0 = a00;
     const float r0 = fast_rcp(piv0);
@@ -209,17 +216,8 @@ AVBD_HD void vertex_hessian(const M3& U, const M3& V, V3 gradN, float a00, float
     const float l21 = (a12 - l20 * a01) * fast_rcp(piv1);
     const float piv2 = a22 - l20 * a02 - l21 * l21 * piv1;
     if (piv0 > 0.f && piv1 > 0.f && piv2 > 0.f) {
-        const V3 m0 = vg0 * U.c[0], m1 = vg1 * U.c[1], m2 = vg2 * U.c[2];
-        // B = M A (columns), H += B M^T
-        const V3 b0 = a00 * m0 + a01 * m1 + a02 * m2;
-        const V3 b1 = a01 * m0 + a11 * m1 + a12 * m2;
-        const V3 b2 = a02 * m0 + a12 * m1 + a22 * m2;
-        H.xx += b0.x * m0.x + b1.x * m1.x + b2.x * m2.x;
-        H.yy += b0.y * m0.y + b1.y * m1.y + b2.y * m2.y;
-        H.zz += b0.z * m0.z + b1.z * m1.z + b2.z * m2.z;
-        H.xy += b0.y * m0.x + b1.y * m1.x + b2.y * m2.x;
-        H.xz += b0.z * m0.x + b1.z * m1.x + b2.z * m2.x;
-        H.yz += b0.z * m0.y + b1.z * m1.y + b2.z * m2.y;
+        k00 = a00 * (g0 * g0); k11 = a11 * (g1 * g1); k22 = a22 * (g2 * g2);
+        k01 = a01 * (g0 * g1); k02 = a02 * (g0 * g2); k12 = a12 * (g1 * g2);
         project_eigenvalues<6>(ev + 3, mode, rho);
     } else {
         V3 w;
@@ -227,22 +225,42 @@ AVBD_HD void vertex_hessian(const M3& U, const M3& V, V3 gradN, float a00, float
         eig3(a00, a11, a22, a01, a02, a12, w, Q);
         ev[0] = w.x; ev[1] = w.y; ev[2] = w.z;
         project_eigenvalues<9>(ev, mode, rho);
+        k00 = k11 = k22 = k01 = k02 = k12 = 0.f;
 #pragma unroll
         for (int k = 0; k < 3; ++k) {
-            V3 c = Q.c[k];
-            V3 ww = (c.x * vg0) * U.c[0] + (c.y * vg1) * U.c[1] + (c.z * vg2) * U.c[2];
-            s3_add_outer(H, ev[k], ww);
+            const float c0 = Q.c[k].x * g0, c1 = Q.c[k].y * g1, c2 = Q.c[k].z * g2;
+            const float l = ev[k];
+            k00 += l * (c0 * c0); k11 += l * (c1 * c1); k22 += l * (c2 * c2);
+            k01 += l * (c0 * c1); k02 += l * (c0 * c2); k12 += l * (c1 * c2);
         }
     }
-    const float is2 = 0.70710678118f;
-    s3_add_outer(H, ev[3], is2 * (vg1 * U.c[0] - vg0 * U.c[1]));
-    s3_add_outer(H, ev[4], is2 * (vg2 * U.c[0] - vg0 * U.c[2]));
-    s3_add_outer(H, ev[5], is2 * (vg2 * U.c[1] - vg1 * U.c[2]));
-    s3_add_outer(H, ev[6], is2 * (vg1 * U.c[0] + vg0 * U.c[1]));
-    s3_add_outer(H, ev[7], is2 * (vg2 * U.c[0] + vg0 * U.c[2]));
-    s3_add_outer(H, ev[8], is2 * (vg2 * U.c[1] + vg1 * U.c[2]));
-    H.xx *= restVolume; H.yy *= restVolume; H.zz *= restVolume;
-    H.xy *= restVolume; H.xz *= restVolume; H.yz *= restVolume;
+    // twist / flip pairs (0,1): ev[3], ev[6]; (0,2): ev[4], ev[7]; (1,2): ev[5], ev[8]
+    {
+        const float s01 = 0.5f * (ev[3] + ev[6]), d01 = 0.5f * (ev[6] - ev[3]);
+        const float s02 = 0.5f * (ev[4] + ev[7]), d02 = 0.5f * (ev[7] - ev[4]);
+        const float s12 = 0.5f * (ev[5] + ev[8]), d12 = 0.5f * (ev[8] - ev[5]);
+        const float q0 = g0 * g0, q1 = g1 * g1, q2 = g2 * g2;
+        k00 += s01 * q1 + s02 * q2;
+        k11 += s01 * q0 + s12 * q2;
+        k22 += s02 * q0 + s12 * q1;
+        k01 += d01 * (g0 * g1);
+        k02 += d02 * (g0 * g2);
+        k12 += d12 * (g1 * g2);
+    }
+    // H = restVolume U K U^T; T = K U^T (row m of T = sum_n K_mn u_n)
+    k00 *= restVolume; k11 *= restVolume; k22 *= restVolume;
+    k01 *= restVolume; k02 *= restVolume; k12 *= restVolume;
+    const V3 u0 = U.c[0], u1 = U.c[1], u2 = U.c[2];
+    const V3 t0 = k00 * u0 + k01 * u1 + k02 * u2;
+    const V3 t1 = k01 * u0 + k11 * u1 + k12 * u2;
+    const V3 t2 = k02 * u0 + k12 * u1 + k22 * u2;
+    // H_ab = sum_m u_m[a] t_m[b]
+    H.xx = u0.x * t0.x + u1.x * t1.x + u2.x * t2.x;
+    H.yy = u0.y * t0.y + u1.y * t1.y + u2.y * t2.y;
+    H.zz = u0.z * t0.z + u1.z * t1.z + u2.z * t2.z;
+    H.xy = u0.x * t0.y + u1.x * t1.y + u2.x * t2.y;
+    H.xz = u0.x * t0.z + u1.x * t1.z + u2.x * t2.z;
+    H.yz = u0.y * t0.z + u1.y * t1.z + u2.y * t2.z;
 }
 
 // NeoHookeanFEM::ComputeEnergyTerms for vertex `role` of the tet
