@@ -569,10 +569,75 @@ __device__ __forceinline__ bool colour_before(const World& W, int pass, int u, i
     return prio_less(colour_priority((uint32_t)lu), lu, colour_priority((uint32_t)lv), lv);
 }
 
+// Resumable scan state of a body in a Jones-Plassmann pass, in per-body
+// scratch the colouring does not otherwise use (the broadphase refills it
+// next step): W.cand_off the next incidence entry to scan (bit 30: a
+// neighbour holds a colour >= 64), W.cand_cnt / W.col_tinc the low / high
+// words of the mask of colours < 64 seen so far.
+constexpr int kJpWide = 1 << 30;
+
+__device__ __forceinline__ void jp_scan_reset(const World& W, int b) {
+    W.cand_off[b] = W.inc_off[b];
+    W.cand_cnt[b] = 0;
+    W.col_tinc[b] = 0;
+}
+
+// Scans body b's incidence from its saved entry: colours of coloured
+// neighbours go into the mask (they all precede b: a follower waits for
+// b), and the scan stops at the first entry holding an uncoloured neighbour
+// that precedes b.  True when every entry was scanned (b is ready).
+__device__ __forceinline__ bool jp_scan(const World& W, int cur, int pass, int b, volatile const int* col,
+                                        unsigned long long& used, bool& wide) {
+    int pos = W.cand_off[b];
+    wide = (pos & kJpWide) != 0;
+    int e = pos & ~kJpWide;
+    used = (unsigned long long)(uint32_t)W.cand_cnt[b] | ((unsigned long long)(uint32_t)W.col_tinc[b] << 32);
+    const int e1 = W.inc_off[b] + W.inc_cnt[b];
+    bool ready = true;
+    auto visit = [&](int n) {
+        if (!ready || n < 0 || n == b) return;
+        const int cn = col[n];
+        if (cn == -2) return;
+        if (cn >= 0) {
+            if (cn < 64) used |= 1ull << cn;
+            else wide = true;
+            return;
+        }
+        if (colour_before(W, pass, n, b)) ready = false;
+    };
+    for (; e < e1; ++e) {
+        const uint32_t ent = W.inc[e];
+        const uint32_t kind = ent_kind(ent), idx = ent_index(ent);
+        if (kind == kEntManifold) {
+            const int2 ab = W.cpair[cur][idx];
+            visit(ab.x == b ? ab.y : ab.x);
+        } else if (kind == kEntForce) {
+            if (W.ftype[idx] & kForceRemoved) continue;
+            const int2 ab = W.fbody[idx];
+            visit(ab.x == b ? ab.y : ab.x);
+        } else if (kind == kEntTet) {
+            if (W.tparam[idx].w != 0.f) continue;
+            const int4 v = W.tidx[idx];
+            visit(v.x); visit(v.y); visit(v.z); visit(v.w);
+        } else {
+            if (W.rparam[idx].w != 0.f) continue;
+            const int4 v = W.ridx[idx];
+            visit(v.x); visit(v.y); visit(v.z);
+        }
+        if (!ready) break;   // resume at this entry (its colours, seen again, change nothing)
+    }
+    W.cand_off[b] = e | (wide ? kJpWide : 0);
+    W.cand_cnt[b] = (int)(uint32_t)used;
+    W.col_tinc[b] = (int)(uint32_t)(used >> 32);
+    return ready;
+}
+
 // One Jones-Plassmann pass over the scene's uncoloured (-1) bodies: a body
 // takes the smallest colour its preceding neighbours do not use once they
 // are all coloured, which equals sequential greedy colouring in priority
-// order whatever the thread schedule.  False (status TIMEOUT) if it stalls.
+// order whatever the thread schedule.  A body's scan resumes each round at
+// the entry that held it up (jp_scan), so a pass reads each incidence entry
+// about once.  False (status TIMEOUT) if it stalls.
 static __device__ bool jp_pass(const Team& T, const World& W, const SceneDesc& sc, SceneState* st, int cur, int pass) {
     int& s_remaining = T.sh->remaining;
     int& s_progress = T.sh->progress;
@@ -581,28 +646,29 @@ static __device__ bool jp_pass(const Team& T, const World& W, const SceneDesc& s
     const int b0 = sc.body0, b1 = sc.body0 + sc.nbody;
     volatile int* col = W.colour;
     const int max_rounds = sc.nbody + 2;
+    for (int b = b0 + tid; b < b1; b += nt) jp_scan_reset(W, b);
+    T.sync();
     for (int round = 0;; ++round) {
         if (tid == 0) { s_remaining = 0; s_progress = 0; }
         T.sync();
         for (int b = b0 + tid; b < b1; b += nt) {
             if (col[b] != -1) continue;
-            bool ready = true;
-            for_each_neighbour(W, cur, b, [&](int n) {
-                if (!ready) return;
-                const int cn = col[n];
-                if (cn == -2) return;
-                if (cn < 0 && colour_before(W, pass, n, b)) ready = false;
-            });
-            if (!ready) { s_remaining = 1; continue; }
-            int chosen = -1;
-            for (int base = 0; base < kMaxColours && chosen < 0; base += 64) {
-                unsigned long long used = 0ull;
-                for_each_neighbour(W, cur, b, [&](int n) {
-                    const int cn = col[n];
-                    if (cn < base || cn >= base + 64) return;
-                    if (colour_before(W, pass, n, b)) used |= 1ull << (cn - base);
-                });
-                if (~used) chosen = base + __ffsll((long long)~used) - 1;
+            unsigned long long used;
+            bool wide;
+            if (!jp_scan(W, cur, pass, b, col, used, wide)) { s_remaining = 1; continue; }
+            int chosen = ~used ? __ffsll((long long)~used) - 1 : -1;
+            if (chosen < 0 || wide) {
+                // some neighbour holds a colour >= 64: first fit over 64-colour windows
+                chosen = -1;
+                for (int base = 0; base < kMaxColours && chosen < 0; base += 64) {
+                    unsigned long long w = 0ull;
+                    for_each_neighbour(W, cur, b, [&](int n) {
+                        const int cn = col[n];
+                        if (cn < base || cn >= base + 64) return;
+                        if (colour_before(W, pass, n, b)) w |= 1ull << (cn - base);
+                    });
+                    if (~w) chosen = base + __ffsll((long long)~w) - 1;
+                }
             }
             if (chosen < 0 || chosen >= kMaxColours) {
                 st->status = kStatusCapacity;
