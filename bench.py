@@ -176,12 +176,27 @@ class _Counter:
         return self.s.make_tet_volume(ox, oy, oz, nx, ny, nz, *a, **k)
 
 
-def pinned(shape):
-    try:
-        import torch
-        return torch.empty(shape, dtype=torch.float32, pin_memory=True).numpy()
-    except Exception:
-        return np.empty(shape, np.float32)
+_PINNED = []   # (pointer, lib) of the page-locked buffers handed out
+
+
+def pinned(shape, device=0):
+    """A float32 array in page-locked host memory (the library's allocator);
+    a pageable array when the host cannot lock it (`pinned.failed` counts
+    those)."""
+    import ctypes
+    from skyephyx_b200._lib import load
+    lib = load()
+    n = int(np.prod(shape))
+    p = ctypes.c_void_p()
+    if lib.avbd_host_alloc_pinned(int(device), n * 4, ctypes.byref(p)) == 0 and p.value:
+        _PINNED.append((p.value, lib))
+        buf = (ctypes.c_float * n).from_address(p.value)
+        return np.frombuffer(buf, dtype=np.float32, count=n).reshape(shape)
+    pinned.failed += 1
+    return np.empty(shape, np.float32)
+
+
+pinned.failed = 0
 
 
 def run_plain_sample(specs, steps, warmup):
@@ -798,7 +813,7 @@ def main():
     batch.prepare()
     nb_total = counts["bodies"]
     # two page-locked pose buffers: a step's poses are read back while the next step runs
-    pose_h = [(pinned((nb_total, 4)), pinned((nb_total, 4))) for _ in range(2)]
+    pose_h = [(pinned((nb_total, 4), device), pinned((nb_total, 4), device)) for _ in range(2)]
 
     def barrier():
         if dist is not None:
@@ -902,6 +917,7 @@ def main():
                    "parallelism": f"scenes x{ws}"},
         "e2e": {"value": e2e_value, "unit": UNIT, "h2d_bytes_per_step": int(upload_bytes / args.steps),
                 "d2h_bytes_per_step": d2h_step,
+                "host_pose_buffers": "page-locked" if pinned.failed == 0 else "pageable (page-locking failed)",
                 "note": "scenes staged in page-locked host memory before the timed region; the first step copies them to the device (one copy per device array); every step's poses are read back to page-locked host memory while the next step runs, the last read completing inside the timed region"},
         "gpu_launches": args.steps,
         "plain_gpu": {"value": plain_v, "unit": UNIT, "sample": f"first {len(plain_specs)} scenes, 3 steps each",

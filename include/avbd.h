@@ -279,6 +279,11 @@ int32_t avbd_batch_scene_body_offset(const AvbdBatch* b, int32_t scene);
 int32_t avbd_batch_prepare(AvbdBatch* b);
 /* Host-to-device bytes the last upload of staged scenes copied (0 before it). */
 int64_t avbd_batch_uploaded_bytes(const AvbdBatch* b);
+/* Page-locked host memory for the caller's pose and instance buffers
+ * (asynchronous copies need it): bytes on the given device's context;
+ * AVBD_ERR_NOMEM when the host cannot lock that much. */
+int32_t avbd_host_alloc_pinned(int32_t device, int64_t bytes, void** out);
+int32_t avbd_host_free_pinned(void* p);
 /* Advances every live scene by `steps` steps (one persistent kernel launch per
  * step, replayed from a CUDA graph). Returns AVBD_STATUS_OK or an error. */
 int32_t avbd_batch_step(AvbdBatch* b, int32_t steps);

@@ -117,6 +117,8 @@ SIGNATURES = [
     ("avbd_batch_remove_scene", [_V, C.c_int32], C.c_int32),
     ("avbd_batch_prepare", [_V], C.c_int32),
     ("avbd_batch_uploaded_bytes", [_V], C.c_int64),
+    ("avbd_host_alloc_pinned", [C.c_int32, C.c_int64, C.POINTER(C.c_void_p)], C.c_int32),
+    ("avbd_host_free_pinned", [_V], C.c_int32),
     ("avbd_batch_step", [_V, C.c_int32], C.c_int32),
     ("avbd_batch_num_scenes", [_V], C.c_int32),
     ("avbd_batch_scene_status", [_V, C.c_int32], C.c_int32),

@@ -745,6 +745,23 @@ int32_t avbd_batch_read_poses(AvbdBatch* b, float* pos, float* quat, int64_t max
     return (int32_t)n;
 }
 
+int32_t avbd_host_alloc_pinned(int32_t device, int64_t bytes, void** out) {
+    if (!out || bytes < 0) return AVBD_ERR_INVALID;
+    *out = nullptr;
+    if (int r = device_ready(device)) return r;
+    if (cudaHostAlloc(out, std::max<int64_t>(bytes, 1), cudaHostAllocPortable) != cudaSuccess) {
+        cudaGetLastError();
+        *out = nullptr;
+        return AVBD_ERR_NOMEM;
+    }
+    return 0;
+}
+
+int32_t avbd_host_free_pinned(void* p) {
+    if (!p) return AVBD_ERR_INVALID;
+    return cudaFreeHost(p) == cudaSuccess ? 0 : AVBD_ERR_CUDA;
+}
+
 int32_t avbd_batch_read_poses_wait(AvbdBatch* b) {
     if (!b) return AVBD_ERR_INVALID;
     if (!b->copy_stream) return 0;
