@@ -236,7 +236,6 @@ struct World {
     // ---- Neo-Hookean tets ----
     int4* tidx;
     float* tDmInv;      // 9 per tet, column-major
-    float* tgradN;      // 12 per tet: gradN0..3
     float4* tparam;     // restVolume, mu, lambda
     int* tkind;         // energy model of each tet (kTetNeoHookean, kTetStvk)
 

@@ -195,13 +195,7 @@ int HostScene::add_nh_tet(const int* v, float E, float nu) {
     tidx.push_back(idx);
     for (int j = 0; j < 3; ++j)
         for (int i = 0; i < 3; ++i) tDmInv.push_back(r[i][j]);   // column-major
-    // gradN1..3 = columns of DmInv^T = rows of DmInv; gradN0 = -g1 - g2 - g3
-    float g[4][3];
-    for (int k = 0; k < 3; ++k)
-        for (int i = 0; i < 3; ++i) g[k + 1][i] = r[k][i];
-    for (int i = 0; i < 3; ++i) g[0][i] = ((-g[1][i]) - g[2][i]) - g[3][i];
-    for (int k = 0; k < 4; ++k)
-        for (int i = 0; i < 3; ++i) tgradN.push_back(g[k][i]);
+    // the shape gradients (neohookeanfem.cpp:31-36) are rebuilt from DmInv on the device
     tparam.push_back(mk4(restVolume, mu, lam, 0.f));
     tkind.push_back(kTetNeoHookean);
     return ntet() - 1;

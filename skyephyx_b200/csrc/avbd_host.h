@@ -27,7 +27,7 @@ struct HostScene {
     std::vector<float> fk, ffrac, ffmin, ffmax;   // 6 per force
     // Neo-Hookean tets
     std::vector<int4> tidx;
-    std::vector<float> tDmInv, tgradN;
+    std::vector<float> tDmInv;
     std::vector<float4> tparam;
     std::vector<int> tkind;   // kTetNeoHookean or kTetStvk
     // StVK triangles

@@ -754,6 +754,17 @@ AVBD_HD void sys_zero(Sys6& s) {
     }
 }
 
+// Shape gradient of a tet's vertex `role` from its Dm^-1 (column-major):
+// gradN1..3 are the rows of Dm^-1 and gradN0 = -g1 - g2 - g3, with the
+// reference's operations (neohookeanfem.cpp:31-36), so the values equal the
+// ones the host computes bit for bit; nothing stores them.
+AVBD_HD V3 tet_shape_grad(const float* D, uint32_t role) {
+    if (role == 0) return v3(((-D[0]) - D[1]) - D[2], ((-D[3]) - D[4]) - D[5], ((-D[6]) - D[7]) - D[8]);
+    if (role == 1) return v3(D[0], D[3], D[6]);
+    if (role == 2) return v3(D[1], D[4], D[7]);
+    return v3(D[2], D[5], D[8]);
+}
+
 // Gradient and projected Hessian of tet `idx` for its vertex `role`
 // (NeoHookeanFEM::ComputeEnergyTerms, neohookeanfem.cpp:40-90, or the StVK
 // tet); false for a removed tet.
@@ -761,13 +772,14 @@ AVBD_HD bool tet_term(const World& W, int idx, int role, V3& g, S3& H) {
     const int4 v = W.tidx[idx];
     const float4 tp = W.tparam[idx];
     if (tp.w != 0.f) return false;   // removed energy
-    const float* gn = W.tgradN + (size_t)idx * 12 + role * 3;
+    const float* D = W.tDmInv + (size_t)idx * 9;
+    const V3 gn = tet_shape_grad(D, (uint32_t)role);
     if (W.tkind[idx] == kTetStvk)
-        stvk_tet_terms(v3(W.pos[v.x]), v3(W.pos[v.y]), v3(W.pos[v.z]), v3(W.pos[v.w]), W.tDmInv + (size_t)idx * 9,
-                       v3(gn[0], gn[1], gn[2]), tp.x, tp.y, tp.z, W.P.projection_mode, W.P.trust_region_rho, g, H);
+        stvk_tet_terms(v3(W.pos[v.x]), v3(W.pos[v.y]), v3(W.pos[v.z]), v3(W.pos[v.w]), D, gn, tp.x, tp.y, tp.z,
+                       W.P.projection_mode, W.P.trust_region_rho, g, H);
     else
-        neohookean_terms(v3(W.pos[v.x]), v3(W.pos[v.y]), v3(W.pos[v.z]), v3(W.pos[v.w]), W.tDmInv + (size_t)idx * 9,
-                         v3(gn[0], gn[1], gn[2]), tp.x, tp.y, tp.z, W.P.projection_mode, W.P.trust_region_rho, g, H);
+        neohookean_terms(v3(W.pos[v.x]), v3(W.pos[v.y]), v3(W.pos[v.z]), v3(W.pos[v.w]), D, gn, tp.x, tp.y, tp.z,
+                         W.P.projection_mode, W.P.trust_region_rho, g, H);
     return true;
 }
 
@@ -788,9 +800,7 @@ __device__ __forceinline__ void write_term_record(const World& W, size_t q, uint
 }
 
 // tet_term from the record in slot q: streamed loads (each record is read
-// once per sweep) and the shape gradient of the term's vertex rebuilt from
-// Dm^-1 with the host's operations (gradN1..3 = rows of Dm^-1, gradN0 =
-// -g1 - g2 - g3), so the values equal the stored ones bit for bit.
+// once per sweep) and the shape gradient of the term's vertex from Dm^-1.
 __device__ __forceinline__ bool tet_term_record(const World& W, size_t q, V3& g, S3& H) {
     const int4 a = __ldcs(W.trv + q);
     const uint32_t x = (uint32_t)a.x;
@@ -798,11 +808,7 @@ __device__ __forceinline__ bool tet_term_record(const World& W, size_t q, V3& g,
     const float4 m0 = __ldcs(W.trm0 + q), m1 = __ldcs(W.trm1 + q), m2 = __ldcs(W.trm2 + q);
     const float D[9] = {m0.x, m0.y, m0.z, m0.w, m1.x, m1.y, m1.z, m1.w, m2.x};
     const uint32_t role = (x >> kTermRoleShift) & 3u;
-    V3 gn;
-    if (role == 0) gn = v3(((-D[0]) - D[1]) - D[2], ((-D[3]) - D[4]) - D[5], ((-D[6]) - D[7]) - D[8]);
-    else if (role == 1) gn = v3(D[0], D[3], D[6]);
-    else if (role == 2) gn = v3(D[1], D[4], D[7]);
-    else gn = v3(D[2], D[5], D[8]);
+    const V3 gn = tet_shape_grad(D, role);
     const V3 p0 = v3(W.pos[x & kTermIdMask]), p1 = v3(W.pos[a.y]), p2 = v3(W.pos[a.z]), p3 = v3(W.pos[a.w]);
     if (x & kTermStvk)
         stvk_tet_terms(p0, p1, p2, p3, D, gn, m2.y, m2.z, m2.w, W.P.projection_mode, W.P.trust_region_rho, g, H);

@@ -127,7 +127,7 @@ struct Pools {
         A(alloc(W.fq, nf)); A(alloc(W.fparam, nf)); A(alloc(W.fC0p, nf)); A(alloc(W.fC0a, nf));
         A(alloc(W.fk, 6 * (size_t)nf)); A(alloc(W.ffrac, 6 * (size_t)nf)); A(alloc(W.ffmin, 6 * (size_t)nf));
         A(alloc(W.ffmax, 6 * (size_t)nf)); A(alloc(W.fpen, 6 * (size_t)nf)); A(alloc(W.flam, 6 * (size_t)nf));
-        A(alloc(W.tidx, nt)); A(alloc(W.tDmInv, 9 * (size_t)nt)); A(alloc(W.tgradN, 12 * (size_t)nt));
+        A(alloc(W.tidx, nt)); A(alloc(W.tDmInv, 9 * (size_t)nt));
         A(alloc(W.tparam, nt)); A(alloc(W.tkind, nt));
         A(alloc(W.trv, 4 * (size_t)nt)); A(alloc(W.trm0, 4 * (size_t)nt)); A(alloc(W.trm1, 4 * (size_t)nt));
         A(alloc(W.trm2, 4 * (size_t)nt));
@@ -136,7 +136,9 @@ struct Pools {
         A(alloc(W.check, 4));
         for (int t = 0; t < 2; ++t) A(alloc_tables(t, ncand, nk));
 #undef A
-        return e;
+        // the zeroing memsets run on the legacy stream; the uploads that follow
+        // run on non-blocking streams and must find the pools zeroed
+        return cudaStreamSynchronize(cudaStreamLegacy);
     }
 
     cudaError_t alloc_tables(int t, int nc, int k) {
@@ -312,6 +314,14 @@ struct DirectSink {
     void put(T* dst, const std::vector<T>& src, size_t at) {
         if (!src.empty()) cudaMemcpyAsync(dst + at, src.data(), src.size() * sizeof(T), cudaMemcpyHostToDevice, st);
     }
+    // `src` into arrays dst[0..n) at the same offset: one host copy, the
+    // others device to device
+    template <typename T>
+    void put_all(T* const* dst, int n, const std::vector<T>& src, size_t at) {
+        put(dst[0], src, at);
+        for (int i = 1; i < n && !src.empty(); ++i)
+            cudaMemcpyAsync(dst[i] + at, dst[0] + at, src.size() * sizeof(T), cudaMemcpyDeviceToDevice, st);
+    }
     template <typename T>
     void zero(T* dst, size_t at, size_t n) {
         if (n) cudaMemsetAsync(dst + at, 0, n * sizeof(T), st);
@@ -326,6 +336,13 @@ struct StagedSink {
         bool locked = false;    // [lo, hi) page-locked
     };
     std::map<char*, Buf> bufs;
+    // Arrays written as copies of another array's range (put_all): filled on
+    // the device from their source after the host copies, [lo, hi) in bytes.
+    struct Mirror {
+        char* src = nullptr;
+        size_t lo = SIZE_MAX, hi = 0;
+    };
+    std::map<char*, Mirror> mirrors;
     const Pools* P = nullptr;   // allocation sizes: each buffer is sized once to its pool array
     cudaStream_t st = nullptr;
     std::mutex m;               // scenes are staged from several host threads
@@ -359,6 +376,18 @@ struct StagedSink {
             std::memcpy(h + at * sizeof(T), src.data(), src.size() * sizeof(T));
     }
     template <typename T>
+    void put_all(T* const* dst, int n, const std::vector<T>& src, size_t at) {
+        put(dst[0], src, at);
+        if (src.empty()) return;
+        std::lock_guard<std::mutex> lock(m);
+        for (int i = 1; i < n; ++i) {
+            Mirror& mi = mirrors[reinterpret_cast<char*>(dst[i])];
+            mi.src = reinterpret_cast<char*>(dst[0]);
+            mi.lo = std::min(mi.lo, at * sizeof(T));
+            mi.hi = std::max(mi.hi, (at + src.size()) * sizeof(T));
+        }
+    }
+    template <typename T>
     void zero(T* dst, size_t at, size_t n) {
         if (!n) return;
         if (char* h = span(dst, at * sizeof(T), n * sizeof(T))) std::memset(h + at * sizeof(T), 0, n * sizeof(T));
@@ -383,6 +412,10 @@ struct StagedSink {
                                 cudaMemcpyHostToDevice, st);
                 copied += (int64_t)(kv.second.hi - kv.second.lo);
             }
+        for (auto& kv : mirrors)
+            if (kv.second.hi > kv.second.lo)
+                cudaMemcpyAsync(kv.first + kv.second.lo, kv.second.src + kv.second.lo, kv.second.hi - kv.second.lo,
+                                cudaMemcpyDeviceToDevice, st);
         cudaStreamSynchronize(st);
         return !overflow;
     }
@@ -393,6 +426,7 @@ struct StagedSink {
             std::free(kv.second.host);
         }
         bufs.clear();
+        mirrors.clear();
     }
 };
 
@@ -449,6 +483,14 @@ struct ArenaSink {
         used = off + n;
         ops.push_back({static_cast<void*>(dst + at), off, n, false});
     }
+    // one staged copy of `src`, scattered to every array dst[0..n)
+    template <typename T>
+    void put_all(T* const* dst, int n, const std::vector<T>& src, size_t at) {
+        put(dst[0], src, at);
+        if (src.empty() || overflow) return;
+        const Op first = ops.back();
+        for (int i = 1; i < n; ++i) ops.push_back({static_cast<void*>(dst[i] + at), first.off, first.bytes, false});
+    }
     template <typename T>
     void zero(T* dst, size_t at, size_t n) {
         if (n) ops.push_back({static_cast<void*>(dst + at), 0, n * sizeof(T), true});
@@ -504,12 +546,14 @@ inline void upload_scene(Pools& P, const HostScene& h, const StaticInc& si, cons
     d.ndynamic = h.ndynamic();
     d.group = group;
     World& W = P.W;
-    sink.put(W.pos, h.pos, d.body0); sink.put(W.rot, h.rot, d.body0); sink.put(W.scale, h.scale, d.body0);
     sink.put(W.vel, h.vel, d.body0); sink.put(W.omega, h.omega, d.body0); sink.put(W.massI, h.massI, d.body0);
     sink.put(W.flags, h.flags, d.body0); sink.put(W.friction, h.friction, d.body0);
     sink.put(W.color, h.color, d.body0);
-    sink.put(W.lpos, h.pos, d.body0); sink.put(W.lrot, h.rot, d.body0);
-    sink.put(W.ipos, h.pos, d.body0); sink.put(W.irot, h.rot, d.body0);
+    // lastPosition and inertialPosition start equal to the pose: one upload of each
+    float4* const pos_to[3] = {W.pos, W.lpos, W.ipos};
+    float4* const rot_to[3] = {W.rot, W.lrot, W.irot};
+    sink.put_all(pos_to, 3, h.pos, d.body0); sink.put_all(rot_to, 3, h.rot, d.body0);
+    sink.put(W.scale, h.scale, d.body0);
     sink.zero(W.pvel, d.body0, d.nbody);
     sink.zero(W.reset_flag, d.body0, d.nbody);
     std::vector<int> tmp(d.nbody);
@@ -535,7 +579,7 @@ inline void upload_scene(Pools& P, const HostScene& h, const StaticInc& si, cons
     std::vector<int4> ti = h.tidx;
     for (auto& t : ti) { t.x += d.body0; t.y += d.body0; t.z += d.body0; t.w += d.body0; }
     sink.put(W.tidx, ti, d.tet0); sink.put(W.tDmInv, h.tDmInv, 9 * (size_t)d.tet0);
-    sink.put(W.tgradN, h.tgradN, 12 * (size_t)d.tet0); sink.put(W.tparam, h.tparam, d.tet0);
+    sink.put(W.tparam, h.tparam, d.tet0);
     sink.put(W.tkind, h.tkind, d.tet0);
     std::vector<int4> ri = h.ridx;
     for (auto& t : ri) { t.x += d.body0; t.y += d.body0; t.z += d.body0; }

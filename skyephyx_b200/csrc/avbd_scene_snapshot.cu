@@ -54,7 +54,6 @@ std::vector<Slice> scene_slices(const Pools& P) {
     for (const float* p : {W.fk, W.ffrac, W.ffmin, W.ffmax, W.fpen, W.flam}) add(p, 4, 6, kUForce);
     add(W.tidx, 16, 1, kUTet);
     add(W.tDmInv, 4, 9, kUTet);
-    add(W.tgradN, 4, 12, kUTet);
     add(W.tparam, 16, 1, kUTet);
     add(W.tkind, 4, 1, kUTet);
     add(W.trv, 16, 4, kUTet);
