@@ -140,7 +140,8 @@ struct SceneState {
     int topo;                // bumped when a force or body is removed
     int coloured_topo;       // topo value the current colouring was made for
     int colours_valid;       // the colour lists describe the current contact graph
-    int pad[2];
+    int npend;               // batched narrowphase: candidate pairs not separated by an axis this step
+    int pad;
 };
 
 // Structure-of-arrays device world.  One instance is passed by value to kernels.

@@ -182,12 +182,11 @@ AVBD_HD void line_line_contacts(V3 posA, V3 scaleA, const M3& rotA, V3 posB, V3 
     out.n = 1;
 }
 
-// CollisionSpace::CollisionBoxBox (collision.cpp:271-447).  scale = full box edges.
-AVBD_HD void collide_box_box(V3 posA, Q4 qA, V3 scaleA, V3 posB, Q4 qB, V3 scaleB, Collision& out) {
-    out.n = 0;
-    const M3 rotA = xrotmat(qA);
-    const M3 rotB = xrotmat(qB);
-    const V3 d = xsub(posB, posA);
+// The separating-axis part of CollisionSpace::CollisionBoxBox
+// (collision.cpp:271-373): the axis of least penetration (0-2 faces of A, 3-5
+// faces of B, 6-14 edge pairs) and its sign, or -1 if an axis separates the
+// boxes (no contacts).  scale = full box edges.
+AVBD_HD int box_box_sat(const M3& rotA, V3 scaleA, const M3& rotB, V3 scaleB, V3 d, float& bestSign) {
     float C[3][3], AR[3][3], T[3];
     for (int i = 0; i < 3; i++) {
         T[i] = xdot(rotA.c[i], d);
@@ -199,10 +198,10 @@ AVBD_HD void collide_box_box(V3 posA, Q4 qA, V3 scaleA, V3 posB, Q4 qB, V3 scale
     const V3 hA = xmul(scaleA, 0.5f), hB = xmul(scaleB, 0.5f);
     float best = 3.402823466e+38f;
     int bestAxis = -1;
-    float bestSign = 1.f;
+    bestSign = 1.f;
 #define AVBD_TEST_AXIS(idx, pen, sgn)              \
     {                                              \
-        if ((pen) < 0.f) return;                   \
+        if ((pen) < 0.f) return -1;                \
         if ((pen) < best) {                        \
             best = (pen); bestAxis = (idx); bestSign = (sgn); \
         }                                          \
@@ -242,7 +241,19 @@ AVBD_HD void collide_box_box(V3 posA, Q4 qA, V3 scaleA, V3 posB, Q4 qB, V3 scale
         }
     }
 #undef AVBD_TEST_AXIS
+    return bestAxis;
+}
+
+// CollisionSpace::CollisionBoxBox (collision.cpp:271-447).  scale = full box edges.
+AVBD_HD void collide_box_box(V3 posA, Q4 qA, V3 scaleA, V3 posB, Q4 qB, V3 scaleB, Collision& out) {
+    out.n = 0;
+    const M3 rotA = xrotmat(qA);
+    const M3 rotB = xrotmat(qB);
+    const V3 d = xsub(posB, posA);
+    float bestSign;
+    const int bestAxis = box_box_sat(rotA, scaleA, rotB, scaleB, d, bestSign);
     if (bestAxis < 0) return;
+    const V3 hA = xmul(scaleA, 0.5f), hB = xmul(scaleB, 0.5f);
 
     V3 normal;
     if (bestAxis < 3) {

@@ -307,7 +307,8 @@ inline bool place_scene(Allocs& A, const HostScene& h, int candcap, int kcap, in
 // Where upload_scene's data goes.  DirectSink: straight to the device, one
 // copy per array of the scene.  StagedSink: into one host buffer per device
 // array at the scene's offsets, flushed with one copy per array, for packing
-// many scenes into fresh (zeroed) pools at once.
+// many scenes into fresh (zeroed) pools at once; what is zero there already
+// (cleared arrays, all-zero data such as scenes at rest) is not copied.
 struct DirectSink {
     cudaStream_t st;
     template <typename T>
@@ -372,8 +373,12 @@ struct StagedSink {
     template <typename T>
     void put(T* dst, const std::vector<T>& src, size_t at) {
         if (src.empty()) return;
-        if (char* h = span(dst, at * sizeof(T), src.size() * sizeof(T)))
-            std::memcpy(h + at * sizeof(T), src.data(), src.size() * sizeof(T));
+        const size_t n = src.size() * sizeof(T);
+        const unsigned char* p = reinterpret_cast<const unsigned char*>(src.data());
+        size_t i = 0;
+        while (i < n && p[i] == 0) ++i;
+        if (i == n) { fits(dst, at * sizeof(T) + n); return; }   // the pool holds these zero bytes already
+        if (char* h = span(dst, at * sizeof(T), n)) std::memcpy(h + at * sizeof(T), src.data(), n);
     }
     template <typename T>
     void put_all(T* const* dst, int n, const std::vector<T>& src, size_t at) {
@@ -387,10 +392,22 @@ struct StagedSink {
             mi.hi = std::max(mi.hi, (at + src.size()) * sizeof(T));
         }
     }
+    // fresh pools are zeroed when allocated
     template <typename T>
     void zero(T* dst, size_t at, size_t n) {
-        if (!n) return;
-        if (char* h = span(dst, at * sizeof(T), n * sizeof(T))) std::memset(h + at * sizeof(T), 0, n * sizeof(T));
+        if (n) fits(dst, (at + n) * sizeof(T));
+    }
+    // Sets overflow if pool array `dst` is shorter than `end` bytes.
+    void fits(const void* dst, size_t end) {
+        if (!P) return;
+        for (size_t i = 0; i < P->owned.size(); ++i)
+            if (P->owned[i] == dst) {
+                if (P->owned_bytes[i] < end) {
+                    std::lock_guard<std::mutex> lock(m);
+                    overflow = true;
+                }
+                return;
+            }
     }
     void finish() {}
     // Page-locks the written range of every buffer, so the copies run at the

@@ -774,10 +774,42 @@ static __device__ __noinline__ bool colour_scene(const Team& T, const World& W, 
 
 // Phase loops of one scene kept out of line, so each gets its own register
 // allocation instead of the union of every inlined phase.
+//
+// Narrowphase in two passes.  Most candidate pairs (bounding spheres that
+// overlap) are separated by an axis, and a pair that touches costs several
+// times more (clipping, contact matching and writes); with one pair per lane,
+// a warp would wait on its few touching lanes at every turn.  So the first
+// pass runs the separating-axis test on every pair and lists the pairs that
+// touch, warp by warp, and the second pass makes their manifolds with every
+// lane busy.  The list borrows the other table's live list, which nothing
+// reads again before this step's narrowphase rewrites that table's slots.
 static __device__ __noinline__ void narrowphase_cta(const Team& T, const World& W, const SceneDesc& sc, SceneState* st,
                                              int cur, int ncand, int old_count) {
-    for (int c = sc.cand0 + T.rank; c < sc.cand0 + ncand; c += T.size)
-        narrowphase_slot(W, sc, st, c, cur, old_count);
+    int* pend = W.live[cur ^ 1] + sc.cand0;
+    const int lane = threadIdx.x & 31;
+    for (int c0 = sc.cand0; c0 < sc.cand0 + ncand; c0 += T.size) {   // uniform over the team's warps
+        const int c = c0 + T.rank;
+        bool touch = false;
+        if (c < sc.cand0 + ncand) {
+            const int2 ab = W.cpair[cur][c];
+            const float4 pa = W.pos[ab.x], pb = W.pos[ab.y];
+            float sign;
+            touch = box_box_sat(xrotmat(q4(W.rot[ab.x])), v3(W.scale[ab.x]), xrotmat(q4(W.rot[ab.y])),
+                                v3(W.scale[ab.y]), xsub(v3(pb), v3(pa)), sign) >= 0;
+            if (!touch) W.cn[cur][c] = 0;
+        }
+        const unsigned m = __ballot_sync(0xffffffffu, touch);
+        if (m) {
+            int base = 0;
+            if (lane == 0) base = atomicAdd(&st->npend, __popc(m));
+            base = __shfl_sync(0xffffffffu, base, 0);
+            const int at = base + __popc(m & ((1u << lane) - 1u));
+            if (touch && AVBD_CHECK(W, at < ncand, 7, at, ncand)) pend[at] = c;
+        }
+    }
+    T.sync();
+    const int npend = __ldcg(&st->npend);
+    for (int i = T.rank; i < npend; i += T.size) narrowphase_slot(W, sc, st, __ldcg(pend + i), cur, old_count);
 }
 
 // Returns true if this thread saw a force fracture.  Manifolds come from the
@@ -1110,7 +1142,7 @@ static __device__ void scene_step(const World& W, int scene, const Team& T) {
         }
         return;
     }
-    if (tid == 0) { st->kused[cur] = 0; st->nlive[cur] = 0; st->nmatched = 0; }
+    if (tid == 0) { st->kused[cur] = 0; st->nlive[cur] = 0; st->nmatched = 0; st->npend = 0; }
     T.sync();
     scene_stamp(W, T, scene, 1);
     // 2. narrowphase + manifold warm start into the other table
