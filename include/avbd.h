@@ -357,12 +357,6 @@ int32_t avbd_batch_set_grid_broadphase(AvbdBatch* b, int32_t min_bodies);
  * estimate of each scene's step time for the largest-first order.
  * Autotuner knob; results do not depend on it. */
 int32_t avbd_batch_set_queue_weight(AvbdBatch* b, int32_t body_weight);
-/* by_time 1 (default): before each step, a one-CTA kernel reorders that
- * queue by each scene's device time in its previous step, longest first
- * (scenes not yet stepped first; ties and the cluster-run head keep the size
- * order); 0: the size order alone.  Autotuner knob; results do not depend on
- * it. */
-int32_t avbd_batch_set_queue_order(AvbdBatch* b, int32_t by_time);
 /* Per-scene device timing (off by default): each step stamps the GPU's
  * global timer (ns) AVBD_SCENE_STAMPS times per scene: when its team starts
  * the step, after the broadphase, the narrowphase, the joint/spring warm

@@ -137,7 +137,6 @@ SIGNATURES = [
     ("avbd_batch_set_cluster", [_V, C.c_int32, C.c_int32], C.c_int32),
     ("avbd_batch_set_scene_timing", [_V, C.c_int32], C.c_int32),
     ("avbd_batch_set_queue_weight", [_V, C.c_int32], C.c_int32),
-    ("avbd_batch_set_queue_order", [_V, C.c_int32], C.c_int32),
     ("avbd_batch_read_poses", [_V, _F, _F, C.c_int64], C.c_int32),
     ("avbd_batch_read_poses_wait", [_V], C.c_int32),
     ("avbd_check_word", [_V, C.POINTER(C.c_int32)], C.c_int32),

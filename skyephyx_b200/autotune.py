@@ -87,8 +87,6 @@ def apply(batch, cfg: dict) -> None:
         batch.set_cluster(cfg["cluster"], cfg.get("cluster_min", 0))
     if cfg.get("queue_body_weight", 1) != 1:
         batch.set_queue_weight(cfg["queue_body_weight"])
-    if not cfg.get("queue_by_time", 1):
-        batch.set_queue_order(False)
 
 
 def candidates(space=SPACE):

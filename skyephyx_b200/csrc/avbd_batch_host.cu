@@ -74,7 +74,6 @@ int batch_reserve(AvbdBatch* b, int64_t bodies, int64_t forces, int64_t tets, in
     P.W.P = to_params(b->params);
     b->A.reset(P);
     if (b->d_order) cudaFree(b->d_order);
-    if (b->d_order_run) cudaFree(b->d_order_run);
     if (b->d_nlive) cudaFree(b->d_nlive);
     if (b->d_queue) cudaFree(b->d_queue);
     if (b->d_fail) cudaFree(b->d_fail);
@@ -88,7 +87,6 @@ int batch_reserve(AvbdBatch* b, int64_t bodies, int64_t forces, int64_t tets, in
         cudaMemset(b->d_scene_ns, 0, n * sizeof(unsigned long long));
     }
     if (cudaMalloc(&b->d_order, std::max<int64_t>(nscenes, 1) * sizeof(int)) != cudaSuccess ||
-        cudaMalloc(&b->d_order_run, std::max<int64_t>(nscenes, 1) * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&b->d_nlive, 2 * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&b->d_queue, 2 * sizeof(int)) != cudaSuccess ||
         cudaMalloc(&b->d_fail, sizeof(int)) != cudaSuccess ||
@@ -437,61 +435,8 @@ int batch_fix_capacity(AvbdBatch* b, int64_t* grown_count) {
     return 0;
 }
 
-// The queue of a step, from the live queue `order` (nlive[0] slots, the
-// first nlive[1] of them run by whole clusters and kept in place): the other
-// slots by decreasing device time of their last step, slots not yet stepped
-// first, ties in the live queue's order (largest first).  Longest first over
-// the CTAs' scene pulls is the classic list-scheduling rule; the measured time
-// of a scene's last step predicts its next far better than its size does (a
-// tall stack of a few boxes outlasts a wide pile of many).  One CTA; a
-// bitonic sort in shared memory of up to kCostSortMax slots, beyond which
-// the live queue is run as it is.
-constexpr int kCostSortMax = 8192;
-__global__ void __launch_bounds__(1024) k_order_by_cost(const int* order, const int* nlive, const unsigned* cost,
-                                                         int* run) {
-    extern __shared__ unsigned long long s_key[];
-    const int n = nlive[0];
-    const int head = min(max(nlive[1], 0), n);
-    const int m = n - head;
-    if (m > kCostSortMax) {
-        for (int i = threadIdx.x; i < n; i += blockDim.x) run[i] = order[i];
-        return;
-    }
-    for (int i = threadIdx.x; i < head; i += blockDim.x) run[i] = order[i];
-    int p = 1;
-    while (p < m) p <<= 1;
-    for (int i = threadIdx.x; i < p; i += blockDim.x) {
-        unsigned long long k = 0;   // padding: below every slot's key
-        if (i < m) {
-            unsigned c = cost[order[head + i]];
-            if (c == 0) c = 0xFFFFFFFFu;
-            k = ((unsigned long long)c << 32) | (0xFFFFFFFFu - (unsigned)i);
-        }
-        s_key[i] = k;
-    }
-    __syncthreads();
-    for (int size = 2; size <= p; size <<= 1)
-        for (int stride = size >> 1; stride > 0; stride >>= 1) {
-            for (int i = threadIdx.x; i < p; i += blockDim.x) {
-                const int j = i ^ stride;
-                if (j > i) {
-                    const unsigned long long x = s_key[i], y = s_key[j];
-                    if (((i & size) == 0) ? x < y : x > y) { s_key[i] = y; s_key[j] = x; }
-                }
-            }
-            __syncthreads();
-        }
-    for (int i = threadIdx.x; i < m; i += blockDim.x)
-        run[head + i] = order[head + (int)(0xFFFFFFFFu - (unsigned)(s_key[i] & 0xFFFFFFFFull))];
-}
-
 int batch_build_graph(AvbdBatch* b) {
     batch_drop_graph(b);
-    const size_t sort_smem = kCostSortMax * sizeof(unsigned long long);
-    if (b->queue_by_time &&
-        cudaFuncSetAttribute(k_order_by_cost, cudaFuncAttributeMaxDynamicSharedMemorySize, (int)sort_smem) !=
-            cudaSuccess)
-        return AVBD_ERR_CUDA;
     cudaGraph_t g;
     if (cudaStreamBeginCapture(b->stream, cudaStreamCaptureModeThreadLocal) != cudaSuccess) return AVBD_ERR_CUDA;
     cudaMemsetAsync(b->d_queue, 0, 2 * sizeof(int), b->stream);
@@ -501,13 +446,7 @@ int batch_build_graph(AvbdBatch* b) {
     b->P.W.grid_min = b->grid_min;
     b->P.W.fail_count = b->d_fail;
     b->P.W.scene_ns = b->d_scene_ns;
-    b->P.W.scene_cost = b->queue_by_time ? b->P.d_cost : nullptr;
-    const int* order = b->d_order;
-    if (b->queue_by_time) {
-        k_order_by_cost<<<1, 1024, sort_smem, b->stream>>>(b->d_order, b->d_nlive, b->P.d_cost, b->d_order_run);
-        order = b->d_order_run;
-    }
-    const cudaError_t launched = launch_batch_kernel(b, b->P.W, order, b->d_nlive, b->d_queue);
+    const cudaError_t launched = launch_batch_kernel(b, b->P.W, b->d_order, b->d_nlive, b->d_queue);
     if (cudaStreamEndCapture(b->stream, &g) != cudaSuccess || launched != cudaSuccess) return AVBD_ERR_CUDA;
     cudaError_t e = cudaGraphInstantiate(&b->graph, g, 0);
     cudaGraphDestroy(g);
@@ -567,7 +506,6 @@ int32_t avbd_batch_destroy(AvbdBatch* b) {
     batch_drop_graph(b);
     if (b->upload) b->upload->release();
     if (b->d_order) cudaFree(b->d_order);
-    if (b->d_order_run) cudaFree(b->d_order_run);
     if (b->d_nlive) cudaFree(b->d_nlive);
     if (b->d_queue) cudaFree(b->d_queue);
     if (b->d_fail) cudaFree(b->d_fail);
@@ -955,13 +893,6 @@ int32_t avbd_batch_scene_times(AvbdBatch* b, int64_t* stamps_ns, int32_t max_slo
                             cudaMemcpyDeviceToHost) != cudaSuccess)
         return AVBD_ERR_CUDA;
     return n;
-}
-
-int32_t avbd_batch_set_queue_order(AvbdBatch* b, int32_t by_time) {
-    if (!b || by_time < 0 || by_time > 1) return AVBD_ERR_INVALID;
-    b->queue_by_time = by_time;
-    batch_drop_graph(b);
-    return 0;
 }
 
 int32_t avbd_batch_set_queue_weight(AvbdBatch* b, int32_t body_weight) {

@@ -36,20 +36,12 @@ namespace avbd {
 namespace {
 
 // Runs one scene's step on team T, stamping its start and end when timing is on
-// (scene_step stamps the phase ends in between), and recording its device
-// time for the next step's queue order.
+// (scene_step stamps the phase ends in between).
 __device__ __forceinline__ void timed_scene_step(const World& W, int scene, const Team& T) {
-    unsigned long long t0 = 0;
-    if (W.scene_cost && T.rank == 0) asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t0));
     scene_stamp(W, T, scene, 0);
     scene_step(W, scene, T);
     T.sync();
     scene_stamp(W, T, scene, kSceneStamps - 1);
-    if (W.scene_cost && T.rank == 0) {
-        unsigned long long t1;
-        asm volatile("mov.u64 %0, %%globaltimer;" : "=l"(t1));
-        W.scene_cost[scene] = (unsigned)max(1ull, min(t1 - t0, 0xFFFFFFFEull));
-    }
 }
 
 // MAXT is the largest CTA the build serves and MINB sets its register budget

@@ -155,8 +155,6 @@ struct World {
     int* check;         // debug builds: first failed index check (code, index, bound) and the failure count
     unsigned long long* scene_ns;   // batched kernel, optional: per scene slot kSceneStamps global-timer
                                     // readings (ns) through its last step
-    unsigned* scene_cost;           // batched kernel, optional: per scene slot the device time (ns) of its
-                                    // last step, 0 before its first; orders the next step's queue
     const SceneDesc* scenes;
     SceneState* sstate;
 

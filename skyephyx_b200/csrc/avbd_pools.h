@@ -65,7 +65,6 @@ struct Pools {
     std::vector<size_t> owned_bytes;   // size of each owned allocation (snapshots)
     SceneDesc* d_scenes = nullptr;
     SceneState* d_sstate = nullptr;
-    unsigned* d_cost = nullptr;   // per slot: device ns of its last step (0 = not yet stepped)
 
     ~Pools() { release(); }
     void release() {
@@ -109,10 +108,8 @@ struct Pools {
 #define A(expr) if ((e = (expr)) != cudaSuccess) return e
         A(alloc(d_scenes, ns));
         A(alloc(d_sstate, ns));
-        A(alloc(d_cost, ns));
         W.scenes = d_scenes;
         W.sstate = d_sstate;
-        W.scene_cost = d_cost;
         W.nscenes = ns;
         A(alloc(W.pos, nb)); A(alloc(W.rot, nb)); A(alloc(W.scale, nb)); A(alloc(W.lpos, nb));
         A(alloc(W.lrot, nb)); A(alloc(W.ipos, nb)); A(alloc(W.irot, nb)); A(alloc(W.vel, nb));
@@ -607,7 +604,6 @@ inline void upload_scene(Pools& P, const HostScene& h, const StaticInc& si, cons
     sink.put(W.rgradN, h.rgradN, 6 * (size_t)d.tri0); sink.put(W.rparam, h.rparam, d.tri0);
     sink.put(P.d_scenes, std::vector<SceneDesc>(1, d), slot);
     sink.zero(P.d_sstate, slot, 1);
-    sink.zero(P.d_cost, slot, 1);
     sink.finish();
 }
 
@@ -703,9 +699,7 @@ struct AvbdBatch {
     avbd::host::Pools P;
     avbd::host::Allocs A;
     int* d_order = nullptr;          // live slots, largest first (queue_key)
-    int* d_order_run = nullptr;      // the queue a step runs: d_order by last step's device time
     int queue_body_weight = 1;       // queue key = weight x bodies + tets (avbd_batch_set_queue_weight)
-    int queue_by_time = 1;           // order each step's queue by device time (avbd_batch_set_queue_order)
     int* d_nlive = nullptr;
     int* d_queue = nullptr;
     int nlive = 0;

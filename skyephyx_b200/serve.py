@@ -202,9 +202,6 @@ class _BatchKnobs:
     def set_queue_weight(self, body_weight):
         check(self._lib.avbd_batch_set_queue_weight(self._h, int(body_weight)), "set_queue_weight")
 
-    def set_queue_order(self, by_time):
-        check(self._lib.avbd_batch_set_queue_order(self._h, int(bool(by_time))), "set_queue_order")
-
     def set_grid_broadphase(self, min_bodies):
         check(self._lib.avbd_batch_set_grid_broadphase(self._h, int(min_bodies)), "set_grid_broadphase")
 

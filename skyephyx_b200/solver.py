@@ -445,11 +445,6 @@ class Batch:
         """Queue order key: body_weight x bodies + tets, largest first."""
         check(self._lib.avbd_batch_set_queue_weight(self._h, int(body_weight)), "set_queue_weight")
 
-    def set_queue_order(self, by_time=True):
-        """Order each step's queue by the scenes' device time in the previous
-        step (longest first; the default) or by size alone."""
-        check(self._lib.avbd_batch_set_queue_order(self._h, int(bool(by_time))), "set_queue_order")
-
     def set_scene_timing(self, on=True):
         """Per-scene device timing of each step (global timer stamps at the
         start and end of every scene's step)."""
