@@ -109,9 +109,9 @@ class ClockSampler:
 
 
 # DRAM bytes (read + write) per launch per dynamic body: one ncu capture of
-# the 1,024-scene mix of this workload under the 4,096-scene launch (3.087 GB
-# read + 0.831 GB written over 432,494 dynamic bodies).
-TRAFFIC_PER_DYNAMIC_BODY = 3.918e9 / 432494
+# the 1,024-scene mix of this workload under the 4,096-scene launch (3.769 GB
+# read + 0.944 GB written over 432,494 dynamic bodies).
+TRAFFIC_PER_DYNAMIC_BODY = 4.714e9 / 432494
 # FMA-pipe and DRAM utilisation of the FEM work: one ncu capture of the FEM
 # blocks of the 1,024-scene mix under the benchmark launch (FMA pipe cycles
 # active, of active cycles: mean over SMs and the busiest SM; DRAM throughput
