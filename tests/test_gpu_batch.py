@@ -292,6 +292,37 @@ def test_prepare_then_remove_and_add_admits_the_new_scene():
     assert same(b.get_state(0)[:2], alone.get_state(0)[:2])
 
 
+def moving_boxes(s, seed, n=24):
+    """Boxes thrown with linear and angular velocity over a static ground."""
+    rng = np.random.default_rng(seed)
+    s.add_body(scenes.CUBE, 1.0, 0.5, (0, -0.5, 0), (40, 1, 40), is_static=True)
+    for i in range(n):
+        s.add_body(scenes.CUBE, 1.0 + 0.1 * i, 0.4, (rng.uniform(-4, 4), rng.uniform(1, 4), rng.uniform(-4, 4)),
+                   (rng.uniform(0.4, 1.2), rng.uniform(0.4, 1.2), rng.uniform(0.4, 1.2)),
+                   vel=tuple(rng.uniform(-3, 3, 3)), omega=tuple(rng.uniform(-2, 2, 3)))
+
+
+def test_staged_upload_equals_direct_upload_for_moving_scenes():
+    """The first step's upload of staged scenes (one copy per device array;
+    zero data left to the freshly zeroed pools; the last and inertial poses
+    filled from the pose on the device) gives the device state a scene placed
+    in reserved pools gets from its own copies, bit for bit, for scenes that
+    start with velocities, at rest, or with tets."""
+    from skyephyx_b200 import Batch
+    builders = [lambda s: moving_boxes(s, 11), lambda s: scenes.fem_scene(s, 700, scenes.rng_for(4, 1)),
+                lambda s: moving_boxes(s, 12, n=40), lambda s: scenes.rigid_pile(s, 40, scenes.rng_for(4, 2))]
+    first = Batch()
+    for f in builders:
+        first.add_scene(staged(f))
+    assert first.step(3) == "ok"
+    later = Batch()
+    later.reserve(4096, 1024, 4096, 256, 8)   # pools in place: each scene is copied on its own
+    slots = [later.add_scene(staged(f)) for f in builders]
+    assert later.step(3) == "ok"
+    for i, slot in enumerate(slots):
+        assert same(first.get_state(i)[:4], later.get_state(slot)[:4]), f"scene {i}"
+
+
 def headline_slice(n_sample=256):
     """A slice of the 4,096-scene batched mix: every 16th scene plus the eight
     largest rigid and the eight largest FEM scenes."""
