@@ -680,81 +680,6 @@ void launch_primal(int group, const World& W, int cur, int first, int count, flo
     }
 }
 
-// ---------------------------------------------------------------------------
-// Flat FEM sweep of the single-scene path.  A scene with tets (and no
-// triangles) whose lanes per body the caller did not fix sweeps each colour as
-// the batched kernel's flat sweep does: one (particle, tet) term per thread
-// into device scratch (k_flat_terms), then each particle adds its rows and its
-// terms in incidence order and solves (k_flat_finish, flat_finish_split).
-// After each new colouring, k_flat_count / k_flat_scan / k_flat_records lay
-// out the tet-term records in colour-list order and leave in W.col_tinc the
-// inclusive prefix of terms over the list.
-// ---------------------------------------------------------------------------
-__global__ void k_flat_count(const __grid_constant__ World W) {
-    const SceneDesc sc = W.scenes[0];
-    const int n = W.col_start[W.sstate->ncolours];
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x)
-        W.col_tinc[sc.body0 + i] = tet_terms(W, W.col_list[sc.body0 + i]);
-}
-
-__global__ void k_flat_scan(const __grid_constant__ World W) {
-    __shared__ TeamShared s_team;
-    const Team T = Team::cta(&s_team, nullptr, 0);
-    const SceneDesc sc = W.scenes[0];
-    const int n = W.col_start[W.sstate->ncolours];
-    block_exclusive_scan(T, W.col_tinc + sc.body0, W.col_tinc + sc.body0, n);
-}
-
-__global__ void k_flat_records(const __grid_constant__ World W) {
-    const SceneDesc sc = W.scenes[0];
-    const int n = W.col_start[W.sstate->ncolours];
-    const size_t rec0 = 4 * (size_t)sc.tet0;
-    int* tinc = W.col_tinc + sc.body0;
-    for (int i = blockIdx.x * blockDim.x + threadIdx.x; i < n; i += gridDim.x * blockDim.x) {
-        const int b = W.col_list[sc.body0 + i];
-        const int k = min(tet_terms(W, b), W.inc_cnt[b]);   // the energies end the body's entries
-        const uint32_t* ent = W.inc + W.inc_off[b] + W.inc_cnt[b] - k;
-        const int q0 = tinc[i];
-        if (AVBD_CHECK(W, q0 >= 0 && q0 + k <= 4 * sc.ntet, 5, q0 + k, 4 * sc.ntet))
-            for (int e = 0; e < k; ++e) write_term_record(W, rec0 + q0 + e, ent[e]);
-        tinc[i] = q0 + k;
-    }
-}
-
-// Terms [q0, q1) of the scene's records into the nine planes of `sm`.
-__global__ void k_flat_terms(const __grid_constant__ World W, int q0, int q1, float* sm, int nslots) {
-    const SceneDesc sc = W.scenes[0];
-    const size_t rec0 = 4 * (size_t)sc.tet0;
-    q1 = min(q1, min(nslots, 4 * sc.ntet));
-    for (int q = max(q0, 0) + blockIdx.x * blockDim.x + threadIdx.x; q < q1; q += gridDim.x * blockDim.x) {
-        V3 g = v3(0.f, 0.f, 0.f);
-        S3 H;
-        s3_zero(H);
-        tet_term_record(W, rec0 + q, g, H);   // removed tets stay zero
-        sm[0 * (size_t)nslots + q] = g.x; sm[1 * (size_t)nslots + q] = g.y; sm[2 * (size_t)nslots + q] = g.z;
-        sm[3 * (size_t)nslots + q] = H.xx; sm[4 * (size_t)nslots + q] = H.yy; sm[5 * (size_t)nslots + q] = H.zz;
-        sm[6 * (size_t)nslots + q] = H.xy; sm[7 * (size_t)nslots + q] = H.xz; sm[8 * (size_t)nslots + q] = H.yz;
-    }
-}
-
-// The list's particles [v, vend) of one colour, L lanes each, across the grid
-// (every block a whole number of warps, so the grid is a team of warps).
-template <int L>
-__global__ void k_flat_finish(const __grid_constant__ World W, int cur, int v, int vend, float alpha, int stick,
-                              const float* sm, int nslots) {
-    Team T;
-    T.rank = blockIdx.x * blockDim.x + threadIdx.x;
-    T.size = gridDim.x * blockDim.x;
-    T.first_warp = 0;
-    T.bar = 0;
-    T.sh = nullptr;
-    T.stage = nullptr;
-    T.stage_cap = 0;
-    const SceneDesc sc = W.scenes[0];
-    flat_finish_split<L>(T, W, cur, W.col_list + sc.body0, W.col_tinc + sc.body0, 0, v, vend, alpha, stick != 0, sm,
-                         nslots);
-}
-
 __global__ void k_dual(const __grid_constant__ World W, int cur, int nlive, float alpha, int last) {
     const SceneDesc sc = W.scenes[0];
     const int n = sc.nforce + nlive;
@@ -970,25 +895,6 @@ int sync_state(AvbdWorld* w) {
     return 0;
 }
 
-// One colour of the flat FEM sweep: the colour's terms, then its particles.
-void launch_flat(AvbdWorld* w, int cur, int first, int count, float alpha, int stick) {
-    const World& W = w->P.W;
-    cudaStream_t s = w->stream;
-    const int q0 = first > 0 ? w->tinc[first - 1] : 0, q1 = w->tinc[first + count - 1];
-    if (q1 > q0) k_flat_terms<<<blocks_for(q1 - q0), kThreads, 0, s>>>(W, q0, q1, w->flat_terms, w->flat_slots);
-    const int v = first, vend = first + count;
-    // 9 lanes per particle while the colour is small, then 3, then 1 (32 / L particles per warp)
-    if (count <= 4096)
-        k_flat_finish<9><<<blocks_for((count + 2) / 3 * 32), kThreads, 0, s>>>(W, cur, v, vend, alpha, stick,
-                                                                           w->flat_terms, w->flat_slots);
-    else if (count <= 16384)
-        k_flat_finish<3><<<blocks_for((count + 9) / 10 * 32), kThreads, 0, s>>>(W, cur, v, vend, alpha, stick,
-                                                                            w->flat_terms, w->flat_slots);
-    else
-        k_flat_finish<1><<<blocks_for(count), kThreads, 0, s>>>(W, cur, v, vend, alpha, stick, w->flat_terms,
-                                                              w->flat_slots);
-}
-
 int upload(AvbdWorld* w) {
     int r = device_ready(w->device);
     if (r) return r;
@@ -1024,9 +930,6 @@ int upload(AvbdWorld* w) {
         P.alloc(w->nbr_key, (size_t)P.nb) != cudaSuccess || P.alloc(w->nbr_pos, (size_t)P.nb) != cudaSuccess ||
         P.alloc(w->nbr_used, (size_t)P.nb) != cudaSuccess)
         return AVBD_ERR_NOMEM;
-    w->flat_slots = std::max(1, 4 * P.nt);
-    if (P.alloc(w->flat_terms, 9 * (size_t)w->flat_slots, false) != cudaSuccess) return AVBD_ERR_NOMEM;
-    w->flat_ready = false;
     w->uploaded = true;
     return 0;
 }
@@ -1151,7 +1054,6 @@ int world_step(AvbdWorld* w) {
     phases.next("colouring");
     // ---- colouring, grid-wide (skipped when the contact graph is unchanged) ----
     const int adaptive = w->group == 0 && (w->h.ntet() > 0 || w->h.ntri() > 0) && d.nbody > 0;
-    int colour_flags[2] = {0, 0};
     {
         ColourState* cs = static_cast<ColourState*>(w->colour);
         const ColourLists L{w->nbr, w->nbr_cnt, w->nbr_key, w->nbr_pos, w->nbr_used};
@@ -1159,7 +1061,7 @@ int world_step(AvbdWorld* w) {
         k_col_init<<<nb, kThreads, 0, s>>>(P.W, cs, L);
         // Rounds in chunks of 8; between chunks the host reads whether the
         // pass has ended (and, after the first, whether colouring is skipped).
-        int* flags = colour_flags;   // skip, done
+        int flags[2] = {0, 0};   // skip, done
         for (int pass = 0; pass < 2 && !flags[0]; ++pass) {
             if (pass == 1) {
                 k_col_repass<<<nb, kThreads, 0, s>>>(P.W, cs);
@@ -1190,25 +1092,10 @@ int world_step(AvbdWorld* w) {
     // for scenes with energies, by this step's incidence entries per body
     // (a 0.05 m tet block's particles carry about 90: 32 lanes share them).
     const int group = adaptive ? adaptive_group(w->st.ninc, d.nbody) : d.group;
-    // the flat sweep where the batched kernel would use it: tets, no triangles
-    const bool flat = w->group == 0 && w->h.ntet() > 0 && w->h.ntri() == 0 && d.nbody > 0;
     w->ncolours = ncol;
     w->col_start.resize(ncol + 1);
     cudaMemcpyAsync(w->col_start.data(), P.W.col_start, (ncol + 1) * sizeof(int), cudaMemcpyDeviceToHost, s);
     cudaStreamSynchronize(s);
-    if (!flat) {
-        w->flat_ready = false;
-    } else if (!colour_flags[0] || !w->flat_ready) {   // new colour lists: records and term prefix
-        const int nlisted = w->col_start[ncol];
-        k_flat_count<<<blocks_for(nlisted), kThreads, 0, s>>>(P.W);
-        k_flat_scan<<<1, 1024, 0, s>>>(P.W);
-        k_flat_records<<<blocks_for(nlisted), kThreads, 0, s>>>(P.W);
-        w->tinc.resize(std::max(nlisted, 1));
-        if (nlisted > 0)
-            cudaMemcpyAsync(w->tinc.data(), P.W.col_tinc + d.body0, nlisted * sizeof(int), cudaMemcpyDeviceToHost, s);
-        if (cudaStreamSynchronize(s) != cudaSuccess) return AVBD_ERR_CUDA;
-        w->flat_ready = true;
-    }
     // ---- prediction ----
     k_predict<<<blocks_for(d.nbody), kThreads, 0, s>>>(P.W);
     cudaEventRecord(w->ev[4], s);
@@ -1219,8 +1106,7 @@ int world_step(AvbdWorld* w) {
     for (int it = 0; it < w->params.num_iterations; ++it) {
         for (int c = 0; c < ncol; ++c) {
             const int n = w->col_start[c + 1] - w->col_start[c];
-            if (n > 0 && flat) launch_flat(w, cur, w->col_start[c], n, alpha, 0);
-            else if (n > 0) launch_primal(group, P.W, cur, w->col_start[c], n, alpha, 0, s);
+            if (n > 0) launch_primal(group, P.W, cur, w->col_start[c], n, alpha, 0, s);
         }
         const int last = it == w->params.num_iterations - 1;
         if (d.nforce + nlive > 0)
@@ -1253,8 +1139,7 @@ int world_step(AvbdWorld* w) {
     if (w->params.post_stabilization) {
         for (int c = 0; c < ncol; ++c) {
             const int n = w->col_start[c + 1] - w->col_start[c];
-            if (n > 0 && flat) launch_flat(w, cur, w->col_start[c], n, 0.f, 1);
-            else if (n > 0) launch_primal(group, P.W, cur, w->col_start[c], n, 0.f, 1, s);
+            if (n > 0) launch_primal(group, P.W, cur, w->col_start[c], n, 0.f, 1, s);
         }
     }
     cudaEventRecord(w->ev[7], s);
@@ -1502,7 +1387,6 @@ int32_t avbd_restore(AvbdWorld* w, const void* src, int64_t bytes) {
     }
     if (cudaStreamSynchronize(w->stream) != cudaSuccess) return AVBD_ERR_CUDA;
     w->stopped = h.stopped != 0;
-    w->flat_ready = false;   // the host's term prefix is re-read with the restored colour lists
     return sync_state(w);
 }
 

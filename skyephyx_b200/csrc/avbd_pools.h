@@ -680,13 +680,6 @@ struct AvbdWorld {
     int* nbr_pos = nullptr;                  // per body: neighbours scanned this pass
     unsigned long long* nbr_used = nullptr;  // per body: colours seen so far
     size_t nbr_cap = 0;
-    // flat FEM sweep: term results (nine planes of flat_slots), the term
-    // prefix over the colour lists as last copied, and whether the tet-term
-    // records describe the current colour lists
-    float* flat_terms = nullptr;
-    int flat_slots = 0;
-    std::vector<int> tinc;
-    bool flat_ready = false;
 };
 
 // ===========================================================================

@@ -116,35 +116,6 @@ def test_flat_sweep_matches_one_lane_per_particle():
         assert np.abs(q1 - qf).max(initial=0.0) <= 1e-5, f"scene {i}"
 
 
-def test_single_scene_flat_sweep_equals_batched_flat_sweep():
-    """A single-scene world with tets (lanes per body left to the library)
-    sweeps its colours term by term across the grid; it gives the batched
-    kernel's flat sweep bit for bit, step after step, and keeps doing so after
-    a snapshot is restored."""
-    from skyephyx_b200 import GROUP_FLAT, Solver
-    steps = 6
-    batched = run_groups(FEM_BUILDERS, GROUP_FLAT, steps)
-    for i, build in enumerate(FEM_BUILDERS):
-        w = Solver()
-        build(w)
-        for _ in range(steps):
-            assert w.step() == "ok"
-        assert same(w.get_state()[:2], batched[i]), f"scene {i}"
-    w = Solver()
-    FEM_BUILDERS[0](w)
-    for _ in range(2):
-        w.step()
-    snap = w.snapshot()
-    for _ in range(steps - 2):
-        w.step()
-    after = w.get_state()[:2]
-    w.restore(snap)
-    for _ in range(steps - 2):
-        w.step()
-    assert same(w.get_state()[:2], after)
-    assert same(after, batched[0])
-
-
 def test_flat_sweep_matches_oracle(oracle_mod):
     from skyephyx_b200 import GROUP_FLAT
     flat = run_groups(FEM_BUILDERS, GROUP_FLAT, 1)
