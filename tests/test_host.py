@@ -180,3 +180,21 @@ def test_cpp_facade_compiles_and_links(tmp_path):
            "-L", os.path.dirname(lib), "-lavbd", "-Wl,-rpath," + os.path.dirname(lib), "-o", str(out)]
     r = subprocess.run(cmd, capture_output=True, text=True)
     assert r.returncode == 0, r.stderr
+
+
+def test_staging_sinks(tmp_path):
+    """The scene staging sinks on the host: a pose staged once for the three
+    arrays that start equal to it (one host buffer plus two device-side
+    copies, or one arena copy scattered three times), zero data left to the
+    freshly zeroed pools, and writes past a pool array refused."""
+    import shutil
+    nvcc = shutil.which("nvcc") or "/usr/local/cuda/bin/nvcc"
+    if not os.path.exists(nvcc) and not shutil.which(nvcc):
+        pytest.skip("no nvcc")
+    out = tmp_path / "staging_sinks"
+    cmd = [nvcc, "-std=c++17", "-O1", "-Wno-deprecated-gpu-targets", "-I", os.path.join(ROOT, "skyephyx_b200", "csrc"),
+           "-I", os.path.join(ROOT, "include"), os.path.join(ROOT, "tests", "cpp", "staging_sinks.cu"), "-o", str(out)]
+    r = subprocess.run(cmd, capture_output=True, text=True)
+    assert r.returncode == 0, r.stderr
+    r = subprocess.run([str(out)], capture_output=True, text=True, timeout=120)
+    assert r.returncode == 0 and r.stdout.strip() == "OK", r.stdout + r.stderr
